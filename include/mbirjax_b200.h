@@ -1,0 +1,178 @@
+/*
+ * mbirjax_b200 -- C ABI of the B200 (sm_100a) kernels for the MBIR hot path.
+ *
+ * Every entry point takes raw device pointers, sizes and a cudaStream_t (passed as void*), returns 0 on
+ * success or a negative MBX_ERR_* code, never throws and never traps.  The caller owns all buffers;
+ * entry points that need scratch memory take a caller-provided workspace whose size the matching
+ * *_workspace_bytes query returns.  Nothing synchronises the stream, so every entry point can be
+ * captured in a CUDA graph.  Out-of-range pixel or view indices found on the device are skipped and
+ * recorded in a device error word that mbx_get_device_error() reads (and clears).
+ *
+ * Data layout (all float32, C order):
+ *   recon / flat recon     (num_recon_rows * num_recon_cols, num_recon_slices)  -- one voxel cylinder per pixel
+ *   voxel_values           (num_pixels, num_recon_slices)
+ *   sinogram               (num_views, num_det_rows, num_det_channels)
+ *   pixel_indices          int32, indices into the flattened (num_recon_rows, num_recon_cols) grid
+ *   view_indices           int32 or NULL (NULL = all views in order)
+ *
+ * Each declaration names the reference (mbirjax v0.6.7) interface it replaces.
+ */
+#ifndef MBIRJAX_B200_H
+#define MBIRJAX_B200_H
+
+#include <stddef.h>
+#include <stdint.h>
+
+#ifdef __cplusplus
+extern "C" {
+#endif
+
+#if defined(__GNUC__)
+#define MBX_API __attribute__((visibility("default")))
+#else
+#define MBX_API
+#endif
+
+#define MBX_OK 0
+#define MBX_ERR_INVALID_ARG (-1)
+#define MBX_ERR_UNSUPPORTED (-2)
+#define MBX_ERR_CUDA (-3)
+#define MBX_ERR_WORKSPACE (-4)
+
+#define MBX_GEOM_PARALLEL 0
+#define MBX_GEOM_CONE 1
+
+/* Largest psf_radius / bp_psf_radius the kernels accept. */
+#define MBX_MAX_PSF_RADIUS 4
+
+/* Projector geometry.  Replaces the (sinogram_shape, recon_shape, geometry_params) namedtuple that
+ * Projectors.create_projectors closes over (projectors.py:47-54), built from
+ * ParallelBeamModel.get_geometry_parameters (parallel_beam.py:94-113) or
+ * ConeBeamModel.get_geometry_parameters (cone_beam.py:110-136). */
+typedef struct mbx_geom {
+    int32_t kind;                        /* MBX_GEOM_PARALLEL or MBX_GEOM_CONE */
+    int32_t num_views;                   /* sinogram_shape[0]; length of angles */
+    int32_t num_det_rows;                /* sinogram_shape[1] */
+    int32_t num_det_channels;            /* sinogram_shape[2] */
+    int32_t num_recon_rows;              /* recon_shape[0] */
+    int32_t num_recon_cols;              /* recon_shape[1] */
+    int32_t num_recon_slices;            /* recon_shape[2] (== num_det_rows for parallel beam) */
+    int32_t psf_radius;                  /* get_psf_radius() */
+    int32_t bp_psf_radius;               /* cone only: ConeBeamModel.bp_psf_radius */
+    int32_t entries_per_cylinder_batch;  /* cone only: 128 in the reference */
+    float delta_det_channel;
+    float delta_det_row;
+    float det_channel_offset;
+    float det_row_offset;
+    float delta_voxel;
+    float recon_slice_offset;            /* cone only */
+    float source_detector_dist;          /* cone only; +inf allowed */
+    float magnification;                 /* cone only; source_detector_dist / source_iso_dist */
+    const float *angles;                 /* device pointer, num_views angles in radians */
+} mbx_geom;
+
+/* qGGMRF prior parameters (b, sigma_x, p, q, T) as TomographyModel.create_vcd_subset_updater builds them
+ * (tomography_model.py:1325-1327); b from get_b_from_nbr_wts (qggmrf.py:388-395), order
+ * [row+1, row-1, col+1, col-1, slice+1, slice-1]. */
+typedef struct mbx_qggmrf_params {
+    float b[6];
+    float sigma_x;
+    float p;
+    float q;
+    float T;
+} mbx_qggmrf_params;
+
+/* Library identification and error reporting. */
+MBX_API const char *mbx_version(void);
+MBX_API const char *mbx_error_string(int code);
+/* The CUDA error code behind the last MBX_ERR_CUDA returned on this host thread. */
+MBX_API int mbx_last_cuda_error(void);
+/* Reads and clears the device error word of the current device (synchronises the device).
+ * Bit 0: a pixel index was out of range; bit 1: a view index was out of range. */
+MBX_API int mbx_get_device_error(int *flags_out);
+
+/* ---- projectors ------------------------------------------------------------------------------- */
+
+/* Workspace the forward projector needs for a call with these sizes (0 when it needs none). */
+MBX_API size_t mbx_forward_project_workspace_bytes(const mbx_geom *g, int64_t num_pixels, int32_t num_views_sel);
+
+/* Sparse forward projection: voxel_values (num_pixels, S) at pixel_indices -> sinogram_out
+ * (num_views_sel, R, C), every element written.  Output view j uses angle view_indices[j] (or j).
+ * Replaces Projectors.sparse_forward_project (projectors.py:61-129) over
+ * ParallelBeamModel.forward_project_pixel_batch_to_one_view (parallel_beam.py:138-178) /
+ * ConeBeamModel.forward_project_pixel_batch_to_one_view (cone_beam.py:189-377), as called by
+ * TomographyModel.sparse_forward_project (tomography_model.py:576-622). */
+MBX_API int mbx_sparse_forward_project(const mbx_geom *g, const float *voxel_values, const int32_t *pixel_indices,
+                               int64_t num_pixels, const int32_t *view_indices, int32_t num_views_sel,
+                               float *sinogram_out, void *workspace, size_t workspace_bytes, void *stream);
+
+/* Workspace the back projector needs for a call with these sizes (0 when it needs none). */
+MBX_API size_t mbx_back_project_workspace_bytes(const mbx_geom *g, int64_t num_pixels, int32_t num_views_sel);
+
+/* Sparse back projection of a full sinogram (num_views, R, C) to out (num_pixels, S) (overwritten):
+ *   out = scale * sum_views A^coeff_power^T (weights * sinogram)
+ * over views view_indices[0..num_views_sel) (or all).  weights may be NULL (all ones); scale is 1 for the
+ * reference's sparse_back_project.  coeff_power is 1 (back projection) or 2 (Hessian diagonal).
+ * Replaces Projectors.sparse_back_project (projectors.py:131-209) over
+ * ParallelBeamModel.back_project_one_view_to_pixel_batch (parallel_beam.py:180-221) /
+ * ConeBeamModel.back_project_one_view_to_pixel_batch (cone_beam.py:379-541), as called by
+ * TomographyModel.sparse_back_project (tomography_model.py:624-677) and compute_hessian_diagonal
+ * (tomography_model.py:679-708). */
+MBX_API int mbx_sparse_back_project(const mbx_geom *g, const float *sinogram, const float *weights,
+                            const int32_t *pixel_indices, int64_t num_pixels, const int32_t *view_indices,
+                            int32_t num_views_sel, int32_t coeff_power, float scale, float *out,
+                            void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- qGGMRF prior ----------------------------------------------------------------------------- */
+
+/* Surrogate gradient and Hessian diagonal at pixel_indices (num_pixels, S) each.
+ * Replaces qggmrf_gradient_and_hessian_at_indices (qggmrf.py:118-279). */
+MBX_API int mbx_qggmrf_grad_hess(const float *flat_recon, int32_t num_recon_rows, int32_t num_recon_cols,
+                         int32_t num_recon_slices, const int32_t *pixel_indices, int64_t num_pixels,
+                         const mbx_qggmrf_params *qp, float *grad_out, float *hess_out, void *stream);
+
+/* Workspace for mbx_qggmrf_loss_grad. */
+MBX_API size_t mbx_qggmrf_loss_grad_workspace_bytes(int32_t num_recon_rows, int32_t num_recon_cols,
+                                            int32_t num_recon_slices);
+
+/* qGGMRF loss (written to *loss_out, a device double) and its gradient grad_out (full recon shape,
+ * overwritten; may be NULL).  Replaces qggmrf_loss (qggmrf.py:31-65) and its autodiff gradient. */
+MBX_API int mbx_qggmrf_loss_grad(const float *recon, int32_t num_recon_rows, int32_t num_recon_cols,
+                         int32_t num_recon_slices, const mbx_qggmrf_params *qp, double *loss_out,
+                         float *grad_out, void *workspace, size_t workspace_bytes, void *stream);
+
+/* ---- VCD subset update ------------------------------------------------------------------------ */
+
+/* Workspace for one mbx_vcd_subset_step with these sizes. */
+MBX_API size_t mbx_vcd_subset_step_workspace_bytes(const mbx_geom *g, int64_t num_pixels);
+
+/* One VCD subset update, fully on the device (no host synchronisation):
+ *   delta = -(g_fwd + g_prior) / (h_fwd + h_prior),  g_fwd = -fm * A^T (w e),  h_fwd = fm * H[idx]
+ *   alpha = clip((fm <w e, A delta> - <g_prior, delta>) / (fm <w A delta, A delta> + <h_prior, delta^2>/2
+ *           + eps), eps, 1.5)
+ *   flat_recon[idx] += alpha delta;  error_sinogram -= alpha A delta
+ * weights may be NULL (constant weights 1).  The inner products accumulate in float64.  stats_out (a device
+ * double[4]) receives {alpha, sum|alpha delta|, forward_linear - prior_linear, denominator}.
+ * Replaces the vcd_subset_updater closure of TomographyModel.create_vcd_subset_updater
+ * (tomography_model.py:1310-1544) with get_forward_lin_quad (tomography_model.py:1546-1631) and
+ * update_recon (tomography_model.py:1820-1823). */
+MBX_API int mbx_vcd_subset_step(const mbx_geom *g, float *flat_recon, float *error_sinogram, const float *weights,
+                        const float *fm_hessian, const int32_t *pixel_indices, int64_t num_pixels,
+                        float fm_constant, const mbx_qggmrf_params *qp, double *stats_out, void *workspace,
+                        size_t workspace_bytes, void *stream);
+
+/* ---- FBP / FDK filtering ---------------------------------------------------------------------- */
+
+/* Direct-recon filtering of a sinogram (num_views, R, C) into out (same shape).
+ * Parallel beam: ramp filter x 1/delta_voxel^2, 'valid' convolution per row, x pi/num_views
+ * (replaces ParallelBeamModel.fbp_filter, parallel_beam.py:303-348).
+ * Cone beam: pre-weight D/sqrt(D^2+u^2+v^2), filter x delta_det_row/(delta_voxel^3 magnification),
+ * convolution, x pi/num_views (replaces ConeBeamModel.fdk_filter, cone_beam.py:779-846).
+ * The filter is generate_direct_recon_filter 'ramp' (tomography_utils.py:4-35). */
+MBX_API int mbx_direct_filter(const mbx_geom *g, const float *sinogram, float *out, void *stream);
+
+#ifdef __cplusplus
+}
+#endif
+
+#endif /* MBIRJAX_B200_H */

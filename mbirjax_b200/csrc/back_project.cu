@@ -1,0 +1,68 @@
+// Sparse back projector for parallel- and cone-beam geometry (sm_100a).
+//
+// Replaces Projectors.sparse_back_project (projectors.py:131-209) over the geometry plugins
+// ParallelBeamModel.back_project_one_view_to_pixel_batch (parallel_beam.py:180-221) and
+// ConeBeamModel.back_project_one_view_to_pixel_batch (cone_beam.py:379-541); coeff_power = 2 gives the
+// Hessian diagonal of TomographyModel.compute_hessian_diagonal (tomography_model.py:679-708).
+//
+// One thread owns one pixel and a tile of ST slices.  Its ST accumulators stay in registers across all
+// views, so there are no global atomics and no per-view partial cylinders.  Lanes run along pixels, so the
+// channel gathers of a warp fall in a narrow channel range of one detector row.  Per-view angle, cos and
+// sin are staged in shared memory.  For cone beam each thread first gathers, for every detector row its
+// slice tile touches in this view, the horizontal fan sum sum_k A_chan_k * sino[m, n_c + k] into its own
+// column of a shared-memory buffer (row-major across threads, so conflict-free), then applies the
+// voxel-centric vertical fan from that buffer; each detector row is therefore gathered once per view
+// instead of once per vertical tap.  The optional weights are multiplied into every gathered value
+// (a fused W * e).  Views may be split over CTAs with a fixed-order second-stage sum when there are too
+// few pixels to fill the GPU (caller workspace).
+#include "back_project.cuh"
+
+namespace mbx {
+
+size_t bp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel) {
+    return plan_bp(g, num_pixels, num_views_sel).workspace;
+}
+
+int back_project(const mbx_geom &g, const float *sino, const float *w, const int32_t *pix, long long num_pixels,
+                 const int32_t *views, int num_views_sel, int coeff_power, float scale, float *out, void *ws,
+                 size_t ws_bytes, cudaStream_t st) {
+    if (num_pixels == 0) return MBX_OK;
+    const BpPlan pl = plan_bp(g, num_pixels, num_views_sel);
+    if (pl.workspace > 0 && (ws == nullptr || ws_bytes < pl.workspace)) return MBX_ERR_WORKSPACE;
+    float *dst = pl.splits > 1 ? static_cast<float *>(ws) : out;
+    const long long stride = num_pixels * (long long)g.num_recon_slices;
+    const long long ss = pl.splits > 1 ? stride : 0;
+    cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
+                        ? launch_bp_parallel(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power,
+                                             scale, dst, ss, st)
+                        : launch_bp_cone(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power, scale,
+                                         dst, ss, st);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    if (pl.splits > 1) {
+        launch_split_sum(dst, stride, pl.splits, scale, out, stride, st);
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return set_cuda_error(e);
+    }
+    return MBX_OK;
+}
+
+}  // namespace mbx
+
+extern "C" size_t mbx_back_project_workspace_bytes(const mbx_geom *g, int64_t num_pixels, int32_t num_views_sel) {
+    if (mbx::validate_geom(g) != MBX_OK || num_pixels < 0 || num_views_sel <= 0) return 0;
+    return mbx::bp_workspace_bytes(*g, num_pixels, num_views_sel);
+}
+
+extern "C" int mbx_sparse_back_project(const mbx_geom *g, const float *sinogram, const float *weights,
+                                       const int32_t *pixel_indices, int64_t num_pixels, const int32_t *view_indices,
+                                       int32_t num_views_sel, int32_t coeff_power, float scale, float *out,
+                                       void *workspace, size_t workspace_bytes, void *stream) {
+    int rc = mbx::validate_geom(g);
+    if (rc != MBX_OK) return rc;
+    if (num_pixels < 0 || num_views_sel <= 0 || !sinogram) return MBX_ERR_INVALID_ARG;
+    if (num_pixels > 0 && (!pixel_indices || !out)) return MBX_ERR_INVALID_ARG;
+    if (coeff_power != 1 && coeff_power != 2) return MBX_ERR_UNSUPPORTED;
+    if (!view_indices && num_views_sel > g->num_views) return MBX_ERR_INVALID_ARG;
+    return mbx::back_project(*g, sinogram, weights, pixel_indices, num_pixels, view_indices, num_views_sel,
+                             coeff_power, scale, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
+}

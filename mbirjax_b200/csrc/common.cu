@@ -1,0 +1,109 @@
+// Library identification, error reporting and device queries for the mbirjax_b200 C ABI.
+#include <cstdio>
+
+#include "mbx_common.cuh"
+#include "mbx_host.hpp"
+
+// Device error word: bit flags set by kernels that met an out-of-range pixel or view index.
+__device__ int g_mbx_device_error = 0;
+
+namespace mbx {
+
+int *device_error_ptr() {
+    static int *cache[64] = {nullptr};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return nullptr;
+    }
+    if (!cache[dev]) {
+        void *p = nullptr;
+        if (cudaGetSymbolAddress(&p, g_mbx_device_error) != cudaSuccess) {
+            cudaGetLastError();
+            return nullptr;
+        }
+        cache[dev] = static_cast<int *>(p);
+    }
+    return cache[dev];
+}
+
+static thread_local int t_last_cuda_error = 0;
+
+int set_cuda_error(cudaError_t e) {
+    t_last_cuda_error = (int)e;
+    return MBX_ERR_CUDA;
+}
+
+int num_sms() {
+    static int cache[64] = {0};
+    int dev = 0;
+    if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
+        cudaGetLastError();
+        return kNumSMsDefault;
+    }
+    if (cache[dev] == 0) {
+        int n = 0;
+        if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
+            cudaGetLastError();
+            n = kNumSMsDefault;
+        }
+        cache[dev] = n;
+    }
+    return cache[dev];
+}
+
+int validate_geom(const mbx_geom *g) {
+    if (!g) return MBX_ERR_INVALID_ARG;
+    if (g->kind != MBX_GEOM_PARALLEL && g->kind != MBX_GEOM_CONE) return MBX_ERR_INVALID_ARG;
+    if (g->num_views <= 0 || g->num_det_rows <= 0 || g->num_det_channels <= 0) return MBX_ERR_INVALID_ARG;
+    if (g->num_recon_rows <= 0 || g->num_recon_cols <= 0 || g->num_recon_slices <= 0) return MBX_ERR_INVALID_ARG;
+    if ((long long)g->num_recon_rows * g->num_recon_cols > 2147483647LL) return MBX_ERR_UNSUPPORTED;
+    if (g->psf_radius < 0 || g->psf_radius > MBX_MAX_PSF_RADIUS) return MBX_ERR_UNSUPPORTED;
+    if (g->kind == MBX_GEOM_CONE && (g->bp_psf_radius < 0 || g->bp_psf_radius > MBX_MAX_PSF_RADIUS))
+        return MBX_ERR_UNSUPPORTED;
+    if (g->kind == MBX_GEOM_CONE && g->entries_per_cylinder_batch <= 0) return MBX_ERR_INVALID_ARG;
+    if (g->kind == MBX_GEOM_PARALLEL && g->num_recon_slices != g->num_det_rows) return MBX_ERR_INVALID_ARG;
+    if (!(g->delta_voxel > 0.0f) || !(g->delta_det_channel > 0.0f) || !(g->delta_det_row > 0.0f))
+        return MBX_ERR_INVALID_ARG;
+    if (g->kind == MBX_GEOM_CONE && (!(g->magnification > 0.0f) || !(g->source_detector_dist > 0.0f)))
+        return MBX_ERR_INVALID_ARG;
+    if (!g->angles) return MBX_ERR_INVALID_ARG;
+    return MBX_OK;
+}
+
+unsigned grid_for(long long n, int threads) {
+    long long blocks = (n + threads - 1) / threads;
+    const long long cap = 16LL * num_sms();
+    if (blocks > cap) blocks = cap;
+    if (blocks < 1) blocks = 1;
+    return (unsigned)blocks;
+}
+
+}  // namespace mbx
+
+extern "C" const char *mbx_version(void) { return "mbirjax_b200 0.1.0 (sm_100a)"; }
+
+extern "C" const char *mbx_error_string(int code) {
+    switch (code) {
+        case MBX_OK: return "ok";
+        case MBX_ERR_INVALID_ARG: return "invalid argument";
+        case MBX_ERR_UNSUPPORTED: return "unsupported configuration";
+        case MBX_ERR_CUDA: return "CUDA error (see mbx_last_cuda_error)";
+        case MBX_ERR_WORKSPACE: return "workspace missing or too small";
+        default: return "unknown error";
+    }
+}
+
+extern "C" int mbx_last_cuda_error(void) { return mbx::t_last_cuda_error; }
+
+extern "C" int mbx_get_device_error(int *flags_out) {
+    if (!flags_out) return MBX_ERR_INVALID_ARG;
+    int value = 0;
+    cudaError_t e = cudaDeviceSynchronize();
+    if (e == cudaSuccess) e = cudaMemcpyFromSymbol(&value, g_mbx_device_error, sizeof(int));
+    const int zero = 0;
+    if (e == cudaSuccess) e = cudaMemcpyToSymbol(g_mbx_device_error, &zero, sizeof(int));
+    if (e != cudaSuccess) return mbx::set_cuda_error(e);
+    *flags_out = value;
+    return MBX_OK;
+}

@@ -1,0 +1,388 @@
+"""TomographyModel: the reference's public model API on top of the mbirjax_b200 CUDA kernels.
+
+Drop-in for ``mbirjax.TomographyModel`` (``tomography_model.py:36-1815``) on the hot path:
+``set_params``/``get_params``, ``forward_project``/``back_project`` (``:531-574``),
+``sparse_forward_project``/``sparse_back_project`` (``:576-677``), ``compute_hessian_diagonal`` (``:679-708``),
+``auto_set_regularization_params`` (``:756-932``), ``direct_recon``/``direct_filter``, ``recon`` (``:966-1084``),
+``vcd_recon`` (``:1086-1255``) and ``get_forward_model_loss`` (``:1633-1658``).
+
+Arrays may be NumPy arrays or torch tensors; results are float32 torch tensors on the model's CUDA device
+(the reference returns JAX device arrays).  Every projection, prior and VCD step runs in the CUDA library
+through the C ABI (``mbirjax_b200._capi``); nothing here computes them on the CPU.  The host keeps only what
+the reference keeps on the host: parameters, partitions (NumPy, same ``np.random`` call order),
+auto-regularisation statistics and the iteration loop.
+"""
+import datetime
+from collections import namedtuple
+
+import numpy as np
+import torch
+
+from . import _capi
+from .parameter_handler import ParameterHandler
+from .vcd_utils import gen_full_indices, gen_set_of_pixel_partitions, gen_partition_sequence
+from .qggmrf import get_b_from_nbr_wts
+
+recon_param_names = ['num_iterations', 'granularity', 'partition_sequence', 'fm_rmse', 'prior_loss',
+                     'regularization_params', 'stop_threshold_change_pct', 'alpha_values']
+ReconParams = namedtuple('ReconParams', recon_param_names)
+
+
+def _cuda_device():
+    if not torch.cuda.is_available():
+        raise _capi.MbxError('mbirjax_b200 needs a CUDA device; none is visible')
+    return torch.device('cuda', torch.cuda.current_device())
+
+
+class TomographyModel(ParameterHandler):
+    """Base class of the geometry models; see ParallelBeamModel and ConeBeamModel."""
+
+    DIRECT_RECON_VIEW_BATCH_SIZE = 100
+
+    def __init__(self, sinogram_shape, **kwargs):
+        super().__init__()
+        self._geom = None
+        self._angles_dev = None
+        self.set_params(no_compile=True, no_warning=True, sinogram_shape=tuple(int(v) for v in sinogram_shape),
+                        **kwargs)
+        if self.get_params('delta_voxel') is None:
+            delta_voxel = self.get_params('delta_det_channel') / self.get_magnification()
+            self.set_params(no_compile=True, no_warning=True, delta_voxel=delta_voxel)
+        self.use_ror_mask = True
+        self.auto_set_recon_size(sinogram_shape, no_compile=True, no_warning=True)
+        self.set_params(geometry_type=str(type(self)))
+        self.verify_valid_params()
+        self.main_device = self.sinogram_device = self.worker = None
+        self.view_batch_size_for_vmap = 512
+        self.pixel_batch_size_for_vmap = 2048
+        self.transfer_pixel_batch_size = 100 * self.pixel_batch_size_for_vmap
+        self.use_gpu = 'full'
+        self.create_projectors()
+
+    # ------------------------------------------------------------------ parameters / geometry
+    def set_params(self, no_warning=False, no_compile=False, **kwargs):
+        recompile = super().set_params(no_warning=no_warning, no_compile=no_compile, **kwargs)
+        if any(self.params[k].recompile_flag for k in kwargs if k in self.params):
+            self._geom = None  # geometry record and device angles are rebuilt on next use
+        if recompile:
+            self.create_projectors()
+
+    def verify_valid_params(self):
+        super().verify_valid_params()
+        use_gpu = self.get_params('use_gpu')
+        if use_gpu not in ['automatic', 'full', 'sinograms', 'projections', 'none']:
+            raise ValueError("use_gpu must be one of 'automatic', 'full', 'sinograms', 'projections', 'none'")
+
+    def create_projectors(self):
+        """Counterpart of tomography_model.py:475-484: invalidates the cached mbx_geom record (built lazily)."""
+        self._geom = None
+
+    def get_geometry_parameters(self):
+        raise NotImplementedError
+
+    def _kind(self):
+        raise NotImplementedError
+
+    def _device(self):
+        return _cuda_device()
+
+    def _geometry(self):
+        """The mbx_geom record for the current parameters (device angle table kept alive on the model)."""
+        if self._geom is None:
+            dev = self._device()
+            sinogram_shape, recon_shape = self.get_params(['sinogram_shape', 'recon_shape'])
+            angles = np.asarray(self.get_params(self.get_params('view_params_name')), dtype=np.float32)
+            self._angles_dev = torch.as_tensor(angles, device=dev).contiguous()
+            gp = self.get_geometry_parameters()
+            g = _capi.MbxGeom()
+            g.kind = self._kind()
+            g.num_views, g.num_det_rows, g.num_det_channels = (int(v) for v in sinogram_shape)
+            g.num_recon_rows, g.num_recon_cols, g.num_recon_slices = (int(v) for v in recon_shape)
+            g.psf_radius = int(gp.psf_radius)
+            g.bp_psf_radius = int(getattr(gp, 'bp_psf_radius', 1))
+            g.entries_per_cylinder_batch = int(getattr(gp, 'entries_per_cylinder_batch', 128))
+            g.delta_det_channel = float(gp.delta_det_channel)
+            g.delta_det_row = float(self.get_params('delta_det_row'))
+            g.det_channel_offset = float(gp.det_channel_offset)
+            g.det_row_offset = float(self.get_params('det_row_offset'))
+            g.delta_voxel = float(gp.delta_voxel)
+            g.recon_slice_offset = float(getattr(gp, 'recon_slice_offset', 0.0))
+            g.source_detector_dist = float(getattr(gp, 'source_detector_dist', np.inf))
+            g.magnification = float(getattr(gp, 'magnification', 1.0))
+            g.angles = self._angles_dev.data_ptr()
+            if g.psf_radius > _capi.MBX_MAX_PSF_RADIUS or g.bp_psf_radius > _capi.MBX_MAX_PSF_RADIUS:
+                raise ValueError('psf radius %d / %d exceeds the supported maximum %d' % (
+                    g.psf_radius, g.bp_psf_radius, _capi.MBX_MAX_PSF_RADIUS))
+            self._geom = g
+        return self._geom
+
+    def _dev(self, x, dtype=torch.float32):
+        dev = self._device()
+        if isinstance(x, torch.Tensor):
+            return x.to(device=dev, dtype=dtype).contiguous()
+        return torch.as_tensor(np.ascontiguousarray(x), device=dev).to(dtype).contiguous()
+
+    # ------------------------------------------------------------------ projections
+    def get_voxels_at_indices(self, recon, indices):
+        recon_shape = self.get_params('recon_shape')
+        r = self._dev(recon).reshape((-1,) + tuple(recon_shape[2:]))
+        return r[self._dev(indices, torch.int64)]
+
+    def reshape_recon(self, recon):
+        return recon.reshape(self.get_params('recon_shape'))
+
+    def sparse_forward_project(self, voxel_values, pixel_indices, view_indices=None, output_device=None):
+        """(N, S) voxel cylinders at pixel_indices -> sinogram (len(view_indices), R, C)."""
+        recon_shape = self.get_params('recon_shape')
+        vox = self._dev(voxel_values)
+        pix = self._dev(pixel_indices, torch.int32)
+        if vox.ndim != 2 or vox.shape[0] != pix.shape[0] or vox.shape[1] != recon_shape[2]:
+            raise ValueError('voxel_values must have shape[0:2] = (num_indices, num_slices)')
+        views = None if view_indices is None else self._dev(view_indices, torch.int32)
+        out = _capi.forward_project(self._geometry(), vox, pix, views)
+        return out.cpu() if output_device == 'cpu' else out
+
+    def sparse_back_project(self, sinogram, pixel_indices, view_indices=None, coeff_power=1, output_device=None):
+        """Full sinogram -> (N, S) at pixel_indices; view_indices select rows of sinogram and angles."""
+        sinogram_shape = self.get_params('sinogram_shape')
+        sino = self._dev(sinogram)
+        if tuple(sino.shape) != tuple(sinogram_shape):
+            raise ValueError('sinogram must have shape {}, got {}'.format(sinogram_shape, tuple(sino.shape)))
+        pix = self._dev(pixel_indices, torch.int32)
+        views = None if view_indices is None else self._dev(view_indices, torch.int32)
+        out = _capi.back_project(self._geometry(), sino, pix, views, coeff_power=coeff_power)
+        return out.cpu() if output_device == 'cpu' else out
+
+    def forward_project(self, recon):
+        recon_shape = self.get_params('recon_shape')
+        full_indices = gen_full_indices(recon_shape, use_ror_mask=self.use_ror_mask)
+        voxel_values = self.get_voxels_at_indices(recon, full_indices)
+        return self.sparse_forward_project(voxel_values, full_indices)
+
+    def back_project(self, sinogram):
+        recon_shape = self.get_params('recon_shape')
+        full_indices = gen_full_indices(recon_shape, use_ror_mask=self.use_ror_mask)
+        cyl = self.sparse_back_project(sinogram, full_indices)
+        recon = torch.zeros((recon_shape[0] * recon_shape[1], recon_shape[2]), dtype=torch.float32,
+                            device=cyl.device)
+        recon[torch.as_tensor(full_indices, device=cyl.device, dtype=torch.int64)] = cyl
+        return recon.reshape(recon_shape)
+
+    def compute_hessian_diagonal(self, weights=None, output_device=None):
+        """Back projection of the weights with squared coefficients over every pixel (no ROR mask)."""
+        sinogram_shape, recon_shape = self.get_params(['sinogram_shape', 'recon_shape'])
+        w = None
+        if weights is not None:
+            w = self._dev(weights)
+            if tuple(w.shape) != tuple(sinogram_shape):
+                raise ValueError('Weights must be constant or an array compatible with sinogram'
+                                 '\nGot weights.shape = {}, but sinogram.shape = {}'.format(tuple(w.shape),
+                                                                                           sinogram_shape))
+        nr, nc, ns = recon_shape
+        idx = torch.arange(nr * nc, dtype=torch.int32, device=self._device())
+        if w is None:
+            w = torch.ones(tuple(sinogram_shape), dtype=torch.float32, device=self._device())
+        return _capi.back_project(self._geometry(), w, idx, coeff_power=2).reshape((nr, nc, ns))
+
+    # ------------------------------------------------------------------ direct recon
+    def direct_filter(self, sinogram, filter_name='ramp', view_batch_size=DIRECT_RECON_VIEW_BATCH_SIZE):
+        if filter_name not in ['ramp']:
+            raise ValueError('Unsupported filter. Supported filters are: ramp.')
+        return _capi.direct_filter(self._geometry(), self._dev(sinogram))
+
+    def direct_recon(self, sinogram, filter_name='ramp', view_batch_size=DIRECT_RECON_VIEW_BATCH_SIZE):
+        return self.back_project(self.direct_filter(sinogram, filter_name=filter_name,
+                                                    view_batch_size=view_batch_size))
+
+    # ------------------------------------------------------------------ regularisation
+    def auto_set_regularization_params(self, sinogram, weights=None):
+        """tomography_model.py:756-796 (host NumPy on at most 20 subsampled views)."""
+        if self.get_params('auto_regularize_flag'):
+            num_views = sinogram.shape[0]
+            max_views_to_use = np.minimum(20, num_views)
+            step_size = num_views // max_views_to_use
+            small_sinogram = _to_numpy(sinogram[::step_size])
+            small_weights = 1 if weights is None else _to_numpy(weights[::step_size])
+            sino_indicator = self._get_sino_indicator(small_sinogram)
+            self.auto_set_sigma_y(small_sinogram, sino_indicator, small_weights)
+            recon_std = self._get_estimate_of_recon_std(small_sinogram, sino_indicator)
+            self.auto_set_sigma_x(recon_std)
+            self.auto_set_sigma_prox(recon_std)
+        names = ['sigma_y', 'sigma_x', 'sigma_prox']
+        return dict(zip(names, [float(v) for v in self.get_params(names)]))
+
+    def auto_set_sigma_y(self, sinogram, sino_indicator, weights=1):
+        snr_db = self.get_params('snr_db')
+        magnification = self.get_magnification()
+        delta_voxel, delta_det_channel = self.get_params(['delta_voxel', 'delta_det_channel'])
+        signal_rms = float(np.average(weights * sinogram ** 2, None, sino_indicator) ** 0.5)
+        rel_noise_std = 10 ** (-snr_db / 20)
+        pixel_pitch_relative_to_default = delta_voxel / (delta_det_channel / magnification)
+        sigma_y = np.float32(rel_noise_std * signal_rms * (pixel_pitch_relative_to_default ** 0.5))
+        self.set_params(no_warning=True, sigma_y=sigma_y, auto_regularize_flag=True)
+
+    def auto_set_sigma_x(self, recon_std):
+        sigma_x = np.float32(0.2 * (2 ** self.get_params('sharpness')) * recon_std)
+        self.set_params(no_warning=True, sigma_x=sigma_x, auto_regularize_flag=True)
+
+    def auto_set_sigma_prox(self, recon_std):
+        sigma_prox = np.float32(0.2 * (2 ** self.get_params('sharpness')) * recon_std)
+        self.set_params(no_warning=True, sigma_prox=sigma_prox, auto_regularize_flag=True)
+
+    @staticmethod
+    def _get_sino_indicator(sinogram):
+        return np.int8(sinogram > (0.01 * 5.0) * np.mean(np.fabs(sinogram)))
+
+    def _get_estimate_of_recon_std(self, sinogram, sino_indicator):
+        delta_det_channel, delta_voxel, recon_shape = self.get_params(['delta_det_channel', 'delta_voxel',
+                                                                       'recon_shape'])
+        magnification = self.get_magnification()
+        typical_sinogram_value = np.average(np.abs(sinogram), weights=sino_indicator)
+        path_space = (2 * recon_shape[0] * recon_shape[1]) / (recon_shape[0] + recon_shape[1]) * delta_voxel
+        path_sino = sinogram.shape[-1] * delta_det_channel / magnification
+        return typical_sinogram_value / np.minimum(path_space, path_sino)
+
+    def _qggmrf_params(self):
+        qggmrf_nbr_wts, sigma_x, p, q, T = self.get_params(['qggmrf_nbr_wts', 'sigma_x', 'p', 'q', 'T'])
+        return get_b_from_nbr_wts(qggmrf_nbr_wts), float(sigma_x), float(p), float(q), float(T)
+
+    # ------------------------------------------------------------------ reconstruction
+    @staticmethod
+    def get_forward_model_loss(error_sinogram, sigma_y, weights=None, normalize=True):
+        """tomography_model.py:1633-1658 (float64 accumulation on the device)."""
+        e = error_sinogram.double() if isinstance(error_sinogram, torch.Tensor) else torch.as_tensor(error_sinogram).double()
+        if weights is None:
+            w, avg = 1.0, 1.0
+        else:
+            w = weights.double() if isinstance(weights, torch.Tensor) else torch.as_tensor(weights).double()
+            avg = w.mean()
+        if normalize:
+            return float(torch.sqrt((1.0 / sigma_y ** 2) * torch.mean((e * e) * (w / avg))))
+        return float((1.0 / (2 * sigma_y ** 2)) * torch.sum((e * e) * w))
+
+    def recon(self, sinogram, weights=None, init_recon=None, max_iterations=15, stop_threshold_change_pct=0.2,
+              first_iteration=0, compute_prior_loss=False, num_iterations=None, logfile_path='./logs/recon.log',
+              print_logs=True):
+        """MBIR reconstruction by multi-granular VCD (tomography_model.py:966-1084)."""
+        if num_iterations is not None:
+            max_iterations = num_iterations
+        if first_iteration == 0 or self.logger is None:
+            self.setup_logger(logfile_path=logfile_path, print_logs=print_logs)
+        regularization_params = self.auto_set_regularization_params(sinogram, weights=weights)
+        recon_shape, granularity = self.get_params(['recon_shape', 'granularity'])
+        partitions = gen_set_of_pixel_partitions(recon_shape, granularity, use_ror_mask=self.use_ror_mask)
+        partition_sequence = gen_partition_sequence(self.get_params('partition_sequence'), max_iterations)
+        partition_sequence = partition_sequence[first_iteration:]
+        recon, loss_vectors = self.vcd_recon(sinogram, partitions, partition_sequence, stop_threshold_change_pct,
+                                             weights=weights, init_recon=init_recon,
+                                             compute_prior_loss=compute_prior_loss, first_iteration=first_iteration)
+        fm_rmse = [float(v) for v in loss_vectors[0]]
+        prior_loss = [float(v) for v in loss_vectors[1]] if compute_prior_loss else [0]
+        recon_params = ReconParams(len(fm_rmse), granularity, [int(v) for v in partition_sequence], fm_rmse,
+                                   prior_loss, regularization_params, [100 * float(v) for v in loss_vectors[2]],
+                                   [float(v) for v in loss_vectors[3]])._asdict()
+        notes = 'Reconstruction completed: {}\n\n'.format(datetime.datetime.now())
+        return recon, self.get_recon_dict(recon_params, notes=notes)
+
+    def get_recon_dict(self, recon_params, notes=''):
+        logs = self.log_buffer.getvalue() if self.log_buffer is not None else ''
+        model_params = {k: v.val for k, v in self.params.items()}
+        return {'recon_params': recon_params, 'notes': notes, 'recon_logs': logs, 'model_params': model_params}
+
+    def vcd_recon(self, sinogram, partitions, partition_sequence, stop_threshold_change_pct, weights=None,
+                  init_recon=None, prox_input=None, compute_prior_loss=False, first_iteration=0):
+        """tomography_model.py:1086-1308; each subset update is one mbx_vcd_subset_step on the device."""
+        if prox_input is not None:
+            raise NotImplementedError('prox_map is not on the mbirjax_b200 hot path')
+        if self.get_params('positivity_flag'):
+            raise NotImplementedError('positivity_flag=True is not on the mbirjax_b200 hot path')
+        recon_shape = self.get_params('recon_shape')
+        num_slices = recon_shape[2]
+        dev = self._device()
+        sino = self._dev(sinogram)
+        w = None if weights is None else self._dev(weights)
+        if init_recon is None:
+            init = self.direct_recon(sino)
+        elif isinstance(init_recon, int) and init_recon == 0:
+            init = torch.zeros(recon_shape, dtype=torch.float32, device=dev)
+        else:
+            init = self._dev(init_recon)
+        if tuple(init.shape) != tuple(recon_shape):
+            raise ValueError('init_recon does not have the correct shape. \nExpected {}, but got shape {} for '
+                             'init_recon shape.'.format(recon_shape, tuple(init.shape)))
+        # alpha minimising (1/2)||y - alpha A x||_W^2 (tomography_model.py:1137-1152)
+        error_sinogram = self.forward_project(init)
+        wes = error_sinogram if w is None else w * error_sinogram
+        norm = float(torch.sum(wes.double() * error_sinogram.double()))
+        alpha = float(torch.sum(wes.double() * sino.double())) / norm if norm > 0 else 1.0
+        error_sinogram = (sino - np.float32(alpha) * error_sinogram).contiguous()
+        flat_recon = (np.float32(alpha) * init).reshape((-1, num_slices)).contiguous()
+        del wes
+        sigma_y = float(self.get_params('sigma_y'))
+        fm_hessian = self.compute_hessian_diagonal(weights=w).reshape((-1, num_slices)).contiguous()
+        fm_constant = 1.0 / (sigma_y ** 2.0)
+        b, sigma_x, p, q, T = self._qggmrf_params()
+        qp = _capi.qggmrf_params(b, sigma_x, p, q, T)
+        geom = self._geometry()
+        dev_partitions = [torch.as_tensor(part, device=dev, dtype=torch.int32).contiguous() for part in partitions]
+        workspaces = {}
+        max_subsets = max(part.shape[0] for part in partitions)
+        stats = torch.zeros((max_subsets, 4), dtype=torch.float64, device=dev)
+        n_iter = len(partition_sequence)
+        fm_rmse, pm_loss, nmae_update, alpha_values = (np.zeros(n_iter) for _ in range(4))
+        num_iters = 0
+        if self.logger is not None:
+            self.logger.info('Starting VCD iterations')
+        for i in range(n_iter):
+            part = dev_partitions[int(partition_sequence[i])]
+            num_subsets, subset_size = part.shape
+            if subset_size not in workspaces:
+                workspaces[subset_size] = _capi.vcd_subset_step_workspace(geom, subset_size, dev)
+            for j, index in enumerate(np.random.permutation(num_subsets)):
+                _capi.vcd_subset_step(geom, flat_recon, error_sinogram, w, fm_hessian, part[int(index)], fm_constant,
+                                      qp, stats[j], workspaces[subset_size])
+            st = stats[:num_subsets].cpu().numpy()
+            ell1 = float(np.sum(st[:, 1]))
+            alpha_values[i] = float(np.mean(st[:, 0]))
+            fm_rmse[i] = self.get_forward_model_loss(error_sinogram, sigma_y, w)
+            nmae_update[i] = ell1 / float(torch.sum(torch.abs(flat_recon.double())))
+            if compute_prior_loss:
+                loss, _ = _capi.qggmrf_loss_grad(flat_recon.reshape(recon_shape), qp, need_grad=False)
+                pm_loss[i] = float(loss) / flat_recon.numel()
+            if self.logger is not None:
+                self.logger.info('After iteration {} of a max of {}: Pct change={:.4f}, Forward loss={:.4f}'.format(
+                    i + first_iteration, n_iter + first_iteration, 100 * nmae_update[i], fm_rmse[i]))
+            num_iters += 1
+            if nmae_update[i] < stop_threshold_change_pct / 100:
+                if self.logger is not None:
+                    self.logger.warning('Change threshold stopping condition reached')
+                break
+        self.last_error_sinogram = error_sinogram
+        return flat_recon.reshape(recon_shape), (fm_rmse[:num_iters], pm_loss[:num_iters], nmae_update[:num_iters],
+                                                 alpha_values[:num_iters])
+
+    # ------------------------------------------------------------------ misc reference helpers
+    def gen_weights(self, sinogram, weight_type):
+        """tomography_model.py:1727-1764."""
+        s = self._dev(sinogram)
+        if weight_type == 'unweighted':
+            return torch.ones_like(s)
+        if weight_type == 'transmission':
+            return torch.exp(-s)
+        if weight_type == 'transmission_root':
+            return torch.exp(-s / 2)
+        if weight_type == 'emission':
+            return 1.0 / (torch.abs(s) + 0.1)
+        raise Exception('gen_weights: undefined weight_type {}'.format(weight_type))
+
+    def scale_recon_shape(self, row_scale=1.0, col_scale=1.0, slice_scale=1.0):
+        old_rows, old_cols, old_slices = self.get_params('recon_shape')
+        new = (int(old_rows * row_scale), int(old_cols * col_scale), int(old_slices * slice_scale))
+        self.set_params(recon_shape=new)
+        return new[0] - old_rows, new[1] - old_cols, new[2] - old_slices
+
+
+def _to_numpy(x):
+    if isinstance(x, torch.Tensor):
+        return x.detach().cpu().numpy()
+    return np.asarray(x)

@@ -1,0 +1,55 @@
+"""Synthetic phantoms and sinograms for the benchmark workloads.
+
+The workloads are seeded synthetic stand-ins (there is no public dataset behind the benchmark): volumes of
+axis-aligned ellipsoids with centres uniform in the inner 70% of the volume, semi-axes uniform in [5, 40]
+voxels and densities uniform in [0.1, 1], summed where they overlap (the same construction as the
+reference's ``add_ellipsoid``, ``utilities.py:856-895``, without rotation).  Generation runs with torch on
+whatever device the caller names (the CPU in tests, the GPU for the large configurations).
+"""
+import numpy as np
+import torch
+
+
+def gen_ellipsoid_phantom(recon_shape, num_ellipsoids, seed, device='cpu', dtype=torch.float32):
+    rng = np.random.default_rng(seed)
+    nr, nc, ns = recon_shape
+    shape = np.array([nr, nc, ns], dtype=np.float64)
+    centres = rng.uniform(0.15, 0.85, size=(num_ellipsoids, 3)) * (shape - 1)
+    axes = rng.uniform(5.0, 40.0, size=(num_ellipsoids, 3))
+    dens = rng.uniform(0.1, 1.0, size=num_ellipsoids)
+    out = torch.zeros((nr, nc, ns), dtype=dtype, device=device)
+    i = torch.arange(nr, device=device, dtype=torch.float64)[:, None, None]
+    j = torch.arange(nc, device=device, dtype=torch.float64)[None, :, None]
+    k = torch.arange(ns, device=device, dtype=torch.float64)[None, None, :]
+    for c, a, d in zip(centres, axes, dens):
+        # bounding box to keep large volumes cheap
+        lo = np.maximum(np.floor(c - a), 0).astype(int)
+        hi = np.minimum(np.ceil(c + a) + 1, shape).astype(int)
+        if np.any(hi <= lo):
+            continue
+        ii, jj, kk = i[lo[0]:hi[0]], j[:, lo[1]:hi[1]], k[:, :, lo[2]:hi[2]]
+        inside = ((ii - c[0]) / a[0]) ** 2 + ((jj - c[1]) / a[1]) ** 2 + ((kk - c[2]) / a[2]) ** 2 <= 1.0
+        out[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] += float(d) * inside.to(dtype)
+    return out
+
+
+def add_noise(sinogram, rel_sigma, seed):
+    """sinogram + N(0, (rel_sigma * max|sinogram|)^2), seeded."""
+    g = torch.Generator(device=sinogram.device).manual_seed(int(seed) + 1000)
+    sigma = float(rel_sigma) * float(sinogram.abs().max())
+    return sinogram + sigma * torch.randn(sinogram.shape, generator=g, device=sinogram.device, dtype=sinogram.dtype)
+
+
+def uniform_angles(num_views, full_circle=False):
+    stop = 2 * np.pi if full_circle else np.pi
+    return np.linspace(0, stop, num_views, endpoint=False).astype(np.float32)
+
+
+def batched_scan_shapes(num_scans=24):
+    """Per-scan (views, det_rows, det_channels) of the uneven parallel-beam batch: scan i draws from seed i
+    views U{60..720}, det_rows U{8..64}, det_channels U{96..512}."""
+    shapes = []
+    for i in range(num_scans):
+        rng = np.random.default_rng(i)
+        shapes.append((int(rng.integers(60, 721)), int(rng.integers(8, 65)), int(rng.integers(96, 513))))
+    return shapes

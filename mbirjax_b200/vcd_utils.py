@@ -1,0 +1,60 @@
+"""Pixel partitions, partition sequences and the region-of-reconstruction mask (host side, NumPy).
+
+Same contract as ``vcd_utils.py:66-124, 176-223, 284-318`` of the reference, including its use of the legacy
+global ``np.random`` stream (``permutation``, then ``choice(..., replace=False)``), so that a run seeded with
+``np.random.seed`` draws the same partitions and subset orders as the reference does.
+"""
+import warnings
+
+import numpy as np
+
+
+def get_2d_ror_mask(recon_shape, *, crop_radius_pixels=0, crop_radius_fraction=0.0):
+    """Boolean (rows, cols) disk inscribed on the longer edge, optionally shrunk (vcd_utils.py:66-102)."""
+    if crop_radius_pixels != 0 and crop_radius_fraction != 0.0:
+        raise ValueError('Only one of crop_radius_pixels and crop_radius_fraction can be nonzero.')
+    num_rows, num_cols = recon_shape[:2]
+    row_center, col_center = (num_rows - 1) / 2, (num_cols - 1) / 2
+    radius = max(row_center, col_center)
+    crop = max(int(radius * crop_radius_fraction), crop_radius_pixels, 0)
+    radius -= crop
+    cols = np.arange(num_cols) - col_center
+    rows = np.arange(num_rows) - row_center
+    return cols[None, :] ** 2 + rows[:, None] ** 2 <= radius ** 2
+
+
+def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True):
+    """(num_subsets, ceil(N/num_subsets)) int32 array of sorted flat pixel indices (vcd_utils.py:176-223)."""
+    num_rows, num_cols = recon_shape[:2]
+    indices = np.arange(num_rows * num_cols, dtype=np.int32)
+    if use_ror_mask:
+        indices = indices[get_2d_ror_mask(recon_shape).flatten()]
+    if num_subsets > len(indices):
+        num_subsets = len(indices)
+        warnings.warn('\nThe number of partition subsets is greater than the number of pixels in the region of '
+                      'reconstruction.  \nReducing the number of subsets to equal the number of indices.')
+    per_subset = int(np.ceil(len(indices) / num_subsets))
+    num_extra = num_subsets * per_subset - len(indices)
+    indices = np.random.permutation(indices)
+    num_non_final = (num_subsets - 1) * per_subset
+    extra = np.random.choice(indices[:num_non_final], size=num_extra, replace=False)
+    indices = np.concatenate((indices, extra)).reshape(num_subsets, -1)
+    return np.sort(indices, axis=1).astype(np.int32)
+
+
+def gen_set_of_pixel_partitions(recon_shape, granularity, output_device=None, use_ror_mask=True):
+    """One partition per entry of granularity (vcd_utils.py:105-124); output_device is accepted and ignored."""
+    return [gen_pixel_partition(recon_shape, k, use_ror_mask=use_ror_mask) for k in granularity]
+
+
+def gen_partition_sequence(partition_sequence, max_iterations):
+    """Extend (or cut) the sequence to max_iterations by repeating its last entry (vcd_utils.py:284-307)."""
+    seq = np.array(partition_sequence)
+    if max_iterations > seq.size:
+        return np.concatenate((seq, np.full(max_iterations - seq.size, seq[-1])))
+    return seq[:max_iterations]
+
+
+def gen_full_indices(recon_shape, use_ror_mask=True):
+    """All pixels of the region of reconstruction, sorted (vcd_utils.py:310-318)."""
+    return gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask)[0]

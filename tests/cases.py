@@ -1,0 +1,49 @@
+"""Geometry cases shared by the CPU and GPU tests: each builds a mbirjax_b200 model and the matching
+oracle geometry from the same arguments."""
+import numpy as np
+
+import mbirjax_b200 as mb
+import oracle as O
+
+
+def angles_for(kind, num_views, num_det_channels, sdd):
+    """Angle set of the reference's projector tests (tests/test_projectors.py:45-52)."""
+    cone_angle = 2 * np.arctan2(num_det_channels / 2, sdd) if kind == 'cone' else 0.0
+    start, end = -(np.pi + cone_angle) / 2, (np.pi + cone_angle) / 2
+    return np.linspace(start, end, num_views, endpoint=False).astype(np.float32)
+
+
+def make_case(kind, views=16, rows=8, channels=32, sdd_factor=4.0, sid_factor=None, **params):
+    """Returns (model, oracle_geometry).  params are set on the model before the oracle geometry is derived."""
+    sdd = sdd_factor * channels
+    sid = sdd if sid_factor is None else sid_factor * channels
+    ang = angles_for(kind, views, channels, sdd)
+    if kind == 'parallel':
+        model = mb.ParallelBeamModel((views, rows, channels), ang)
+    else:
+        model = mb.ConeBeamModel((views, rows, channels), ang, source_detector_dist=sdd, source_iso_dist=sid)
+    if params:
+        model.set_params(**params)
+    return model, oracle_geometry(model)
+
+
+def oracle_geometry(model):
+    sino_shape, recon_shape = model.get_params(['sinogram_shape', 'recon_shape'])
+    ang = np.asarray(model.get_params('angles'), dtype=np.float32)
+    kw = dict(delta_det_channel=model.get_params('delta_det_channel'), delta_det_row=model.get_params('delta_det_row'),
+              det_channel_offset=model.get_params('det_channel_offset'),
+              det_row_offset=model.get_params('det_row_offset'), delta_voxel=model.get_params('delta_voxel'),
+              recon_shape=recon_shape)
+    if isinstance(model, mb.ConeBeamModel):
+        g = O.cone_geometry(sino_shape, ang, model.get_params('source_detector_dist'),
+                            model.get_params('source_iso_dist'), recon_slice_offset=model.get_params('recon_slice_offset'),
+                            **kw)
+    else:
+        g = O.parallel_geometry(sino_shape, ang, **kw)
+    return g
+
+
+def rel_l2(a, b):
+    a = np.asarray(a, dtype=np.float64)
+    b = np.asarray(b, dtype=np.float64)
+    return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))

@@ -1,0 +1,125 @@
+"""CPU tests of the host side: the C-ABI library loads and exports every declared symbol, argument validation
+returns error codes without touching a GPU, and the host logic (parameters, geometry radii, partitions,
+auto-regularisation) matches the oracle."""
+import ctypes
+import os
+import re
+
+import numpy as np
+import pytest
+
+import mbirjax_b200 as mb
+from mbirjax_b200 import _capi
+import oracle as O
+from cases import make_case, oracle_geometry
+
+ROOT = os.path.dirname(os.path.dirname(os.path.abspath(__file__)))
+
+
+def _declared_symbols():
+    text = open(os.path.join(ROOT, 'include', 'mbirjax_b200.h')).read()
+    return sorted(set(re.findall(r'^MBX_API [^;(]*?\b(mbx_\w+)\s*\(', text, flags=re.M)))
+
+
+def test_library_exports_every_declared_symbol():
+    lib = _capi.load_library()
+    declared = _declared_symbols()
+    assert len(declared) >= 14
+    for name in declared:
+        assert hasattr(lib, name), name
+    assert sorted(_capi.exported_symbols()) == declared
+    assert 'sm_100a' in _capi.version()
+
+
+def test_invalid_arguments_return_error_codes():
+    lib = _capi.load_library()
+    g = _capi.MbxGeom()
+    assert lib.mbx_sparse_forward_project(ctypes.byref(g), None, None, 0, None, 1, None, None, 0, None) == -1
+    assert lib.mbx_sparse_back_project(None, None, None, None, 0, None, 1, 1, 1.0, None, None, 0, None) == -1
+    assert lib.mbx_direct_filter(None, None, None, None) == -1
+    assert lib.mbx_error_string(-4).decode().startswith('workspace')
+    g.kind, g.num_views, g.num_det_rows, g.num_det_channels = 0, 4, 2, 8
+    g.num_recon_rows = g.num_recon_cols = 8
+    g.num_recon_slices = 2
+    g.delta_det_channel = g.delta_det_row = g.delta_voxel = 1.0
+    g.psf_radius = 7  # above MBX_MAX_PSF_RADIUS
+    g.angles = 1
+    assert lib.mbx_sparse_forward_project(ctypes.byref(g), None, None, 0, None, 1, 1, None, 0, None) == -2
+
+
+def test_compute_without_gpu_fails_loudly(monkeypatch):
+    import torch
+    if torch.cuda.is_available():
+        pytest.skip('GPU present')
+    model, _ = make_case('parallel')
+    with pytest.raises(mb.MbxError):
+        model.forward_project(np.zeros(model.get_params('recon_shape'), dtype=np.float32))
+
+
+@pytest.mark.parametrize('kind,kw', [('parallel', {}), ('cone', {}), ('cone', {'sid_factor': 2.0}),
+                                     ('parallel', {'delta_voxel': 2.5}), ('cone', {'delta_voxel': 3.0})])
+def test_geometry_matches_oracle(kind, kw):
+    model, geom = make_case(kind, views=8, rows=10, channels=40, **kw)
+    gp = model.get_geometry_parameters()
+    assert gp.psf_radius == geom.psf_radius
+    if kind == 'cone':
+        assert gp.bp_psf_radius == geom.bp_psf_radius
+        assert model.get_magnification() == pytest.approx(geom.magnification)
+    # default recon sizes (parallel_beam.py:125-136, cone_beam.py:174-187)
+    m2, g2 = make_case(kind, views=8, rows=10, channels=40)
+    assert tuple(m2.get_params('recon_shape')) == tuple(g2.recon_shape)
+
+
+def test_set_params_semantics():
+    model, _ = make_case('parallel')
+    with pytest.raises(ValueError):
+        model.set_params(not_a_param=1)
+    with pytest.warns(UserWarning):
+        model.set_params(sigma_x=0.5)
+    assert model.get_params('auto_regularize_flag') is False
+    with pytest.warns(UserWarning):
+        model.set_params(sharpness=0.0)
+    assert model.get_params('auto_regularize_flag') is True
+    with pytest.raises(ValueError):
+        model.set_params(recon_shape=(32, 32, 5))  # slices must equal det rows for parallel beam
+
+
+def test_partitions_reproduce_oracle_stream():
+    shape = (37, 37, 4)
+    np.random.seed(11)
+    a = mb.gen_set_of_pixel_partitions(shape, [1, 4, 7])
+    a_perm = np.random.permutation(4)
+    np.random.seed(11)
+    b = O.gen_set_of_pixel_partitions(shape, [1, 4, 7])
+    b_perm = np.random.permutation(4)
+    for x, y in zip(a, b):
+        np.testing.assert_array_equal(x, y)
+    np.testing.assert_array_equal(a_perm, b_perm)
+    np.testing.assert_array_equal(mb.get_2d_ror_mask(shape), O.get_2d_ror_mask(shape))
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_auto_regularization_matches_oracle(kind):
+    model, geom = make_case(kind, views=40, rows=6, channels=32)
+    rng = np.random.default_rng(5)
+    sino = rng.random(geom.sinogram_shape).astype(np.float32)
+    sino[:, :, :4] = 0
+    w = rng.random(geom.sinogram_shape).astype(np.float32)
+    model.set_params(sharpness=0.0, snr_db=30.0)
+    reg = model.auto_set_regularization_params(sino, weights=w)
+    sy, sx, sp = O.auto_regularization(geom, sino, w, snr_db=30.0, sharpness=0.0)
+    assert reg['sigma_y'] == pytest.approx(sy, rel=1e-7)
+    assert reg['sigma_x'] == pytest.approx(sx, rel=1e-7)
+    assert reg['sigma_prox'] == pytest.approx(sp, rel=1e-7)
+
+
+def test_qggmrf_b_weights():
+    assert mb.get_b_from_nbr_wts([1.0, 2.0, 3.0]) == pytest.approx(O.get_b_from_nbr_wts([1.0, 2.0, 3.0]))
+
+
+def test_batched_scan_shapes_are_in_range():
+    from mbirjax_b200.utilities import batched_scan_shapes
+    shapes = batched_scan_shapes()
+    assert len(shapes) == 24
+    for v, r, c in shapes:
+        assert 60 <= v <= 720 and 8 <= r <= 64 and 96 <= c <= 512

@@ -1,0 +1,130 @@
+"""CPU tests of the oracle: pinned against the reference's golden vectors and its structural tests
+(reference tests/test_qggmrf.py:23-172, tests/test_projectors.py:152-303, tests/test_fbp_fdk.py)."""
+import json
+import os
+
+import numpy as np
+import pytest
+
+import oracle as O
+
+GOLDEN = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'qggmrf_golden.json')
+
+
+def _golden():
+    with open(GOLDEN) as f:
+        return json.load(f)
+
+
+def test_qggmrf_golden_vectors():
+    g = _golden()
+    params = (O.get_b_from_nbr_wts([1, 1, 1]), g['sigma_x'], g['p'], g['q'], g['T'])
+    flat = np.array(g['flat_recon'])
+    grad, hess = O.qggmrf_gradient_and_hessian_at_indices(flat, tuple(g['recon_shape']), np.arange(flat.shape[0]),
+                                                          params)
+    # np.allclose defaults, as the reference test (tests/test_qggmrf.py:133-134)
+    assert np.allclose(grad, g['grad_ref'])
+    assert np.allclose(hess, g['hess_ref'])
+
+
+def test_b_tilde_definition():
+    rng = np.random.default_rng(3)
+    p = rng.random() + 1
+    q = p - 0.9 * rng.random()
+    T = 0.5 + rng.random()
+    sigma_x = 0.1 + rng.random()
+    delta = 0.1 + rng.random(10)
+    b2 = O.get_2_b_tilde(delta, 1.0, ((1,) * 6, sigma_x, p, q, T), dt=np.float64)
+    assert np.allclose(b2 / 2, O.b_tilde_by_definition(delta, sigma_x, p, q, T))
+
+
+def test_qggmrf_loss_gradient_finite_difference():
+    # tests/test_qggmrf.py:136-172 shape of test, in float64
+    p, q, T, sigma_x = 2.0413, 1.124, 1.46, 0.789
+    params = (O.get_b_from_nbr_wts([1, 1, 1]), sigma_x, p, q, T)
+    rng = np.random.default_rng(0)
+    x = rng.random((3, 3, 3))
+    d = rng.random((3, 3, 3))
+    eps = 1e-7
+    fd = (O.qggmrf_loss(x + eps * d, params) - O.qggmrf_loss(x, params)) / eps
+    g_surr, h_surr = O.qggmrf_gradient_and_hessian_at_indices(x.reshape(9, 3), (3, 3, 3), np.arange(9), params,
+                                                              dt=np.float64)
+    assert np.allclose(fd, np.sum(g_surr.reshape(x.shape) * d), rtol=1e-3)
+    g_loss = O.qggmrf_loss_grad(x, params)
+    assert np.allclose(fd, np.sum(g_loss * d), rtol=1e-5)
+    g_ref, h_ref = O.compute_qggmrf_grad_and_hessian(x, params)
+    assert np.allclose(h_ref, h_surr.reshape(x.shape))
+    assert np.allclose(g_ref, g_surr.reshape(x.shape))
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_oracle_adjoint_exact_in_float64(kind):
+    from cases import make_case
+    _, geom = make_case(kind, views=12, rows=6, channels=24)
+    nr, nc, ns = geom.recon_shape
+    rng = np.random.default_rng(1)
+    idx = np.arange(nr * nc)
+    x = rng.random((nr * nc, ns))
+    y = rng.random(geom.sinogram_shape)
+    ax = O.sparse_forward_project(geom, x, idx, dtype=np.float64)
+    aty = O.sparse_back_project(geom, y, idx, dtype=np.float64)
+    assert abs(np.sum(ax * y) - np.sum(aty * x)) <= 1e-12 * abs(np.sum(ax * y))
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_oracle_hessian_finite_difference(kind):
+    # tests/test_projectors.py:264-303
+    from cases import make_case
+    _, geom = make_case(kind, views=10, rows=6, channels=20)
+    nr, nc, ns = geom.recon_shape
+    hess = O.compute_hessian_diagonal(geom, dtype=np.float64)
+    i, j, k = nr // 3, nc // 2, ns // 2
+    x = np.zeros((nr * nc, ns))
+    x[i * nc + j, k] = 0.01
+    idx = np.arange(nr * nc)
+    atax = O.sparse_back_project(geom, O.sparse_forward_project(geom, x, idx, dtype=np.float64), idx,
+                                 dtype=np.float64).reshape(nr, nc, ns)
+    assert np.isclose(hess[i, j, k], atax[i, j, k] / 0.01)
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_oracle_view_batching(kind):
+    # tests/test_projectors.py:152-198; exact here since the oracle rounds consistently
+    from cases import make_case
+    _, geom = make_case(kind, views=12, rows=6, channels=24)
+    nr, nc, ns = geom.recon_shape
+    np.random.seed(2)
+    idx = O.gen_full_indices(geom.recon_shape)
+    x = np.random.rand(len(idx), ns).astype(np.float32)
+    full = O.sparse_forward_project(geom, x, idx)
+    for j in range(3):
+        views = np.arange(j, 12, 3)
+        np.testing.assert_array_equal(O.sparse_forward_project(geom, x, idx, views), full[views])
+    bp = O.sparse_back_project(geom, full, idx)
+    parts = sum(O.sparse_back_project(geom, full, idx, np.arange(j, 12, 3)) for j in range(3))
+    assert np.abs(parts - bp).max() <= 1e-5 * np.abs(bp).max()
+
+
+def test_oracle_partitions_match_reference_contract():
+    np.random.seed(0)
+    shape = (20, 20, 3)
+    p = O.gen_pixel_partition(shape, 7)
+    mask = O.get_2d_ror_mask(shape).flatten()
+    n = int(mask.sum())
+    assert p.shape == (7, int(np.ceil(n / 7)))
+    assert np.all(np.diff(p, axis=1) > 0)                       # sorted, no duplicates inside a subset
+    assert set(np.unique(p)) == set(np.flatnonzero(mask))       # covers the ROR exactly
+    assert list(O.gen_partition_sequence([0, 2, 4], 6)) == [0, 2, 4, 4, 4, 4]
+
+
+def test_oracle_fbp_recovers_phantom():
+    # sanity floor in the spirit of tests/test_fbp_fdk.py: FBP of a forward projection resembles the phantom
+    from cases import make_case
+    _, geom = make_case('parallel', views=64, rows=2, channels=48)
+    nr, nc, ns = geom.recon_shape
+    ph = np.zeros(geom.recon_shape, dtype=np.float32)
+    ph[16:32, 14:30, :] = 1.0
+    sino = O.forward_project(geom, ph)
+    rec = O.back_project(geom, O.fbp_filter(sino, geom.delta_voxel))
+    inner = (slice(18, 30), slice(16, 28))
+    assert abs(float(np.mean(rec[inner])) - 1.0) < 0.1

@@ -1,0 +1,184 @@
+"""GPU parity of the sparse projectors (through the C ABI) against the oracle.
+
+Bars: forward/back projection within 1e-5 relative L2 of the float32 oracle; adjointness <y, Ax> = <A^T y, x>
+within 1e-5 relative to the float64 oracle's value; view subsets and coefficient power 2 likewise.
+Test shapes follow the reference's tests/test_projectors.py (adjoint :200-262, Hessian :264-303, view
+batching :152-198)."""
+import numpy as np
+import pytest
+import torch
+
+import mbirjax_b200 as mb
+from mbirjax_b200 import _capi
+import oracle as O
+from cases import make_case, oracle_geometry, rel_l2
+
+pytestmark = pytest.mark.gpu
+
+TOL = 1e-5
+
+CASES = [
+    ('parallel', dict(views=16, rows=8, channels=32)),
+    ('parallel', dict(views=9, rows=5, channels=33)),                       # odd channels, ragged tiles
+    ('parallel', dict(views=12, rows=6, channels=40, delta_voxel=3.0, delta_det_row=3.0)),  # psf radius 2
+    ('parallel', dict(views=20, rows=3, channels=24, det_channel_offset=1.3)),
+    ('cone', dict(views=16, rows=8, channels=32)),
+    ('cone', dict(views=16, rows=12, channels=32, sid_factor=2.0)),         # magnification 2
+    ('cone', dict(views=10, rows=7, channels=27, det_row_offset=0.7, det_channel_offset=-1.1,
+                  recon_slice_offset=0.4)),
+    ('cone', dict(views=12, rows=10, channels=30, delta_voxel=2.2)),        # psf radius 2
+]
+
+
+def _ids():
+    return ['%s-%d' % (k, i) for i, (k, _) in enumerate(CASES)]
+
+
+def _case(kind, kw):
+    kw = dict(kw)
+    params = {k: kw.pop(k) for k in list(kw) if k in ('delta_voxel', 'delta_det_row', 'det_channel_offset',
+                                                     'det_row_offset', 'recon_slice_offset')}
+    model, _ = make_case(kind, **kw)
+    if params:
+        model.set_params(no_warning=True, **params)
+        if 'delta_voxel' in params:  # re-derive the recon size for the new voxel size, as a user would
+            model.auto_set_recon_size(model.get_params('sinogram_shape'), no_warning=True)
+    return model, oracle_geometry(model)
+
+
+@pytest.mark.parametrize('kind,kw', CASES, ids=_ids())
+def test_forward_back_parity(cuda, kind, kw):
+    model, geom = _case(kind, kw)
+    nr, nc, ns = geom.recon_shape
+    np.random.seed(7)
+    idx = O.gen_full_indices(geom.recon_shape)
+    rng = np.random.default_rng(1)
+    x = rng.random((len(idx), ns)).astype(np.float32)
+    y = rng.random(geom.sinogram_shape).astype(np.float32)
+
+    ax_gpu = model.sparse_forward_project(x, idx).cpu().numpy()
+    ax_ref = O.sparse_forward_project(geom, x, idx)
+    assert rel_l2(ax_gpu, ax_ref) <= TOL
+
+    aty_gpu = model.sparse_back_project(y, idx).cpu().numpy()
+    aty_ref = O.sparse_back_project(geom, y, idx)
+    assert rel_l2(aty_gpu, aty_ref) <= TOL
+
+    h_gpu = model.sparse_back_project(y, idx, coeff_power=2).cpu().numpy()
+    h_ref = O.sparse_back_project(geom, y, idx, coeff_power=2)
+    assert rel_l2(h_gpu, h_ref) <= TOL
+
+    # adjointness against the float64 oracle
+    ref64 = np.sum(O.sparse_forward_project(geom, x, idx, dtype=np.float64) * y)
+    lhs = np.sum(ax_gpu.astype(np.float64) * y)
+    rhs = np.sum(aty_gpu.astype(np.float64) * x)
+    assert abs(lhs - ref64) <= TOL * abs(ref64)
+    assert abs(rhs - ref64) <= TOL * abs(ref64)
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_view_subsets_and_weights(cuda, kind):
+    model, geom = make_case(kind, views=15, rows=6, channels=28)
+    nr, nc, ns = geom.recon_shape
+    rng = np.random.default_rng(3)
+    idx = rng.permutation(nr * nc)[: nr * nc // 3].astype(np.int32)       # unsorted sparse subset
+    x = rng.standard_normal((len(idx), ns)).astype(np.float32)
+    y = rng.standard_normal(geom.sinogram_shape).astype(np.float32)
+    w = rng.random(geom.sinogram_shape).astype(np.float32)
+    views = np.array([14, 0, 7, 3, 3], dtype=np.int32)
+    fp = model.sparse_forward_project(x, idx, view_indices=views).cpu().numpy()
+    assert rel_l2(fp, O.sparse_forward_project(geom, x, idx, views)) <= TOL
+    bp = model.sparse_back_project(y, idx, view_indices=views).cpu().numpy()
+    assert rel_l2(bp, O.sparse_back_project(geom, y, idx, views)) <= TOL
+    # fused weights: A^T (w * y)
+    g = model._geometry()
+    bw = _capi.back_project(g, torch.as_tensor(y, device='cuda'), torch.as_tensor(idx, device='cuda'),
+                            weights=torch.as_tensor(w, device='cuda')).cpu().numpy()
+    assert rel_l2(bw, O.sparse_back_project(geom, w * y, idx)) <= TOL
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_view_batching_consistency(cuda, kind):
+    # tests/test_projectors.py:152-198: interleaved view subsets reassemble the full projection
+    model, geom = make_case(kind, views=24, rows=8, channels=32)
+    ns = geom.recon_shape[2]
+    np.random.seed(1)
+    idx = mb.gen_full_indices(geom.recon_shape)
+    x = np.random.rand(len(idx), ns).astype(np.float32)
+    full = model.sparse_forward_project(x, idx).cpu().numpy()
+    y = full
+    bp = model.sparse_back_project(y, idx).cpu().numpy()
+    parts = np.zeros_like(bp)
+    for j in range(5):
+        v = np.arange(j, 24, 5)
+        np.testing.assert_allclose(model.sparse_forward_project(x, idx, view_indices=v).cpu().numpy(), full[v],
+                                   rtol=1e-6, atol=1e-6 * np.abs(full).max())
+        parts += model.sparse_back_project(y, idx, view_indices=v).cpu().numpy()
+    assert np.abs(parts - bp).max() <= 1e-5 * np.abs(bp).max()
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_hessian_diagonal(cuda, kind):
+    model, geom = make_case(kind, views=12, rows=6, channels=24)
+    h = model.compute_hessian_diagonal().cpu().numpy()
+    assert rel_l2(h, O.compute_hessian_diagonal(geom)) <= TOL
+    w = np.random.default_rng(0).random(geom.sinogram_shape).astype(np.float32)
+    hw = model.compute_hessian_diagonal(weights=w).cpu().numpy()
+    assert rel_l2(hw, O.compute_hessian_diagonal(geom, w)) <= TOL
+    # finite-difference check of the Hessian (tests/test_projectors.py:264-303)
+    nr, nc, ns = geom.recon_shape
+    i, j, k = nr // 3, nc // 2, ns // 2
+    xx = np.zeros((nr * nc, ns), dtype=np.float32)
+    xx[i * nc + j, k] = 0.01
+    idx = np.arange(nr * nc, dtype=np.int32)
+    atax = model.sparse_back_project(model.sparse_forward_project(xx, idx), idx).cpu().numpy().reshape(nr, nc, ns)
+    assert np.isclose(h[i, j, k], atax[i, j, k] / 0.01, rtol=1e-5)
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_full_projection_reference_test_geometry(cuda, kind):
+    # the reference's projector-test geometry: 64 views, 40 rows, 128 channels, cone sdd = sid = 512
+    model, geom = make_case(kind, views=64, rows=40, channels=128)
+    rng = np.random.default_rng(2)
+    recon = rng.random(geom.recon_shape).astype(np.float32)
+    np.random.seed(5)
+    sino = model.forward_project(recon).cpu().numpy()
+    np.random.seed(5)
+    sino_ref = O.forward_project(geom, recon)
+    assert rel_l2(sino, sino_ref) <= TOL
+    bp = model.back_project(sino).cpu().numpy()
+    assert rel_l2(bp, O.back_project(geom, sino_ref)) <= TOL
+
+
+def test_edge_cases(cuda):
+    model, geom = make_case('parallel', views=6, rows=4, channels=16)
+    ns = geom.recon_shape[2]
+    # empty pixel set: the forward projection is all zeros, the back projection empty
+    empty = np.zeros(0, dtype=np.int32)
+    fp = model.sparse_forward_project(np.zeros((0, ns), np.float32), empty).cpu().numpy()
+    assert fp.shape == geom.sinogram_shape and not fp.any()
+    assert model.sparse_back_project(np.ones(geom.sinogram_shape, np.float32), empty).shape == (0, ns)
+    # duplicated pixels accumulate
+    idx = np.array([5, 5, 9], dtype=np.int32)
+    x = np.ones((3, ns), np.float32)
+    np.testing.assert_allclose(model.sparse_forward_project(x, idx).cpu().numpy(),
+                               O.sparse_forward_project(geom, x, idx), rtol=1e-5, atol=1e-6)
+    # shape errors raise before any launch
+    with pytest.raises(ValueError):
+        model.sparse_forward_project(np.zeros((2, ns + 1), np.float32), idx[:2])
+    # an out-of-range pixel index is skipped by the kernels' own bounds checks and reported
+    mb._capi.get_device_error()
+    bad = np.array([3, 10 ** 6], dtype=np.int32)
+    out = model.sparse_forward_project(np.ones((2, ns), np.float32), bad).cpu().numpy()
+    assert mb._capi.get_device_error() & 1
+    np.testing.assert_allclose(out, O.sparse_forward_project(geom, np.ones((1, ns), np.float32), bad[:1]),
+                               rtol=1e-5, atol=1e-6)
+
+
+def test_determinism_of_back_projection(cuda):
+    model, geom = make_case('cone', views=16, rows=8, channels=32)
+    idx = np.arange(geom.recon_shape[0] * geom.recon_shape[1], dtype=np.int32)
+    y = np.random.default_rng(0).random(geom.sinogram_shape).astype(np.float32)
+    a = model.sparse_back_project(y, idx).cpu().numpy()
+    b = model.sparse_back_project(y, idx).cpu().numpy()
+    np.testing.assert_array_equal(a, b)   # no float atomics on the back-projection side
