@@ -1,0 +1,390 @@
+#!/usr/bin/env python
+"""Benchmark of the MBIR hot path on B200.
+
+Workload (default ``--workload cone``): plain cone-beam VCD on one scan -- sinogram 256 views x 128 rows x 256
+channels (views uniform on [0, 2pi)), source_detector_dist = source_iso_dist = 1024, unit detector pitch, recon
+256x256x128 (auto size), forward-projected from 20 seeded random ellipsoids (seed 1) with 1% Gaussian noise,
+qGGMRF p=2, q=1.2, T=1, sharpness 0, 4 pixel subsets, 20 VCD iterations with FDK initialisation.
+A step is one full ``ConeBeamModel.recon`` of that scan; the value is recons/s.
+
+Synthetic data stands in for measured scans (the reference publishes no benchmark dataset).
+Timing: W untimed warm-up steps, then exactly K steps between barriers + device synchronisations, timed with
+CUDA events on the launching stream; max over ranks.  The recon working set (about 70 MB) fits in L2, so L2 is
+flushed (a 256 MB write) before every step, inside the timed region.  SM clocks and throttle reasons are
+sampled with nvidia-smi during the timed region.  ``e2e`` repeats the measurement through the public API with
+the sinogram in pinned host memory and the recon copied back each step.  ``roofline`` times the dominant
+kernels (one VCD subset's back projection and forward projection) with CUDA events and divides their
+algorithmic bytes by the measured HBM copy bandwidth.  ``cpu_baseline`` times the oracle's restatement of the
+reference arithmetic on all host cores for one subset update and scales it to one recon.
+
+``--impl reference`` times the reference arithmetic (the oracle port: JAX is not installable offline, so the
+reference's own JAX CPU path cannot run) on the host cores on the same workload and metric.
+Multi-GPU (torchrun, one process per GPU): independent replicas, no collective on the data path.
+"""
+import argparse
+import json
+import os
+import re
+import statistics
+import subprocess
+import sys
+import tempfile
+import time
+
+import numpy as np
+
+ROOT = os.path.dirname(os.path.abspath(__file__))
+if ROOT not in sys.path:
+    sys.path.insert(0, ROOT)
+
+METRIC = 'batched vs plain recons/s at 1e-4 NRMSE; proj HBM GB/s; autograd/fwd time'
+CONE = dict(views=256, rows=128, channels=256, sdd=1024.0, sid=1024.0, ellipsoids=20, seed=1, subsets=4,
+            iterations=20)
+
+
+def parse_args():
+    ap = argparse.ArgumentParser()
+    ap.add_argument('--gpus', type=int, default=1)
+    ap.add_argument('--steps', type=int, default=5)
+    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--impl', default='mbirjax_b200', choices=['mbirjax_b200', 'reference'])
+    ap.add_argument('--workload', default='cone', choices=['cone'])
+    ap.add_argument('--no-e2e', action='store_true')
+    ap.add_argument('--no-cpu-baseline', action='store_true')
+    return ap.parse_args()
+
+
+# ----------------------------------------------------------------------------------------------- helpers
+def load_peaks():
+    try:
+        with open(os.path.join(ROOT, 'MEASURED_PEAKS.json')) as f:
+            d = json.load(f)
+        return float(d['hbm_gbs']), 'measured'
+    except Exception:
+        return 6650.0, 'fallback'
+
+
+class ClockSampler:
+    """nvidia-smi sampling of SM clock and throttle reasons while the timed region runs."""
+
+    FIELDS = ('index,clocks.sm,clocks.max.sm,power.draw,clocks_event_reasons.active,'
+              'clocks_event_reasons.hw_slowdown,clocks_event_reasons.hw_thermal_slowdown,'
+              'clocks_event_reasons.sw_thermal_slowdown,clocks_event_reasons.sw_power_cap')
+
+    def __init__(self, gpu_index):
+        self.gpu = gpu_index
+        self.proc = None
+        self.path = None
+
+    def start(self):
+        fd, self.path = tempfile.mkstemp(suffix='.csv')
+        os.close(fd)
+        try:
+            self.proc = subprocess.Popen(['nvidia-smi', '-i', str(self.gpu), '--query-gpu=' + self.FIELDS,
+                                          '--format=csv,noheader,nounits', '-lms', '200'],
+                                         stdout=open(self.path, 'w'), stderr=subprocess.DEVNULL)
+        except Exception:
+            self.proc = None
+
+    def stop(self):
+        if self.proc is None:
+            return {'sm_mhz': None, 'sm_max_mhz': None, 'reasons': ['nvidia-smi unavailable']}
+        self.proc.terminate()
+        try:
+            self.proc.wait(timeout=5)
+        except Exception:
+            self.proc.kill()
+        sm, smax, reasons = [], None, set()
+        names = ['hw_slowdown', 'hw_thermal_slowdown', 'sw_thermal_slowdown', 'sw_power_cap']
+        for line in open(self.path):
+            parts = [p.strip() for p in line.split(',')]
+            if len(parts) < 9:
+                continue
+            try:
+                sm.append(float(parts[1]))
+                smax = float(parts[2])
+            except ValueError:
+                continue
+            for name, val in zip(names, parts[5:9]):
+                if val.lower() == 'active':
+                    reasons.add(name)
+        os.unlink(self.path)
+        return {'sm_mhz': statistics.median(sm) if sm else None, 'sm_max_mhz': smax, 'reasons': sorted(reasons),
+                'samples': len(sm)}
+
+
+def dist_setup(n_gpus):
+    import torch
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    local = int(os.environ.get('LOCAL_RANK', '0'))
+    if world > 1:
+        import datetime
+        import torch.distributed as dist
+        torch.cuda.set_device(local)
+        dist.init_process_group('nccl', timeout=datetime.timedelta(seconds=300),
+                                device_id=torch.device('cuda', local))
+    elif torch.cuda.is_available():
+        torch.cuda.set_device(0)
+    return world, rank, local
+
+
+def barrier(world):
+    if world > 1:
+        import torch.distributed as dist
+        dist.barrier()
+
+
+def max_over_ranks(value, world):
+    if world == 1:
+        return value
+    import torch
+    import torch.distributed as dist
+    t = torch.tensor([value], dtype=torch.float64, device='cuda')
+    dist.all_reduce(t, op=dist.ReduceOp.MAX)
+    return float(t.item())
+
+
+# ----------------------------------------------------------------------------------------------- workload
+def cone_angles():
+    return np.linspace(0, 2 * np.pi, CONE['views'], endpoint=False).astype(np.float32)
+
+
+def build_cone_workload(device):
+    import torch
+    import mbirjax_b200 as mb
+    from mbirjax_b200.utilities import gen_ellipsoid_phantom, add_noise
+    model = mb.ConeBeamModel((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(),
+                             source_detector_dist=CONE['sdd'], source_iso_dist=CONE['sid'])
+    model.set_params(sharpness=0.0, snr_db=30.0, granularity=[CONE['subsets']], partition_sequence=[0], verbose=0)
+    phantom = gen_ellipsoid_phantom(model.get_params('recon_shape'), CONE['ellipsoids'], CONE['seed'], device=device)
+    np.random.seed(CONE['seed'])
+    sino = add_noise(model.forward_project(phantom), 0.01, CONE['seed']).contiguous()
+    return model, sino, phantom
+
+
+def recon_once(model, sino):
+    np.random.seed(CONE['seed'])
+    rec, _ = model.recon(sino, max_iterations=CONE['iterations'], stop_threshold_change_pct=0, logfile_path=None,
+                         print_logs=False)
+    return rec
+
+
+def timed_steps(step_fn, steps, warmup, world, flush):
+    import torch
+    for _ in range(warmup):
+        step_fn()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    start, end = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+    start.record()
+    for _ in range(steps):
+        flush()
+        step_fn()
+    end.record()
+    torch.cuda.synchronize()
+    barrier(world)
+    torch.cuda.synchronize()
+    return start.elapsed_time(end)
+
+
+def kernel_roofline(model, sino, peak_gbs, peak_kind):
+    """Average duration of one VCD subset's back and forward projection (CUDA events, 20 launches each)."""
+    import torch
+    from mbirjax_b200 import _capi
+    import mbirjax_b200 as mb
+    g = model._geometry()
+    V, R, C = model.get_params('sinogram_shape')
+    S = model.get_params('recon_shape')[2]
+    np.random.seed(CONE['seed'])
+    subset = mb.gen_pixel_partition(model.get_params('recon_shape'), CONE['subsets'])[0]
+    pix = torch.as_tensor(subset, device='cuda')
+    n = int(pix.shape[0])
+    vox = torch.rand((n, S), device='cuda')
+    out_fp = torch.empty((V, R, C), device='cuda')
+    out_bp = torch.empty((n, S), device='cuda')
+    res = {}
+    for name, fn in (('bp_cone', lambda: _capi.back_project(g, sino, pix, out=out_bp)),
+                     ('fp_cone', lambda: _capi.forward_project(g, vox, pix, out=out_fp))):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        reps = 20
+        s.record()
+        for _ in range(reps):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        ms = s.elapsed_time(e) / reps
+        alg_bytes = 4.0 * (V * n * S + V * R * C)
+        achieved = alg_bytes / (ms * 1e-3) / 1e9
+        res[name] = {'ms': ms, 'alg_bytes': alg_bytes, 'achieved_gbs': achieved}
+    dom = max(res, key=lambda k: res[k]['ms'])
+    d = res[dom]
+    traffic = profile_traffic(dom)
+    return {'kernel': dom, 'bound': 'hbm', 'achieved': round(d['achieved_gbs'], 1), 'peak': peak_gbs,
+            'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': round(d['achieved_gbs'] / peak_gbs, 4),
+            'traffic': traffic, 'launch_ms': round(d['ms'], 4),
+            'alg_bytes_per_launch': d['alg_bytes'],
+            'other': {k: {'launch_ms': round(v['ms'], 4), 'achieved_gbs': round(v['achieved_gbs'], 1)}
+                      for k, v in res.items() if k != dom}}
+
+
+def profile_traffic(kernel):
+    """DRAM bytes per launch of the kernel, from the committed ncu summary (profiles/<kernel>_*.md)."""
+    pdir = os.path.join(ROOT, 'profiles')
+    if not os.path.isdir(pdir):
+        return None
+    for fn in sorted(os.listdir(pdir)):
+        if fn.startswith(kernel) and fn.endswith('.md'):
+            m = re.search(r'traffic_bytes_per_launch:\s*([0-9.eE+]+)', open(os.path.join(pdir, fn)).read())
+            if m:
+                return float(m.group(1))
+    return None
+
+
+def cpu_reference_sample(workers=None):
+    """One VCD subset update of the workload with the oracle on all host cores; returns (seconds, cores, note)."""
+    import oracle as O
+    from oracle.pool import OraclePool, vcd_subset_update_pooled
+    geom = O.cone_geometry((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(), CONE['sdd'], CONE['sid'])
+    nr, nc, ns = geom.recon_shape
+    rng = np.random.default_rng(0)
+    flat = rng.random((nr * nc, ns)).astype(np.float32) * 0.1
+    err = rng.standard_normal(geom.sinogram_shape).astype(np.float32)
+    hess = np.full((nr * nc, ns), 1000.0, dtype=np.float32)
+    np.random.seed(CONE['seed'])
+    subset = O.gen_pixel_partition(geom.recon_shape, CONE['subsets'])[0]
+    params = (O.get_b_from_nbr_wts([1, 1, 1]), 0.05, 2.0, 1.2, 1.0)
+    pool = OraclePool(geom, workers)
+    try:
+        vcd_subset_update_pooled(pool, flat, err, None, hess, subset[:256], 100.0, params)  # start workers
+        t0 = time.perf_counter()
+        vcd_subset_update_pooled(pool, flat, err, None, hess, subset, 100.0, params)
+        dt = time.perf_counter() - t0
+    finally:
+        pool.close()
+    return dt, pool.workers
+
+
+def cpu_recons_per_s(subset_seconds):
+    # one recon = subsets x iterations subset updates (the FDK initialisation and Hessian are not counted)
+    return 1.0 / (subset_seconds * CONE['subsets'] * CONE['iterations'])
+
+
+# ----------------------------------------------------------------------------------------------- arms
+def run_reference(args):
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    samples = []
+    cores = None
+    for i in range(args.warmup + args.steps):
+        dt, cores = cpu_reference_sample()
+        if i >= args.warmup:
+            samples.append(dt)
+    mean = float(np.mean(samples))
+    value = cpu_recons_per_s(mean)
+    sample = ('one VCD subset update (1 of %d subsets, 1 of %d iterations) of the cone workload per step, oracle '
+              'port on %d processes; scaled x%d to one recon' % (CONE['subsets'], CONE['iterations'], cores,
+                                                                CONE['subsets'] * CONE['iterations']))
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'recons/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': cone_config(world),
+            'cpu_baseline': {'value': value, 'unit': 'recons/s', 'cores': cores, 'kind': 'port', 'sample': sample},
+            'e2e': {'value': value, 'unit': 'recons/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+            'note': 'reference JAX CPU path unavailable (jax not installable offline); oracle NumPy port timed'}
+    print(json.dumps(line), flush=True)
+
+
+def cone_config(world):
+    return {'workload': 'plain cone-beam VCD, sinogram 256x128x256, recon 256x256x128, 20 iterations x 4 subsets, '
+                        'FDK init, sdd=sid=1024', 'views': CONE['views'], 'det_rows': CONE['rows'],
+            'det_channels': CONE['channels'], 'recon_shape': [256, 256, 128], 'iterations': CONE['iterations'],
+            'subsets': CONE['subsets'], 'parallelism': 'replicas x%d' % world, 'l2': 'flushed before every step'}
+
+
+def run_gpu(args):
+    import torch
+    import mbirjax_b200 as mb
+    from mbirjax_b200 import _capi
+    world, rank, local = dist_setup(args.gpus)
+    device = torch.device('cuda', local)
+    lib = _capi.load_library()
+    peak_gbs, peak_kind = load_peaks()
+    model, sino, phantom = build_cone_workload(device)
+    flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
+
+    def flush():
+        flush_buf.zero_()
+
+    # device-resident: sinogram already in HBM
+    def step():
+        recon_once(model, sino)
+
+    clocks = ClockSampler(local)
+    launches0 = None
+    for _ in range(args.warmup):
+        step()
+    torch.cuda.synchronize()
+    clocks.start()
+    launches0 = lib.mbx_launch_count()
+    ms = timed_steps(step, args.steps, 0, world, flush)
+    launches = lib.mbx_launch_count() - launches0
+    clk = clocks.stop()
+    ms = max_over_ranks(ms, world)
+    ms_per_step = ms / args.steps
+    value = world * args.steps / (ms * 1e-3)
+
+    # accuracy of this recon against the phantom (sanity) is reported; parity vs the oracle is in the tests
+    rec = recon_once(model, sino)
+    nrmse_phantom = float(torch.linalg.norm(rec - phantom) / torch.linalg.norm(phantom))
+
+    line = {'metric': METRIC, 'value': round(value, 3), 'unit': 'recons/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': round(ms_per_step, 3), 'higher_is_better': True, 'scaling': 'weak',
+            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': cone_config(world),
+            'gpu_launches': int(launches), 'clocks': clk, 'nrmse_vs_phantom': round(nrmse_phantom, 4)}
+
+    if not args.no_e2e:
+        host_sino = sino.cpu().pin_memory()
+        out_host = torch.empty(tuple(model.get_params('recon_shape')), dtype=torch.float32).pin_memory()
+
+        def e2e_step():
+            r = recon_once(model, host_sino)          # H2D of the sinogram happens inside the public API call
+            out_host.copy_(r, non_blocking=True)      # D2H of the recon
+        e_ms = timed_steps(e2e_step, args.steps, 1, world, flush)
+        e_ms = max_over_ranks(e_ms, world)
+        line['e2e'] = {'value': round(world * args.steps / (e_ms * 1e-3), 3), 'unit': 'recons/s',
+                       'h2d_bytes_per_step': int(host_sino.numel() * 4),
+                       'd2h_bytes_per_step': int(out_host.numel() * 4)}
+
+    line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind)
+
+    if rank == 0 and world == 1 and not args.no_cpu_baseline:
+        dt, cores = cpu_reference_sample()
+        line['cpu_baseline'] = {'value': round(cpu_recons_per_s(dt), 6), 'unit': 'recons/s', 'cores': cores,
+                                'kind': 'port',
+                                'sample': 'one VCD subset update of the workload (oracle NumPy port, %d processes), '
+                                          'scaled x%d to one recon; %.2f s measured' % (
+                                              cores, CONE['subsets'] * CONE['iterations'], dt)}
+    if rank == 0:
+        print(json.dumps(line), flush=True)
+    if world > 1:
+        import torch.distributed as dist
+        dist.destroy_process_group()
+
+
+def main():
+    args = parse_args()
+    if args.impl == 'reference':
+        run_reference(args)
+    else:
+        run_gpu(args)
+
+
+if __name__ == '__main__':
+    main()

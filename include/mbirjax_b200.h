@@ -90,6 +90,9 @@ MBX_API int mbx_last_cuda_error(void);
 /* Reads and clears the device error word of the current device (synchronises the device).
  * Bit 0: a pixel index was out of range; bit 1: a view index was out of range. */
 MBX_API int mbx_get_device_error(int *flags_out);
+/* Number of kernel launches this library has submitted since it was loaded (host-side count, all devices and
+ * streams; launches replayed from a captured CUDA graph are not re-counted). */
+MBX_API uint64_t mbx_launch_count(void);
 
 /* ---- projectors ------------------------------------------------------------------------------- */
 

@@ -228,6 +228,7 @@ static cudaError_t launch_bp_t(const mbx_geom &g, const BpPlan &pl, const float 
     dim3 grid(pl.gx, pl.gy, pl.splits);
     kern<<<grid, BP_THREADS, pl.smem, st>>>(g, sino, w, pix, n, views, nv, pl.views_per_split, cp, scale, dst, ss,
                                             pl.cache_rows, device_error_ptr());
+    mbx::note_launch();
     return cudaGetLastError();
 }
 

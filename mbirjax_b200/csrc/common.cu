@@ -1,4 +1,5 @@
 // Library identification, error reporting and device queries for the mbirjax_b200 C ABI.
+#include <atomic>
 #include <cstdio>
 
 #include "mbx_common.cuh"
@@ -26,6 +27,10 @@ int *device_error_ptr() {
     }
     return cache[dev];
 }
+
+static std::atomic<unsigned long long> g_launches{0};
+
+void note_launch() { g_launches.fetch_add(1, std::memory_order_relaxed); }
 
 static thread_local int t_last_cuda_error = 0;
 
@@ -95,6 +100,8 @@ extern "C" const char *mbx_error_string(int code) {
 }
 
 extern "C" int mbx_last_cuda_error(void) { return mbx::t_last_cuda_error; }
+
+extern "C" uint64_t mbx_launch_count(void) { return mbx::g_launches.load(std::memory_order_relaxed); }
 
 extern "C" int mbx_get_device_error(int *flags_out) {
     if (!flags_out) return MBX_ERR_INVALID_ARG;

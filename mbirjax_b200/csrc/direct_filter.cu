@@ -117,6 +117,7 @@ extern "C" int mbx_direct_filter(const mbx_geom *g, const float *sinogram, float
     mbx::direct_filter_kernel<<<blocks, mbx::FILT_THREADS, smem, static_cast<cudaStream_t>(stream)>>>(
         sinogram, out, rows_total, R, C, filter_scale, out_scale, fdk, g->source_detector_dist, g->delta_det_channel,
         g->delta_det_row, g->det_channel_offset, g->det_row_offset);
+    mbx::note_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? MBX_OK : mbx::set_cuda_error(e);
 }

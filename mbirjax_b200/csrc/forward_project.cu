@@ -131,6 +131,7 @@ __global__ void split_sum_kernel(const float *__restrict__ ws, long long stride,
 void launch_split_sum(const float *ws, long long stride, int splits, float scale, float *out, long long n,
                       cudaStream_t st) {
     split_sum_kernel<<<grid_for(n, 256), 256, 0, st>>>(ws, stride, splits, scale, out, n);
+    mbx::note_launch();
 }
 
 struct FpPlan {
@@ -188,6 +189,7 @@ static cudaError_t launch_fp_t(const mbx_geom &g, const FpPlan &pl, const float 
     dim3 grid(num_views_sel, pl.tiles, pl.splits), block(pl.bx, pl.by);
     kern<<<grid, block, pl.smem, st>>>(g, vox, pix, num_pixels, views, dst, pl.row_tile, pl.c_pad,
                                        pl.pixels_per_split, split_stride, device_error_ptr());
+    mbx::note_launch();
     return cudaGetLastError();
 }
 

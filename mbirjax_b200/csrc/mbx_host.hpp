@@ -12,6 +12,9 @@ namespace mbx {
 // Number of SMs of the current device (cached per device; 148 when no device can be queried).
 int num_sms();
 
+// Counts kernel launches submitted by this library (host-side, all devices); read by mbx_launch_count().
+void note_launch();
+
 // Records a CUDA error for mbx_last_cuda_error() and returns MBX_ERR_CUDA.
 int set_cuda_error(cudaError_t e);
 

@@ -106,6 +106,7 @@ int qggmrf_grad_hess(const float *recon, int nr, int nc, int ns, const int32_t *
     const long long total = num_pixels * ns;
     qggmrf_grad_hess_kernel<<<grid_for(total, 256), 256, 0, st>>>(recon, nr, nc, ns, pix, num_pixels, q, grad, hess,
                                                                    device_error_ptr());
+    mbx::note_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
 }
@@ -144,6 +145,7 @@ extern "C" int mbx_qggmrf_loss_grad(const float *recon, int32_t num_recon_rows, 
     double *partials = static_cast<double *>(workspace);
     mbx::qggmrf_loss_grad_kernel<<<blocks, 256, 0, st>>>(recon, num_recon_rows, num_recon_cols, num_recon_slices, q,
                                                           grad_out, partials);
+    mbx::note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return mbx::set_cuda_error(e);
     mbx::launch_sum_partials(partials, (int)blocks, 1, loss_out, st);

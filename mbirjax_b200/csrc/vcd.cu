@@ -36,6 +36,7 @@ __global__ void sum_partials_kernel(const double *__restrict__ partials, int nbl
 
 void launch_sum_partials(const double *partials, int nblocks, int nv, double *out, cudaStream_t st) {
     sum_partials_kernel<<<1, 256, 0, st>>>(partials, nblocks, nv, out);
+    mbx::note_launch();
 }
 
 __device__ __forceinline__ double fixed_order_sum(const double *__restrict__ partials, int nblocks, int nv, int v) {
@@ -233,19 +234,24 @@ int vcd_subset_step(const mbx_geom &g, float *recon, float *err_sino, const floa
     const unsigned nb1 = red_blocks(ncyl, L.max_blocks);
     vcd_delta_kernel<<<nb1, 256, 0, st>>>(recon, g.num_recon_rows, g.num_recon_cols, ns, pix, num_pixels, bp,
                                           fm_hessian, fm_constant, make_qparams(qp), delta, prior_partials, err);
+    mbx::note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e);
     rc = forward_project(g, delta, pix, num_pixels, nullptr, g.num_views, dsino, base + L.fpws, L.fp_bytes, st);
     if (rc != MBX_OK) return rc;
     const unsigned nb2 = red_blocks(nsino / 4 + 1, L.max_blocks);
     vcd_linquad_kernel<<<nb2, 256, 0, st>>>(dsino, err_sino, wts, nsino, fwd_partials);
+    mbx::note_launch();
     vcd_alpha_kernel<<<1, 32, 0, st>>>(prior_partials, (int)nb1, fwd_partials, (int)nb2, (double)fm_constant, alpha,
                                        stats);
+    mbx::note_launch();
     const unsigned nb3 = red_blocks(ncyl, L.max_blocks);
     vcd_apply_kernel<<<nb3, 256, 0, st>>>(recon, ns, pix, num_pixels, g.num_recon_rows * g.num_recon_cols, delta,
                                           alpha, l1_partials);
+    mbx::note_launch();
     vcd_error_kernel<<<grid_for(nsino / 4 + 1, 256), 256, 0, st>>>(err_sino, dsino, nsino, alpha, l1_partials,
                                                                   (int)nb3, stats);
+    mbx::note_launch();
     e = cudaGetLastError();
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
 }
