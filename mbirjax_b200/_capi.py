@@ -41,6 +41,7 @@ _SIGNATURES = {
     'mbx_error_string': (ctypes.c_char_p, [ctypes.c_int]),
     'mbx_last_cuda_error': (ctypes.c_int, []),
     'mbx_get_device_error': (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
+    'mbx_launch_count': (ctypes.c_uint64, []),
     'mbx_forward_project_workspace_bytes': (c_size_t, [ctypes.POINTER(MbxGeom), c_int64, c_int32]),
     'mbx_sparse_forward_project': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_int64, c_void_p,
                                                   c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),
