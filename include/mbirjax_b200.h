@@ -88,7 +88,8 @@ MBX_API const char *mbx_error_string(int code);
 /* The CUDA error code behind the last MBX_ERR_CUDA returned on this host thread. */
 MBX_API int mbx_last_cuda_error(void);
 /* Reads and clears the device error word of the current device (synchronises the device).
- * Bit 0: a pixel index was out of range; bit 1: a view index was out of range. */
+ * Bit 0: a pixel index was out of range; bit 1: a view index was out of range; bit 2: a projector tile
+ * exceeded its shared-memory row cache (the geometry check should make this impossible). */
 MBX_API int mbx_get_device_error(int *flags_out);
 /* Number of kernel launches this library has submitted since it was loaded (host-side count, all devices and
  * streams; launches replayed from a captured CUDA graph are not re-counted). */

@@ -16,17 +16,57 @@
 // (a fused W * e).  Views may be split over CTAs with a fixed-order second-stage sum when there are too
 // few pixels to fill the GPU (caller workspace).
 #include "back_project.cuh"
+#include "bp_fast.cuh"
 
 namespace mbx {
 
 size_t bp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel) {
+    const BpfPlan fp = plan_bp_fast(g, num_pixels, num_views_sel);
+    if (fp.ok) return fp.workspace;
     return plan_bp(g, num_pixels, num_views_sel).workspace;
+}
+
+template <int KIND>
+static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const float *sino, const float *w,
+                                  const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
+                                  float *dst, long long ss, cudaStream_t st) {
+    auto kern = bp_fast_kernel<KIND>;
+    static bool attr_set = false;
+    if (!attr_set) {
+        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        if (e != cudaSuccess) return e;
+        attr_set = true;
+    }
+    dim3 grid(pl.gx, pl.gy, pl.splits);
+    kern<<<grid, BPF_THREADS, pl.smem, st>>>(g, sino, w, pix, n, views, nv, pl.views_per_split, cp, scale, dst, ss,
+                                             pl.nsl, pl.npg, pl.vc, device_error_ptr());
+    note_launch();
+    return cudaGetLastError();
 }
 
 int back_project(const mbx_geom &g, const float *sino, const float *w, const int32_t *pix, long long num_pixels,
                  const int32_t *views, int num_views_sel, int coeff_power, float scale, float *out, void *ws,
                  size_t ws_bytes, cudaStream_t st) {
     if (num_pixels == 0) return MBX_OK;
+    const BpfPlan fpl = plan_bp_fast(g, num_pixels, num_views_sel);
+    if (fpl.ok) {
+        if (fpl.workspace > 0 && (ws == nullptr || ws_bytes < fpl.workspace)) return MBX_ERR_WORKSPACE;
+        float *dst = fpl.splits > 1 ? static_cast<float *>(ws) : out;
+        const long long stride = num_pixels * (long long)g.num_recon_slices;
+        const long long ss = fpl.splits > 1 ? stride : 0;
+        cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
+                            ? launch_bp_fast<MBX_GEOM_PARALLEL>(g, fpl, sino, w, pix, num_pixels, views, num_views_sel,
+                                                                coeff_power, scale, dst, ss, st)
+                            : launch_bp_fast<MBX_GEOM_CONE>(g, fpl, sino, w, pix, num_pixels, views, num_views_sel,
+                                                            coeff_power, scale, dst, ss, st);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        if (fpl.splits > 1) {
+            launch_split_sum(dst, stride, fpl.splits, scale, out, stride, st);
+            e = cudaGetLastError();
+            if (e != cudaSuccess) return set_cuda_error(e);
+        }
+        return MBX_OK;
+    }
     const BpPlan pl = plan_bp(g, num_pixels, num_views_sel);
     if (pl.workspace > 0 && (ws == nullptr || ws_bytes < pl.workspace)) return MBX_ERR_WORKSPACE;
     float *dst = pl.splits > 1 ? static_cast<float *>(ws) : out;

@@ -1,0 +1,313 @@
+// Back projector specialised for psf_radius == 1 (the reference's default geometry: delta_voxel equal to the
+// detector pitch at the magnification), for parallel and cone beam.  Same contract and arithmetic as the
+// general bp_kernel (back_project.cuh); organised to minimise instructions per (pixel, slice, view):
+//
+//  * CTA = 256 threads = 8 warps; lanes run along 32 pixels, warps along slice tiles of ST slices (or along
+//    further pixel groups when the cylinder has fewer than 8 tiles).  Accumulators stay in registers.
+//  * Per chunk of views, each (pixel, view) footprint is computed once, by one thread, into shared memory and
+//    read by every warp of that pixel: centre channel, the three channel coefficients (already raised to
+//    coeff_power) and, for cone beam, the affine map slice -> detector row m_p(k) = A0 + k*A1 and the
+//    vertical-angle factor c2 = (mag/D)^2 so that 1/cos(phi_k) = sqrt(1 + c2 z_k^2).  The cone footprint is
+//    trig-free: cos/sin(theta - theta_p) and 1/cos(theta_p) come from the per-view cos/sin and
+//    rsqrt(D^2 + u^2) instead of atan2/cos/sin per pixel.
+//  * Cone: every detector row a warp's slice tile touches is gathered once per view into the thread's column
+//    of a shared-memory row cache ([row][thread], conflict-free), rows outside the detector cached as 0; the
+//    vertical fan then reads three cached rows per slice with no bounds tests.  plan_bp_fast admits a geometry
+//    only when the rows of a slice tile (ST * max |dm/dk| + 4) fit the cache.
+#pragma once
+
+#include "back_project.cuh"
+
+namespace mbx {
+
+constexpr int BPF_THREADS = 256;
+constexpr int BPF_ST = 16;          // slices per thread
+constexpr int BPF_CACHE_ROWS = 48;  // row-cache depth per thread (cone): ST * max|dm/dk| + 4 must fit
+
+struct BpfPlan {
+    int nsl;    // slice tiles per CTA (warps per pixel group)
+    int npg;    // pixel groups of 32 per CTA
+    int vc;     // views per footprint chunk
+    int gx, gy, splits, views_per_split;
+    size_t smem, workspace;
+    bool ok;
+};
+
+// Footprint record in shared memory (structure of arrays, [vc][pixels]).
+struct BpfShared {
+    int *nc;
+    float *a0, *a1, *a2, *A0, *A1, *c2;
+};
+
+template <int KIND>
+__device__ __forceinline__ void bpf_footprint(const mbx_geom &g, float cs, float sn, float x_tilde, float y_tilde,
+                                              int coeff_power, int &nc, float &a0, float &a1, float &a2, float &A0,
+                                              float &A1, float &c2) {
+    const float inv_dc = 1.0f / g.delta_det_channel;
+    const float det_center_channel = 0.5f * (float)(g.num_det_channels - 1);
+    float n_p, w, scale;  // scale = delta_voxel / cos_alpha
+    if (KIND == MBX_GEOM_PARALLEL) {
+        const float x = cs * x_tilde - sn * y_tilde;
+        n_p = (x + g.det_channel_offset) * inv_dc + det_center_channel;
+        const float cos_alpha = fmaxf(fabsf(cs), fabsf(sn));
+        w = (g.delta_voxel * inv_dc) * cos_alpha;
+        scale = g.delta_voxel / cos_alpha;
+        A0 = A1 = c2 = 0.0f;
+    } else {
+        const float x_p = cs * x_tilde - sn * y_tilde;
+        const float y_p = sn * x_tilde + cs * y_tilde;
+        const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
+        const float mag = 1.0f / (1.0f / g.magnification - y_p * inv_d);
+        const float u = mag * x_p;
+        n_p = (u + g.det_channel_offset) * inv_dc + det_center_channel;
+        // theta_p = atan2(u, D): cos = D / h, sin = u / h with h = sqrt(D^2 + u^2)  (D = inf: cos 1, sin 0)
+        const float t = u * inv_d;
+        const float inv_h = rsqrtf(fmaf(t, t, 1.0f));                    // cos(theta_p)
+        const float cos_tp = inv_h, sin_tp = t * inv_h;
+        const float cd = cs * cos_tp + sn * sin_tp;                       // cos(theta - theta_p)
+        const float sd = sn * cos_tp - cs * sin_tp;                       // sin(theta - theta_p)
+        const float cos_alpha = fmaxf(fabsf(cd), fabsf(sd));
+        w = mag * (g.delta_voxel * inv_dc) * (cos_alpha / cos_tp);
+        scale = g.delta_voxel / cos_alpha;
+        const float inv_dr = 1.0f / g.delta_det_row;
+        const float center_slice = 0.5f * (float)(g.num_recon_slices - 1);
+        const float z0 = g.recon_slice_offset - g.delta_voxel * center_slice;
+        A1 = mag * g.delta_voxel * inv_dr;
+        A0 = (mag * z0 + g.det_row_offset) * inv_dr + 0.5f * (float)(g.num_det_rows - 1);
+        const float mr = mag * inv_d;
+        c2 = mr * mr;
+    }
+    nc = (int)rintf(n_p);
+    const float half_w = (w + 1.0f) * 0.5f;
+    const float l_max = fminf(1.0f, w);
+    const float d = n_p - (float)nc;
+    float c[3];
+#pragma unroll
+    for (int k = -1; k <= 1; ++k) {
+        const int n = nc + k;
+        float a = scale * fminf(fmaxf(half_w - fabsf(d - (float)k), 0.0f), l_max);
+        if (n < 0 || n >= g.num_det_channels) a = 0.0f;
+        c[k + 1] = (coeff_power == 2) ? a * a : a;
+    }
+    a0 = c[0];
+    a1 = c[1];
+    a2 = c[2];
+}
+
+// sum_k a_k * (w * sino)[row, nc + k], the three taps gathered with clamped (in-range) addresses.
+__device__ __forceinline__ float bpf_row(const float *__restrict__ row, const float *__restrict__ wrow, int n0, int n1,
+                                         int n2, float a0, float a1, float a2) {
+    float v0 = __ldg(row + n0), v1 = __ldg(row + n1), v2 = __ldg(row + n2);
+    if (wrow) {
+        v0 *= __ldg(wrow + n0);
+        v1 *= __ldg(wrow + n1);
+        v2 *= __ldg(wrow + n2);
+    }
+    return fmaf(a0, v0, fmaf(a1, v1, a2 * v2));
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(BPF_THREADS, 3)
+bp_fast_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restrict__ wts,
+               const int32_t *__restrict__ pix, long long num_pixels, const int32_t *__restrict__ views,
+               int num_views_sel, int views_per_split, int coeff_power, float scale, float *__restrict__ dst,
+               long long split_stride, int nsl, int npg, int vc, int *err) {
+    extern __shared__ __align__(16) float smf[];
+    const int pcta = 32 * npg;                       // pixels per CTA
+    const int nfp = vc * pcta;                       // footprints per chunk
+    BpfShared sh;
+    sh.nc = reinterpret_cast<int *>(smf);
+    sh.a0 = smf + nfp;
+    sh.a1 = smf + 2 * nfp;
+    sh.a2 = smf + 3 * nfp;
+    sh.A0 = smf + 4 * nfp;
+    sh.A1 = smf + 5 * nfp;
+    sh.c2 = smf + 6 * nfp;
+    float *s_cs = smf + 7 * nfp;
+    float *s_sn = s_cs + vc;
+    int *s_vi = reinterpret_cast<int *>(s_sn + vc);
+    float *cache = reinterpret_cast<float *>(s_vi + vc);  // [BPF_CACHE_ROWS][BPF_THREADS] (cone)
+    // 16-byte alignment of the cache is not needed (scalar accesses)
+
+    const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
+    const int pg = warp / nsl, stl = warp - pg * nsl;
+    const int pl = pg * 32 + lane;                                   // pixel within CTA
+    const long long p = (long long)blockIdx.x * pcta + pl;
+    const int s0 = (blockIdx.y * nsl + stl) * BPF_ST;
+    const int num_rows = g.num_det_rows, num_channels = g.num_det_channels, num_slices = g.num_recon_slices;
+    const int ns = min(BPF_ST, num_slices - s0);
+    const int split = blockIdx.z;
+    const int v_begin = split * views_per_split;
+    const int v_end = min(num_views_sel, v_begin + views_per_split);
+    const int npix_grid = g.num_recon_rows * g.num_recon_cols;
+
+    // pixel geometry of the pixel this thread computes footprints for (pixel tid % pcta)
+    const int fpl = tid % pcta;
+    const long long fp_pixel = (long long)blockIdx.x * pcta + fpl;
+    float fxt = 0.0f, fyt = 0.0f;
+    bool fvalid = false;
+    if (fp_pixel < num_pixels) {
+        const int idx = pix[fp_pixel];
+        if (idx >= 0 && idx < npix_grid) {
+            pixel_tilde(g, idx, fxt, fyt);
+            fvalid = true;
+        } else if (blockIdx.y == 0 && split == 0 && tid < pcta) {
+            flag_error(err, MBX_ERRFLAG_PIXEL);
+        }
+    }
+    bool active = p < num_pixels && ns > 0;
+    if (active) {
+        const int idx = pix[p];
+        active = idx >= 0 && idx < npix_grid;
+    }
+
+    float acc[BPF_ST];
+#pragma unroll
+    for (int s = 0; s < BPF_ST; ++s) acc[s] = 0.0f;
+
+    const float z0 = g.recon_slice_offset - g.delta_voxel * 0.5f * (float)(num_slices - 1);
+    float *mycache = cache + tid;
+
+    for (int vb = v_begin; vb < v_end; vb += vc) {
+        const int nv = min(vc, v_end - vb);
+        __syncthreads();
+        if (tid < nv) {
+            const int vi = views ? views[vb + tid] : vb + tid;
+            const bool ok = vi >= 0 && vi < g.num_views;
+            if (!ok && blockIdx.x == 0 && blockIdx.y == 0) flag_error(err, MBX_ERRFLAG_VIEW);
+            const float ang = ok ? g.angles[vi] : 0.0f;
+            s_vi[tid] = ok ? vi : -1;
+            s_cs[tid] = cosf(ang);
+            s_sn[tid] = sinf(ang);
+        }
+        __syncthreads();
+        for (int f = tid; f < nv * pcta; f += BPF_THREADS) {
+            const int t = f / pcta;
+            int nc = INT_MIN;
+            float a0 = 0.f, a1 = 0.f, a2 = 0.f, A0 = 0.f, A1 = 0.f, c2 = 0.f;
+            if (fvalid && s_vi[t] >= 0)
+                bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, nc, a0, a1, a2, A0, A1, c2);
+            sh.nc[f] = nc;
+            sh.a0[f] = a0;
+            sh.a1[f] = a1;
+            sh.a2[f] = a2;
+            sh.A0[f] = A0;
+            sh.A1[f] = A1;
+            sh.c2[f] = c2;
+        }
+        __syncthreads();
+        if (!active) continue;
+        for (int t = 0; t < nv; ++t) {
+            const int f = t * pcta + pl;
+            const int nc = sh.nc[f];
+            if (nc == INT_MIN) continue;
+            const int vi = s_vi[t];
+            const float a0 = sh.a0[f], a1 = sh.a1[f], a2 = sh.a2[f];
+            const int n0 = min(max(nc - 1, 0), num_channels - 1);
+            const int n1 = min(max(nc, 0), num_channels - 1);
+            const int n2 = min(max(nc + 1, 0), num_channels - 1);
+            const float *view = sino + (long long)vi * num_rows * num_channels;
+            const float *wview = wts ? wts + (long long)vi * num_rows * num_channels : nullptr;
+            if (KIND == MBX_GEOM_PARALLEL) {
+                const float *row = view + (long long)s0 * num_channels;
+                const float *wrow = wview ? wview + (long long)s0 * num_channels : nullptr;
+#pragma unroll
+                for (int s = 0; s < BPF_ST; ++s) {
+                    if (s < ns) acc[s] += bpf_row(row, wrow, n0, n1, n2, a0, a1, a2);
+                    row += num_channels;
+                    if (wrow) wrow += num_channels;
+                }
+            } else {
+                const float A0 = sh.A0[f], A1 = sh.A1[f], c2 = sh.c2[f];
+                const float half_w = (A1 + 1.0f) * 0.5f;
+                const float l_max = fminf(1.0f, A1);
+                const int mc_first = (int)rintf(fmaf((float)s0, A1, A0));
+                const int mc_last = (int)rintf(fmaf((float)(s0 + ns - 1), A1, A0));
+                const int m_lo = min(mc_first, mc_last) - 1;
+                const int m_hi = max(mc_first, mc_last) + 1;
+                if (m_hi - m_lo + 1 > BPF_CACHE_ROWS) {  // excluded by plan_bp_fast; never read past the cache
+                    flag_error(err, MBX_ERRFLAG_CACHE);
+                    continue;
+                }
+                for (int m = m_lo; m <= m_hi; ++m) {
+                    float c = 0.0f;
+                    if (m >= 0 && m < num_rows) {
+                        const long long off = (long long)m * num_channels;
+                        c = bpf_row(view + off, wview ? wview + off : nullptr, n0, n1, n2, a0, a1, a2);
+                    }
+                    mycache[(m - m_lo) * BPF_THREADS] = c;
+                }
+#pragma unroll
+                for (int s = 0; s < BPF_ST; ++s) {
+                    if (s < ns) {
+                        const float k = (float)(s0 + s);
+                        const float m_p = fmaf(k, A1, A0);
+                        const int m_c = (int)rintf(m_p);
+                        const float d = m_p - (float)m_c;
+                        const float z = fmaf(k, g.delta_voxel, z0);
+                        const float q = fmaf(c2, z * z, 1.0f);
+                        float sec = q * rsqrtf(q);                       // 1 / cos(phi_k)
+                        const float l_m = fminf(fmaxf(half_w - fabsf(d + 1.0f), 0.0f), l_max);
+                        const float l_0 = fminf(fmaxf(half_w - fabsf(d), 0.0f), l_max);
+                        const float l_p = fminf(fmaxf(half_w - fabsf(d - 1.0f), 0.0f), l_max);
+                        const float *cc = mycache + (m_c - m_lo) * BPF_THREADS;
+                        const float cm = cc[-BPF_THREADS], c0 = cc[0], cp = cc[BPF_THREADS];
+                        if (coeff_power == 2) {
+                            sec *= sec;
+                            acc[s] = fmaf(sec, fmaf(l_m * l_m, cm, fmaf(l_0 * l_0, c0, (l_p * l_p) * cp)), acc[s]);
+                        } else {
+                            acc[s] = fmaf(sec, fmaf(l_m, cm, fmaf(l_0, c0, l_p * cp)), acc[s]);
+                        }
+                    }
+                }
+            }
+        }
+    }
+    if (!active && p >= num_pixels) return;
+    if (ns <= 0) return;
+    float *out = dst + (long long)split * split_stride + p * (long long)num_slices + s0;
+    const float sc = (split_stride == 0) ? scale : 1.0f;
+#pragma unroll
+    for (int s = 0; s < BPF_ST; ++s)
+        if (s < ns) out[s] = active ? sc * acc[s] : 0.0f;
+}
+
+inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_views_sel) {
+    BpfPlan pl;
+    pl.ok = (g.psf_radius == 1);
+    const int S = g.num_recon_slices;
+    const int tiles = ceil_div(S, BPF_ST);
+    pl.nsl = tiles >= 8 ? 8 : (tiles >= 4 ? 4 : (tiles >= 2 ? 2 : 1));
+    pl.npg = 8 / pl.nsl;
+    pl.vc = pl.nsl;  // footprints per chunk = 256
+    const int pcta = 32 * pl.npg;
+    pl.gx = ceil_div(num_pixels > 0 ? num_pixels : 1, pcta);
+    pl.gy = ceil_div(tiles, pl.nsl);
+    if (g.kind == MBX_GEOM_CONE) {
+        // the row cache must hold the rows of a slice tile: BPF_ST * max |dm/dk| + 4
+        const double half_r = 0.5 * (g.num_recon_rows - 1), half_c = 0.5 * (g.num_recon_cols - 1);
+        const double rho = g.delta_voxel * std::sqrt(half_r * half_r + half_c * half_c);
+        const double inv = 1.0 / g.magnification - (std::isinf(g.source_detector_dist) ? 0.0 : rho / g.source_detector_dist);
+        const double max_mag = inv > 1e-6 ? 1.0 / inv : 1e6;
+        const double slope = max_mag * g.delta_voxel / g.delta_det_row;
+        if (BPF_ST * slope + 4 > BPF_CACHE_ROWS) pl.ok = false;
+    }
+    const long long base = (long long)pl.gx * pl.gy;
+    const int sms = num_sms();
+    long long splits = 1;
+    if (base < 2LL * sms && num_views_sel >= 16) {
+        splits = (2LL * sms + base - 1) / base;
+        long long maxs = num_views_sel / 8;
+        if (splits > maxs) splits = maxs;
+        if (splits > 64) splits = 64;
+        if (splits < 1) splits = 1;
+    }
+    pl.views_per_split = ceil_div(num_views_sel, splits);
+    pl.splits = ceil_div(num_views_sel, pl.views_per_split);
+    const size_t nfp = (size_t)pl.vc * pcta;
+    pl.smem = nfp * 7 * 4 + (size_t)pl.vc * 12 + (g.kind == MBX_GEOM_CONE ? (size_t)BPF_CACHE_ROWS * BPF_THREADS * 4 : 0);
+    pl.workspace = pl.splits > 1 ? align256((size_t)pl.splits * num_pixels * S * 4) : 0;
+    return pl;
+}
+
+}  // namespace mbx

@@ -17,6 +17,7 @@
 
 #define MBX_ERRFLAG_PIXEL 1
 #define MBX_ERRFLAG_VIEW 2
+#define MBX_ERRFLAG_CACHE 4
 
 namespace mbx {
 
