@@ -165,6 +165,55 @@ MBX_API int mbx_vcd_subset_step(const mbx_geom *g, float *flat_recon, float *err
                         float fm_constant, const mbx_qggmrf_params *qp, double *stats_out, void *workspace,
                         size_t workspace_bytes, void *stream);
 
+/* ---- batched VCD over many scans ------------------------------------------------------------- */
+
+/* One scan of a batch: its geometry, device buffers and VCD parameters (the state the reference keeps per
+ * TomographyModel in vcd_recon, tomography_model.py:1086-1255). */
+typedef struct mbx_scan {
+    mbx_geom geom;
+    float *flat_recon;              /* (Nr*Nc, S), updated in place */
+    float *error_sinogram;          /* (V, R, C), updated in place; 16-byte aligned */
+    const float *weights;           /* (V, R, C) or NULL for constant weights 1 */
+    const float *fm_hessian;        /* (Nr*Nc, S): back projection of the weights with squared coefficients */
+    const int32_t *partition;       /* (num_subsets, subset_size) pixel indices, as gen_pixel_partition */
+    const int32_t *partition_order; /* optional (num_subsets, subset_size): a permutation of each subset's
+                                       positions giving the order the back projector visits them (locality) */
+    int32_t num_subsets;
+    int32_t subset_size;
+    float fm_constant;              /* 1 / sigma_y^2 */
+    mbx_qggmrf_params qp;
+} mbx_scan;
+
+/* Opaque host-side record of a prepared batch (filled by mbx_vcd_batched_prepare). */
+typedef struct mbx_batched_plan {
+    uint64_t opaque[64];
+} mbx_batched_plan;
+
+/* Workspace for a batch with num_steps subset steps in its schedule (0 if the batch is not supported). */
+MBX_API size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps);
+
+/* Validates the batch, lays out the workspace and uploads the per-scan argument records, the tile work lists
+ * and the subset schedule (schedule[step * num_scans + scan] = subset index that scan updates at that step;
+ * the reference draws it with np.random.permutation per iteration, tomography_model.py:1281).  step_stats
+ * (device, num_steps * num_scans * 4 doubles) receives per step and scan {alpha, l1 of the update, alpha
+ * numerator, alpha denominator}; iter_stats (device, num_iterations * num_scans * 4) receives
+ * {sum W e^2, sum |recon|, 0, 0} from mbx_vcd_batched_iteration_stats.  All scans must share one geometry kind
+ * and one num_subsets and have psf_radius (and for cone beam bp_psf_radius) 1; otherwise MBX_ERR_UNSUPPORTED.  Synchronises the
+ * stream (call it before any stream capture).  Replaces running the reference's vcd_recon once per scan. */
+MBX_API int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans, const int32_t *schedule,
+                                    int32_t num_steps, int32_t num_iterations, double *step_stats,
+                                    double *iter_stats, void *workspace, size_t workspace_bytes,
+                                    mbx_batched_plan *plan_out, void *stream);
+
+/* One subset update for every scan of the batch: eight persistent launches, each walking the packed work list
+ * of all scans (no host synchronisation; capturable in a CUDA graph).  Replaces one vcd_subset_updater call
+ * (tomography_model.py:1343-1542) per scan. */
+MBX_API int mbx_vcd_batched_step(const mbx_batched_plan *plan, int32_t step, void *stream);
+
+/* Per-scan iteration statistics into iter_stats[iteration] (inputs of the reference's fm_rmse and NMAE,
+ * tomography_model.py:1219-1220). */
+MBX_API int mbx_vcd_batched_iteration_stats(const mbx_batched_plan *plan, int32_t iteration, void *stream);
+
 /* ---- FBP / FDK filtering ---------------------------------------------------------------------- */
 
 /* Direct-recon filtering of a sinogram (num_views, R, C) into out (same shape).

@@ -35,6 +35,19 @@ class MbxQggmrfParams(ctypes.Structure):
     _fields_ = [('b', c_float * 6), ('sigma_x', c_float), ('p', c_float), ('q', c_float), ('T', c_float)]
 
 
+class MbxScan(ctypes.Structure):
+    """Mirror of ``mbx_scan``."""
+    _fields_ = [('geom', MbxGeom), ('flat_recon', c_void_p), ('error_sinogram', c_void_p), ('weights', c_void_p),
+                ('fm_hessian', c_void_p), ('partition', c_void_p), ('partition_order', c_void_p),
+                ('num_subsets', c_int32), ('subset_size', c_int32), ('fm_constant', c_float),
+                ('qp', MbxQggmrfParams)]
+
+
+class MbxBatchedPlan(ctypes.Structure):
+    """Mirror of ``mbx_batched_plan`` (opaque)."""
+    _fields_ = [('opaque', ctypes.c_uint64 * 64)]
+
+
 # name -> (restype, argtypes); must match include/mbirjax_b200.h
 _SIGNATURES = {
     'mbx_version': (ctypes.c_char_p, []),
@@ -58,6 +71,12 @@ _SIGNATURES = {
     'mbx_vcd_subset_step': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_int64, c_float, ctypes.POINTER(MbxQggmrfParams), c_void_p, c_void_p,
                                            c_size_t, c_void_p]),
+    'mbx_vcd_batched_workspace_bytes': (c_size_t, [ctypes.POINTER(MbxScan), c_int32, c_int32]),
+    'mbx_vcd_batched_prepare': (ctypes.c_int, [ctypes.POINTER(MbxScan), c_int32, c_void_p, c_int32, c_int32,
+                                               c_void_p, c_void_p, c_void_p, c_size_t,
+                                               ctypes.POINTER(MbxBatchedPlan), c_void_p]),
+    'mbx_vcd_batched_step': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_void_p]),
+    'mbx_vcd_batched_iteration_stats': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_void_p]),
     'mbx_direct_filter': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p]),
 }
 
@@ -232,3 +251,33 @@ def direct_filter(geom, sinogram, out=None):
         out = torch.empty_like(sinogram)
     _check(lib.mbx_direct_filter(ctypes.byref(geom), _ptr(sinogram), _ptr(out), _stream()), 'mbx_direct_filter')
     return out
+
+
+def vcd_batched_prepare(scans, schedule, num_iterations, step_stats, iter_stats, device):
+    """scans: list of MbxScan; schedule: int32 numpy (num_steps, num_scans).  Returns (plan, workspace)."""
+    import numpy as np
+    lib = load_library()
+    n = len(scans)
+    arr = (MbxScan * n)(*scans)
+    sched = np.ascontiguousarray(schedule, dtype=np.int32)
+    num_steps = int(sched.shape[0])
+    nbytes = lib.mbx_vcd_batched_workspace_bytes(arr, n, num_steps)
+    if nbytes == 0:
+        raise MbxError('mbx_vcd_batched_workspace_bytes: batch not supported (mixed geometry kinds, psf radius '
+                       'other than 1, or invalid scans)')
+    ws = torch.empty(int(nbytes), dtype=torch.uint8, device=device)
+    plan = MbxBatchedPlan()
+    rc = lib.mbx_vcd_batched_prepare(arr, n, sched.ctypes.data_as(c_void_p), num_steps, int(num_iterations),
+                                     _ptr(step_stats), _ptr(iter_stats), _ptr(ws), int(nbytes), ctypes.byref(plan),
+                                     _stream())
+    _check(rc, 'mbx_vcd_batched_prepare')
+    return plan, ws
+
+
+def vcd_batched_step(plan, step):
+    _check(load_library().mbx_vcd_batched_step(ctypes.byref(plan), int(step), _stream()), 'mbx_vcd_batched_step')
+
+
+def vcd_batched_iteration_stats(plan, iteration):
+    _check(load_library().mbx_vcd_batched_iteration_stats(ctypes.byref(plan), int(iteration), _stream()),
+           'mbx_vcd_batched_iteration_stats')

@@ -37,9 +37,26 @@ static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const fl
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
+    BpArgs A;
+    A.g = g;
+    A.sino = sino;
+    A.wts = w;
+    A.pix = pix;
+    A.num_pixels = n;
+    A.order = nullptr;
+    A.views = views;
+    A.num_views_sel = nv;
+    A.views_per_split = pl.views_per_split;
+    A.coeff_power = cp;
+    A.scale = scale;
+    A.out = dst;
+    A.split_stride = ss;
+    A.out_by_index = 0;
+    A.nsl = pl.nsl;
+    A.npg = pl.npg;
+    A.vc = pl.vc;
     dim3 grid(pl.gx, pl.gy, pl.splits);
-    kern<<<grid, BPF_THREADS, pl.smem, st>>>(g, sino, w, pix, n, views, nv, pl.views_per_split, cp, scale, dst, ss,
-                                             pl.nsl, pl.npg, pl.vc, device_error_ptr());
+    kern<<<grid, BPF_THREADS, pl.smem, st>>>(A, device_error_ptr());
     note_launch();
     return cudaGetLastError();
 }

@@ -106,13 +106,33 @@ __device__ __forceinline__ float bpf_row(const float *__restrict__ row, const fl
     return fmaf(a0, v0, fmaf(a1, v1, a2 * v2));
 }
 
+// Arguments of one back projection (one scan).
+struct BpArgs {
+    mbx_geom g;
+    const float *sino;         // full sinogram (num_views, R, C)
+    const float *wts;          // optional weights, same shape (NULL: ones)
+    const int32_t *pix;        // (num_pixels,) flat pixel indices
+    long long num_pixels;
+    const int32_t *order;      // optional permutation of [0, num_pixels): processing order (locality)
+    const int32_t *views;      // (num_views_sel,) or NULL
+    int num_views_sel, views_per_split, coeff_power;
+    float scale;
+    float *out;                // (num_pixels, S) in list order, or a flat recon when out_by_index
+    long long split_stride;    // 0: final output; else partial-sum workspace stride
+    int out_by_index;
+    int nsl, npg, vc;
+};
+
 template <int KIND>
-__global__ void __launch_bounds__(BPF_THREADS, 3)
-bp_fast_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restrict__ wts,
-               const int32_t *__restrict__ pix, long long num_pixels, const int32_t *__restrict__ views,
-               int num_views_sel, int views_per_split, int coeff_power, float scale, float *__restrict__ dst,
-               long long split_stride, int nsl, int npg, int vc, int *err) {
-    extern __shared__ __align__(16) float smf[];
+__device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf, int *err) {
+    const mbx_geom &g = A.g;
+    const float *__restrict__ sino = A.sino;
+    const float *__restrict__ wts = A.wts;
+    const int32_t *__restrict__ pix = A.pix;
+    const long long num_pixels = A.num_pixels;
+    const int32_t *__restrict__ views = A.views;
+    const int num_views_sel = A.num_views_sel, views_per_split = A.views_per_split, coeff_power = A.coeff_power;
+    const int nsl = A.nsl, npg = A.npg, vc = A.vc;
     const int pcta = 32 * npg;                       // pixels per CTA
     const int nfp = vc * pcta;                       // footprints per chunk
     BpfShared sh;
@@ -132,18 +152,20 @@ bp_fast_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pg = warp / nsl, stl = warp - pg * nsl;
     const int pl = pg * 32 + lane;                                   // pixel within CTA
-    const long long p = (long long)blockIdx.x * pcta + pl;
-    const int s0 = (blockIdx.y * nsl + stl) * BPF_ST;
+    const long long slot = (long long)bx * pcta + pl;
+    const long long p = (A.order && slot < num_pixels) ? A.order[slot] : slot;  // list entry of this thread
+    const int s0 = (by * nsl + stl) * BPF_ST;
     const int num_rows = g.num_det_rows, num_channels = g.num_det_channels, num_slices = g.num_recon_slices;
     const int ns = min(BPF_ST, num_slices - s0);
-    const int split = blockIdx.z;
+    const int split = bz;
     const int v_begin = split * views_per_split;
     const int v_end = min(num_views_sel, v_begin + views_per_split);
     const int npix_grid = g.num_recon_rows * g.num_recon_cols;
 
     // pixel geometry of the pixel this thread computes footprints for (pixel tid % pcta)
     const int fpl = tid % pcta;
-    const long long fp_pixel = (long long)blockIdx.x * pcta + fpl;
+    const long long fp_slot = (long long)bx * pcta + fpl;
+    const long long fp_pixel = (A.order && fp_slot < num_pixels) ? A.order[fp_slot] : fp_slot;
     float fxt = 0.0f, fyt = 0.0f;
     bool fvalid = false;
     if (fp_pixel < num_pixels) {
@@ -151,7 +173,7 @@ bp_fast_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__
         if (idx >= 0 && idx < npix_grid) {
             pixel_tilde(g, idx, fxt, fyt);
             fvalid = true;
-        } else if (blockIdx.y == 0 && split == 0 && tid < pcta) {
+        } else if (by == 0 && split == 0 && tid < pcta) {
             flag_error(err, MBX_ERRFLAG_PIXEL);
         }
     }
@@ -174,7 +196,7 @@ bp_fast_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__
         if (tid < nv) {
             const int vi = views ? views[vb + tid] : vb + tid;
             const bool ok = vi >= 0 && vi < g.num_views;
-            if (!ok && blockIdx.x == 0 && blockIdx.y == 0) flag_error(err, MBX_ERRFLAG_VIEW);
+            if (!ok && bx == 0 && by == 0) flag_error(err, MBX_ERRFLAG_VIEW);
             const float ang = ok ? g.angles[vi] : 0.0f;
             s_vi[tid] = ok ? vi : -1;
             s_cs[tid] = cosf(ang);
@@ -263,13 +285,23 @@ bp_fast_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__
             }
         }
     }
-    if (!active && p >= num_pixels) return;
-    if (ns <= 0) return;
-    float *out = dst + (long long)split * split_stride + p * (long long)num_slices + s0;
-    const float sc = (split_stride == 0) ? scale : 1.0f;
+    if (p >= num_pixels || ns <= 0) return;
+    long long row_of_out = p;
+    if (A.out_by_index) {  // write into a flat recon at the pixel's index (skipped for invalid indices)
+        if (!active) return;
+        row_of_out = pix[p];
+    }
+    float *out = A.out + (long long)split * A.split_stride + row_of_out * (long long)num_slices + s0;
+    const float sc = (A.split_stride == 0) ? A.scale : 1.0f;
 #pragma unroll
     for (int s = 0; s < BPF_ST; ++s)
         if (s < ns) out[s] = active ? sc * acc[s] : 0.0f;
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(BPF_THREADS, 3) bp_fast_kernel(const BpArgs A, int *err) {
+    extern __shared__ __align__(16) float smf[];
+    bp_fast_tile<KIND>(A, blockIdx.x, blockIdx.y, blockIdx.z, smf, err);
 }
 
 inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_views_sel) {

@@ -17,7 +17,7 @@
 
 #include "mbx_common.cuh"
 #include "mbx_host.hpp"
-#include "fp_fast.cuh"
+#include "fp_cb.cuh"
 
 namespace mbx {
 
@@ -207,24 +207,21 @@ static cudaError_t launch_fp_kind(const mbx_geom &g, const FpPlan &pl, const flo
 }
 
 size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel) {
-    const FpfPlan fpl = plan_fp_fast(g, num_pixels, num_views_sel);
-    if (fpl.ok) return fpl.workspace;
+    if (plan_fp_cb(g).ok) return 0;
     return plan_fp(g, num_pixels, num_views_sel).workspace;
 }
 
-static cudaError_t launch_fp_cone_fast(const mbx_geom &g, const FpfPlan &pl, const float *vox, const int32_t *pix,
-                                       long long n, const int32_t *views, int nv, float *dst, long long ss,
-                                       cudaStream_t st) {
+template <int KIND>
+static cudaError_t launch_fp_cb(const FpArgs &A, cudaStream_t st) {
     static bool attr_set = false;
     if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(fp_cone_fast_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
+        cudaError_t e = cudaFuncSetAttribute(fp_cb_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              200 * 1024);
         if (e != cudaSuccess) return e;
         attr_set = true;
     }
-    dim3 grid(nv, pl.tiles, pl.splits), block(pl.bx, pl.by);
-    fp_cone_fast_kernel<<<grid, block, pl.smem, st>>>(g, vox, pix, n, views, dst, pl.mt, pl.c_pad,
-                                                      pl.pixels_per_split, ss, device_error_ptr());
+    dim3 grid(A.num_views_sel, A.plan.cblocks);
+    fp_cb_kernel<KIND><<<grid, CB_THREADS, A.plan.smem, st>>>(A, device_error_ptr());
     note_launch();
     return cudaGetLastError();
 }
@@ -232,20 +229,21 @@ static cudaError_t launch_fp_cone_fast(const mbx_geom &g, const FpfPlan &pl, con
 int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, long long num_pixels,
                     const int32_t *views, int num_views_sel, float *out, void *ws, size_t ws_bytes,
                     cudaStream_t st) {
-    const FpfPlan fpl = plan_fp_fast(g, num_pixels, num_views_sel);
-    if (fpl.ok) {
-        if (fpl.workspace > 0 && (ws == nullptr || ws_bytes < fpl.workspace)) return MBX_ERR_WORKSPACE;
-        float *dst = fpl.splits > 1 ? static_cast<float *>(ws) : out;
-        const long long stride = (long long)num_views_sel * g.num_det_rows * g.num_det_channels;
-        cudaError_t e = launch_fp_cone_fast(g, fpl, vox, pix, num_pixels, views, num_views_sel, dst,
-                                            fpl.splits > 1 ? stride : 0, st);
-        if (e != cudaSuccess) return set_cuda_error(e);
-        if (fpl.splits > 1) {
-            launch_split_sum(dst, stride, fpl.splits, 1.0f, out, stride, st);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return set_cuda_error(e);
-        }
-        return MBX_OK;
+    const CbPlan cpl = plan_fp_cb(g);
+    if (cpl.ok) {
+        FpArgs A;
+        A.g = g;
+        A.vox = vox;
+        A.pix = pix;
+        A.num_pixels = num_pixels;
+        A.views = views;
+        A.num_views_sel = num_views_sel;
+        A.out = out;
+        A.vox_by_index = 0;
+        A.plan = cpl;
+        cudaError_t e = (g.kind == MBX_GEOM_PARALLEL) ? launch_fp_cb<MBX_GEOM_PARALLEL>(A, st)
+                                                       : launch_fp_cb<MBX_GEOM_CONE>(A, st);
+        return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
     }
     const FpPlan pl = plan_fp(g, num_pixels, num_views_sel);
     if (pl.workspace > 0 && (ws == nullptr || ws_bytes < pl.workspace)) return MBX_ERR_WORKSPACE;

@@ -1,0 +1,623 @@
+// Batched VCD: many independent scans of uneven geometry reconstructed together (sm_100a).
+//
+// The per-scan reconstruction is the reference's VCD subset update (tomography_model.py:1343-1542, as in
+// vcd.cu).  Batching replaces one launch per scan per stage with ONE persistent launch per stage for all scans:
+// each stage kernel walks a packed work list -- the concatenation of every scan's tiles, described by
+// per-stage prefix offsets over scans -- with a grid sized to the resident CTAs of the device, and decodes each
+// tile into (scan, local tile) by binary search.  Stages of one subset step:
+//   b_bp      back projection of W*e at each scan's current subset (bp_fast tiles)
+//   b_delta   qGGMRF gradient/Hessian + delta; float64 partials of the prior terms, one per tile
+//   b_fp      forward projection of delta (channel-block tiles of fp_cb)
+//   b_linquad float64 partials of <We, dA> and <W dA, dA> per sinogram tile
+//   b_alpha   one warp per scan: fixed-order sums of that scan's partials -> alpha
+//   b_apply   recon[idx] += alpha*delta, l1 partials
+//   b_error   e -= alpha*dA, then b_l1 folds the l1 partials per scan
+// The subset each scan updates at each step comes from a schedule table in device memory, and every per-(scan,
+// subset) argument record is built once in mbx_vcd_batched_prepare, so the launches of a step depend only on
+// the step number: the whole multi-iteration reconstruction can be captured once in a CUDA graph and replayed.
+#include <algorithm>
+#include <cstring>
+#include <vector>
+
+#include "back_project.cuh"
+#include "bp_fast.cuh"
+#include "fp_cb.cuh"
+#include "mbx_common.cuh"
+#include "mbx_host.hpp"
+#include "mbx_reduce.cuh"
+#include "qggmrf.cuh"
+
+namespace mbx {
+
+constexpr int BT_THREADS = 256;
+constexpr int BT_ELEM_TILE = 2048;   // cylinder elements per tile (delta, apply)
+constexpr int BT_SINO_TILE = 4096;   // sinogram / recon elements per tile (linquad, error, stats)
+constexpr float BT_EPS_F32 = 1.1920928955078125e-07f;
+
+struct VcdScan {
+    float *recon;               // flat (Nr*Nc, S)
+    float *err;                 // (V, R, C)
+    const float *wts;           // (V, R, C) or NULL
+    const float *hess;          // flat (Nr*Nc, S)
+    const int32_t *partition;   // (K, M)
+    float *bp, *delta, *dsino;  // workspace slices
+    long long nsino, nrecon;
+    int K, M, nr, nc, ns;
+    float fm_constant;
+    QParams q;
+};
+
+struct BatchedTables {
+    VcdScan *scans;
+    BpArgs *bpargs;     // [scan][subset]
+    FpArgs *fpargs;     // [scan][subset]
+    int *bp_off, *fp_off, *el_off, *sn_off, *rc_off;  // [num_scans + 1] tile prefix offsets
+    int *fp_cblocks;    // [num_scans]
+    int *bp_gx;         // [num_scans]
+    int *schedule;      // [num_steps][num_scans]
+    double *p_prior, *p_fwd, *p_l1, *p_iter;
+    float *alpha;       // [num_scans]
+    double *step_stats; // [num_steps][num_scans][4]
+    double *iter_stats; // [num_iterations][num_scans][4]
+};
+
+struct BatchedPlanHost {
+    BatchedTables t;
+    int num_scans, kind, num_steps, num_iterations;
+    int bp_total, fp_total, el_total, sn_total, rc_total;
+    int bp_grid, fp_grid, el_grid, sn_grid, rc_grid;
+    size_t bp_smem, fp_smem;
+    int magic;
+};
+static_assert(sizeof(BatchedPlanHost) <= sizeof(mbx_batched_plan), "plan record too large");
+constexpr int BT_MAGIC = 0x6d627862;
+
+__device__ __forceinline__ int find_scan(const int *__restrict__ off, int num_scans, int t) {
+    int lo = 0, hi = num_scans;  // off[lo] <= t < off[hi]
+    while (hi - lo > 1) {
+        const int mid = (lo + hi) >> 1;
+        if (__ldg(off + mid) <= t) lo = mid; else hi = mid;
+    }
+    return lo;
+}
+
+// Sum of NV values over the block into slot[NV * t + i] (fixed order).
+template <int NV>
+__device__ __forceinline__ void tile_reduce(const double (&v)[NV], double *slot) {
+    __shared__ double sh[32][NV];
+    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
+#pragma unroll
+    for (int i = 0; i < NV; ++i) {
+        const double a = warp_sum(v[i]);
+        if (lane == 0) sh[warp][i] = a;
+    }
+    __syncthreads();
+    if (warp == 0) {
+#pragma unroll
+        for (int i = 0; i < NV; ++i) {
+            double a = lane < BT_THREADS / 32 ? sh[lane][i] : 0.0;
+            a = warp_sum(a);
+            if (lane == 0) slot[i] = a;
+        }
+    }
+    __syncthreads();
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(BPF_THREADS, 2) b_bp(BatchedTables T, int num_scans, int step, int total, int *err) {
+    extern __shared__ __align__(16) float smb[];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.bp_off, num_scans, t);
+        const int local = t - __ldg(T.bp_off + s);
+        const int sub = __ldg(T.schedule + step * num_scans + s);
+        const int K = T.scans[s].K;
+        const int gx = __ldg(T.bp_gx + s);
+        bp_fast_tile<KIND>(T.bpargs[s * K + sub], local % gx, local / gx, 0, smb, err);
+    }
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(CB_THREADS, 2) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
+    extern __shared__ __align__(16) float smf2[];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.fp_off, num_scans, t);
+        const int local = t - __ldg(T.fp_off + s);
+        const int sub = __ldg(T.schedule + step * num_scans + s);
+        const int K = T.scans[s].K;
+        const int cbs = __ldg(T.fp_cblocks + s);
+        fp_cb_tile<KIND>(T.fpargs[s * K + sub], local / cbs, local % cbs, smf2, err);
+    }
+}
+
+__global__ void __launch_bounds__(BT_THREADS) b_delta(BatchedTables T, int num_scans, int step, int total, int *err) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.el_off, num_scans, t);
+        const int local = t - __ldg(T.el_off + s);
+        const VcdScan &sc = T.scans[s];
+        const int sub = __ldg(T.schedule + step * num_scans + s);
+        const int32_t *pix = sc.partition + (long long)sub * sc.M;
+        const long long n = (long long)sc.M * sc.ns;
+        const long long e0 = (long long)local * BT_ELEM_TILE;
+        const long long e1 = min(n, e0 + BT_ELEM_TILE);
+        const int npix = sc.nr * sc.nc;
+        double pl = 0.0, pq = 0.0;
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
+            const long long p = i / sc.ns;
+            const int k = (int)(i - p * sc.ns);
+            const int idx = pix[p];
+            float d = 0.0f;
+            if (idx < 0 || idx >= npix) {
+                flag_error(err, MBX_ERRFLAG_PIXEL);
+            } else {
+                float gp, hp;
+                qggmrf_voxel(sc.recon, sc.nr, sc.nc, sc.ns, idx, k, sc.q, gp, hp);
+                const float gf = -sc.fm_constant * sc.bp[i];
+                const float hf = sc.fm_constant * __ldg(sc.hess + (long long)idx * sc.ns + k);
+                d = -((gf + gp) / (hf + hp));
+                pl += (double)(gp * d);
+                pq += (double)(hp * (d * d));
+            }
+            sc.delta[i] = d;
+        }
+        const double v[2] = {pl, pq};
+        tile_reduce<2>(v, T.p_prior + 2 * t);
+    }
+}
+
+__global__ void __launch_bounds__(BT_THREADS) b_linquad(BatchedTables T, int num_scans, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.sn_off, num_scans, t);
+        const int local = t - __ldg(T.sn_off + s);
+        const VcdScan &sc = T.scans[s];
+        const long long e0 = (long long)local * BT_SINO_TILE;
+        const long long e1 = min(sc.nsino, e0 + BT_SINO_TILE);
+        double fl = 0.0, fq = 0.0;
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
+            const float ds = sc.dsino[i], e = sc.err[i];
+            const float w = sc.wts ? sc.wts[i] : 1.0f;
+            fl += (double)((w * e) * ds);
+            fq += (double)(ds * ds * w);
+        }
+        const double v[2] = {fl, fq};
+        tile_reduce<2>(v, T.p_fwd + 2 * t);
+    }
+}
+
+__device__ __forceinline__ double warp_range_sum(const double *__restrict__ p, int b, int e, int nv, int v) {
+    const int lane = threadIdx.x & 31;
+    double s = 0.0;
+    for (int i = b + lane; i < e; i += 32) s += p[(long long)i * nv + v];
+    s = warp_sum(s);
+    return __shfl_sync(0xffffffffu, s, 0);
+}
+
+__global__ void b_alpha(BatchedTables T, int num_scans, int step) {
+    const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (s >= num_scans) return;
+    const VcdScan &sc = T.scans[s];
+    const int eb = __ldg(T.el_off + s), ee = __ldg(T.el_off + s + 1);
+    const int sb = __ldg(T.sn_off + s), se = __ldg(T.sn_off + s + 1);
+    const double pl = warp_range_sum(T.p_prior, eb, ee, 2, 0);
+    const double pq = 0.5 * warp_range_sum(T.p_prior, eb, ee, 2, 1);
+    const double fm = (double)sc.fm_constant;
+    const double fl = fm * warp_range_sum(T.p_fwd, sb, se, 2, 0);
+    const double fq = fm * warp_range_sum(T.p_fwd, sb, se, 2, 1);
+    if ((threadIdx.x & 31) == 0) {
+        const double num = fl - pl, den = fq + pq + (double)BT_EPS_F32;
+        float a = (float)(num / den);
+        a = fminf(fmaxf(a, BT_EPS_F32), 1.5f);
+        if (num != num || den != den) a = nanf("");
+        T.alpha[s] = a;
+        double *st = T.step_stats + ((long long)step * num_scans + s) * 4;
+        st[0] = (double)a;
+        st[2] = num;
+        st[3] = den;
+    }
+}
+
+__global__ void __launch_bounds__(BT_THREADS) b_apply(BatchedTables T, int num_scans, int step, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.el_off, num_scans, t);
+        const int local = t - __ldg(T.el_off + s);
+        const VcdScan &sc = T.scans[s];
+        const int sub = __ldg(T.schedule + step * num_scans + s);
+        const int32_t *pix = sc.partition + (long long)sub * sc.M;
+        const float alpha = T.alpha[s];
+        const long long n = (long long)sc.M * sc.ns;
+        const long long e0 = (long long)local * BT_ELEM_TILE;
+        const long long e1 = min(n, e0 + BT_ELEM_TILE);
+        const int npix = sc.nr * sc.nc;
+        double l1 = 0.0;
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
+            const long long p = i / sc.ns;
+            const int k = (int)(i - p * sc.ns);
+            const int idx = pix[p];
+            if (idx < 0 || idx >= npix) continue;
+            const float d = alpha * sc.delta[i];
+            atomicAdd(sc.recon + (long long)idx * sc.ns + k, d);
+            l1 += (double)fabsf(d);
+        }
+        const double v[1] = {l1};
+        tile_reduce<1>(v, T.p_l1 + t);
+    }
+}
+
+__global__ void __launch_bounds__(BT_THREADS) b_error(BatchedTables T, int num_scans, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.sn_off, num_scans, t);
+        const int local = t - __ldg(T.sn_off + s);
+        const VcdScan &sc = T.scans[s];
+        const float alpha = T.alpha[s];
+        const long long e0 = (long long)local * BT_SINO_TILE;
+        const long long e1 = min(sc.nsino, e0 + BT_SINO_TILE);
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) sc.err[i] -= alpha * sc.dsino[i];
+    }
+}
+
+__global__ void b_l1(BatchedTables T, int num_scans, int step) {
+    const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (s >= num_scans) return;
+    const double l1 = warp_range_sum(T.p_l1, __ldg(T.el_off + s), __ldg(T.el_off + s + 1), 1, 0);
+    if ((threadIdx.x & 31) == 0) T.step_stats[((long long)step * num_scans + s) * 4 + 1] = l1;
+}
+
+// Per-iteration statistics: sum of w e^2, sum of |recon| (the reference's fm_rmse and NMAE inputs).
+__global__ void __launch_bounds__(BT_THREADS) b_iter_partials(BatchedTables T, int num_scans, int total_sn,
+                                                             int total_rc) {
+    for (int t = blockIdx.x; t < total_sn + total_rc; t += gridDim.x) {
+        double a = 0.0;
+        if (t < total_sn) {
+            const int s = find_scan(T.sn_off, num_scans, t);
+            const int local = t - __ldg(T.sn_off + s);
+            const VcdScan &sc = T.scans[s];
+            const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nsino, e0 + BT_SINO_TILE);
+            for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
+                const float e = sc.err[i];
+                const float w = sc.wts ? sc.wts[i] : 1.0f;
+                a += (double)(e * e) * (double)w;
+            }
+        } else {
+            const int tr = t - total_sn;
+            const int s = find_scan(T.rc_off, num_scans, tr);
+            const int local = tr - __ldg(T.rc_off + s);
+            const VcdScan &sc = T.scans[s];
+            const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nrecon, e0 + BT_SINO_TILE);
+            for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) a += (double)fabsf(sc.recon[i]);
+        }
+        const double v[1] = {a};
+        tile_reduce<1>(v, T.p_iter + t);
+    }
+}
+
+__global__ void b_iter_final(BatchedTables T, int num_scans, int iteration, int total_sn) {
+    const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (s >= num_scans) return;
+    const double e2 = warp_range_sum(T.p_iter, __ldg(T.sn_off + s), __ldg(T.sn_off + s + 1), 1, 0);
+    const double ax = warp_range_sum(T.p_iter + total_sn, __ldg(T.rc_off + s), __ldg(T.rc_off + s + 1), 1, 0);
+    if ((threadIdx.x & 31) == 0) {
+        double *st = T.iter_stats + ((long long)iteration * num_scans + s) * 4;
+        st[0] = e2;
+        st[1] = ax;
+        st[2] = 0.0;
+        st[3] = 0.0;
+    }
+}
+
+// ------------------------------------------------------------------------------------------------ host side
+struct ScanSizes {
+    long long ncyl, nsino, nrecon;
+    int bp_tiles, bp_gx, fp_tiles, el_tiles, sn_tiles, rc_tiles;
+    BpfPlan bpp;
+    CbPlan fpp;
+};
+
+static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
+    const mbx_geom &g = sc.geom;
+    int rc = validate_geom(&g);
+    if (rc != MBX_OK) return rc;
+    if (!sc.flat_recon || !sc.error_sinogram || !sc.fm_hessian || !sc.partition) return MBX_ERR_INVALID_ARG;
+    if (sc.num_subsets <= 0 || sc.subset_size <= 0) return MBX_ERR_INVALID_ARG;
+    if (!(sc.qp.sigma_x > 0.0f) || !(sc.qp.T > 0.0f) || !(sc.qp.p > 0.0f)) return MBX_ERR_INVALID_ARG;
+    z.bpp = plan_bp_fast(g, sc.subset_size, g.num_views);
+    z.fpp = plan_fp_cb(g);
+    if (!z.bpp.ok || !z.fpp.ok) return MBX_ERR_UNSUPPORTED;  // batched path needs the radius-1 kernels
+    z.ncyl = (long long)sc.subset_size * g.num_recon_slices;
+    z.nsino = (long long)g.num_views * g.num_det_rows * g.num_det_channels;
+    z.nrecon = (long long)g.num_recon_rows * g.num_recon_cols * g.num_recon_slices;
+    z.bp_gx = z.bpp.gx;
+    z.bp_tiles = z.bpp.gx * z.bpp.gy;
+    z.fp_tiles = g.num_views * z.fpp.cblocks;
+    z.el_tiles = (int)((z.ncyl + BT_ELEM_TILE - 1) / BT_ELEM_TILE);
+    z.sn_tiles = (int)((z.nsino + BT_SINO_TILE - 1) / BT_SINO_TILE);
+    z.rc_tiles = (int)((z.nrecon + BT_SINO_TILE - 1) / BT_SINO_TILE);
+    return MBX_OK;
+}
+
+struct Layout {
+    size_t scans, bpargs, fpargs, offs, cblocks, gx, sched, p_prior, p_fwd, p_l1, p_iter, alpha, bufs, total;
+    int bp_total, fp_total, el_total, sn_total, rc_total;
+    std::vector<size_t> buf_off;  // per scan: bp, delta, dsino
+};
+
+static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::vector<ScanSizes> &zs) {
+    zs.resize(n);
+    L.bp_total = L.fp_total = L.el_total = L.sn_total = L.rc_total = 0;
+    int kind = -1, ksum = 0;
+    for (int s = 0; s < n; ++s) {
+        int rc = scan_sizes(scans[s], zs[s]);
+        if (rc != MBX_OK) return rc;
+        if (kind >= 0 && scans[s].geom.kind != kind) return MBX_ERR_UNSUPPORTED;  // one geometry kind per batch
+        if (scans[s].num_subsets != scans[0].num_subsets) return MBX_ERR_UNSUPPORTED;  // argument table is [scan][K]
+        kind = scans[s].geom.kind;
+        L.bp_total += zs[s].bp_tiles;
+        L.fp_total += zs[s].fp_tiles;
+        L.el_total += zs[s].el_tiles;
+        L.sn_total += zs[s].sn_tiles;
+        L.rc_total += zs[s].rc_tiles;
+        ksum += scans[s].num_subsets;
+    }
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += align256(bytes); return o; };
+    L.scans = take(sizeof(VcdScan) * n);
+    L.bpargs = take(sizeof(BpArgs) * ksum);
+    L.fpargs = take(sizeof(FpArgs) * ksum);
+    L.offs = take(sizeof(int) * 5 * (n + 1));
+    L.cblocks = take(sizeof(int) * n);
+    L.gx = take(sizeof(int) * n);
+    L.sched = take(sizeof(int) * (size_t)num_steps * n);
+    L.p_prior = take(sizeof(double) * 2 * (size_t)L.el_total);
+    L.p_fwd = take(sizeof(double) * 2 * (size_t)L.sn_total);
+    L.p_l1 = take(sizeof(double) * (size_t)L.el_total);
+    L.p_iter = take(sizeof(double) * ((size_t)L.sn_total + L.rc_total));
+    L.alpha = take(sizeof(float) * n);
+    L.buf_off.resize(3 * (size_t)n);
+    for (int s = 0; s < n; ++s) {
+        L.buf_off[3 * s] = take(4 * (size_t)zs[s].ncyl);
+        L.buf_off[3 * s + 1] = take(4 * (size_t)zs[s].ncyl);
+        L.buf_off[3 * s + 2] = take(4 * (size_t)zs[s].nsino);
+    }
+    L.total = off;
+    return MBX_OK;
+}
+
+template <typename K>
+static int occupancy_grid(K kern, size_t smem, int total) {
+    int per_sm = 0;
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT_THREADS, smem) != cudaSuccess || per_sm < 1) {
+        cudaGetLastError();
+        per_sm = 1;
+    }
+    const long long g = (long long)per_sm * num_sms();
+    return (int)std::max(1LL, std::min<long long>(g, total));
+}
+
+}  // namespace mbx
+
+using namespace mbx;
+
+extern "C" size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps) {
+    if (!scans || num_scans <= 0 || num_steps <= 0) return 0;
+    Layout L;
+    std::vector<ScanSizes> zs;
+    if (layout(scans, num_scans, num_steps, L, zs) != MBX_OK) return 0;
+    return L.total;
+}
+
+extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans, const int32_t *schedule,
+                                       int32_t num_steps, int32_t num_iterations, double *step_stats,
+                                       double *iter_stats, void *workspace, size_t workspace_bytes,
+                                       mbx_batched_plan *plan_out, void *stream) {
+    if (!scans || num_scans <= 0 || !schedule || num_steps <= 0 || num_iterations < 0 || !plan_out || !step_stats ||
+        (num_iterations > 0 && !iter_stats))
+        return MBX_ERR_INVALID_ARG;
+    Layout L;
+    std::vector<ScanSizes> zs;
+    int rc = layout(scans, num_scans, num_steps, L, zs);
+    if (rc != MBX_OK) return rc;
+    if (!workspace || workspace_bytes < L.total) return MBX_ERR_WORKSPACE;
+    for (int st = 0; st < num_steps; ++st)
+        for (int s = 0; s < num_scans; ++s) {
+            const int v = schedule[(size_t)st * num_scans + s];
+            if (v < 0 || v >= scans[s].num_subsets) return MBX_ERR_INVALID_ARG;
+        }
+    char *base = static_cast<char *>(workspace);
+    std::vector<char> host(L.sched + sizeof(int) * (size_t)num_steps * num_scans, 0);
+    VcdScan *hs = reinterpret_cast<VcdScan *>(host.data() + L.scans);
+    BpArgs *hb = reinterpret_cast<BpArgs *>(host.data() + L.bpargs);
+    FpArgs *hf = reinterpret_cast<FpArgs *>(host.data() + L.fpargs);
+    int *hoff = reinterpret_cast<int *>(host.data() + L.offs);
+    int *hcb = reinterpret_cast<int *>(host.data() + L.cblocks);
+    int *hgx = reinterpret_cast<int *>(host.data() + L.gx);
+    int *hsched = reinterpret_cast<int *>(host.data() + L.sched);
+    const int n1 = num_scans + 1;
+    int *o_bp = hoff, *o_fp = hoff + n1, *o_el = hoff + 2 * n1, *o_sn = hoff + 3 * n1, *o_rc = hoff + 4 * n1;
+    o_bp[0] = o_fp[0] = o_el[0] = o_sn[0] = o_rc[0] = 0;
+    size_t smem_bp = 0, smem_fp = 0;
+    int ki = 0;
+    for (int s = 0; s < num_scans; ++s) {
+        const mbx_scan &sc = scans[s];
+        const ScanSizes &z = zs[s];
+        VcdScan &v = hs[s];
+        v.recon = sc.flat_recon;
+        v.err = sc.error_sinogram;
+        v.wts = sc.weights;
+        v.hess = sc.fm_hessian;
+        v.partition = sc.partition;
+        v.bp = reinterpret_cast<float *>(base + L.buf_off[3 * s]);
+        v.delta = reinterpret_cast<float *>(base + L.buf_off[3 * s + 1]);
+        v.dsino = reinterpret_cast<float *>(base + L.buf_off[3 * s + 2]);
+        v.nsino = z.nsino;
+        v.nrecon = z.nrecon;
+        v.K = sc.num_subsets;
+        v.M = sc.subset_size;
+        v.nr = sc.geom.num_recon_rows;
+        v.nc = sc.geom.num_recon_cols;
+        v.ns = sc.geom.num_recon_slices;
+        v.fm_constant = sc.fm_constant;
+        v.q = make_qparams(sc.qp);
+        for (int k = 0; k < sc.num_subsets; ++k, ++ki) {
+            BpArgs &a = hb[ki];
+            a.g = sc.geom;
+            a.sino = sc.error_sinogram;
+            a.wts = sc.weights;
+            a.pix = sc.partition + (size_t)k * sc.subset_size;
+            a.num_pixels = sc.subset_size;
+            a.order = sc.partition_order ? sc.partition_order + (size_t)k * sc.subset_size : nullptr;
+            a.views = nullptr;
+            a.num_views_sel = sc.geom.num_views;
+            a.views_per_split = sc.geom.num_views;
+            a.coeff_power = 1;
+            a.scale = 1.0f;
+            a.out = v.bp;
+            a.split_stride = 0;
+            a.out_by_index = 0;
+            a.nsl = z.bpp.nsl;
+            a.npg = z.bpp.npg;
+            a.vc = z.bpp.vc;
+            FpArgs &f = hf[ki];
+            f.g = sc.geom;
+            f.vox = v.delta;
+            f.pix = a.pix;
+            f.num_pixels = sc.subset_size;
+            f.views = nullptr;
+            f.num_views_sel = sc.geom.num_views;
+            f.out = v.dsino;
+            f.vox_by_index = 0;
+            f.plan = z.fpp;
+        }
+        // bp_fast smem without view splits
+        smem_bp = std::max(smem_bp, z.bpp.smem);
+        smem_fp = std::max(smem_fp, z.fpp.smem);
+        hcb[s] = z.fpp.cblocks;
+        hgx[s] = z.bp_gx;
+        o_bp[s + 1] = o_bp[s] + z.bp_tiles;
+        o_fp[s + 1] = o_fp[s] + z.fp_tiles;
+        o_el[s + 1] = o_el[s] + z.el_tiles;
+        o_sn[s + 1] = o_sn[s] + z.sn_tiles;
+        o_rc[s + 1] = o_rc[s] + z.rc_tiles;
+    }
+    std::memcpy(hsched, schedule, sizeof(int) * (size_t)num_steps * num_scans);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    cudaError_t e = cudaMemcpyAsync(base, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_cuda_error(e);
+
+    BatchedPlanHost P;
+    std::memset(&P, 0, sizeof(P));
+    P.t.scans = reinterpret_cast<VcdScan *>(base + L.scans);
+    P.t.bpargs = reinterpret_cast<BpArgs *>(base + L.bpargs);
+    P.t.fpargs = reinterpret_cast<FpArgs *>(base + L.fpargs);
+    int *doff = reinterpret_cast<int *>(base + L.offs);
+    P.t.bp_off = doff;
+    P.t.fp_off = doff + n1;
+    P.t.el_off = doff + 2 * n1;
+    P.t.sn_off = doff + 3 * n1;
+    P.t.rc_off = doff + 4 * n1;
+    P.t.fp_cblocks = reinterpret_cast<int *>(base + L.cblocks);
+    P.t.bp_gx = reinterpret_cast<int *>(base + L.gx);
+    P.t.schedule = reinterpret_cast<int *>(base + L.sched);
+    P.t.p_prior = reinterpret_cast<double *>(base + L.p_prior);
+    P.t.p_fwd = reinterpret_cast<double *>(base + L.p_fwd);
+    P.t.p_l1 = reinterpret_cast<double *>(base + L.p_l1);
+    P.t.p_iter = reinterpret_cast<double *>(base + L.p_iter);
+    P.t.alpha = reinterpret_cast<float *>(base + L.alpha);
+    P.t.step_stats = step_stats;
+    P.t.iter_stats = iter_stats;
+    P.num_scans = num_scans;
+    P.kind = scans[0].geom.kind;
+    P.num_steps = num_steps;
+    P.num_iterations = num_iterations;
+    P.bp_total = L.bp_total;
+    P.fp_total = L.fp_total;
+    P.el_total = L.el_total;
+    P.sn_total = L.sn_total;
+    P.rc_total = L.rc_total;
+    P.bp_smem = smem_bp;
+    P.fp_smem = smem_fp;
+    // kernel attributes and resident-CTA grids
+    if (P.kind == MBX_GEOM_PARALLEL) {
+        cudaFuncSetAttribute(b_bp<MBX_GEOM_PARALLEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        cudaFuncSetAttribute(b_fp<MBX_GEOM_PARALLEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, smem_bp, L.bp_total);
+        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_PARALLEL>, smem_fp, L.fp_total);
+    } else {
+        cudaFuncSetAttribute(b_bp<MBX_GEOM_CONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
+        cudaFuncSetAttribute(b_fp<MBX_GEOM_CONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_CONE>, smem_bp, L.bp_total);
+        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_CONE>, smem_fp, L.fp_total);
+    }
+    {   // load every stage kernel now (lazy module loading must not happen inside a stream capture)
+        cudaFuncAttributes fa;
+        cudaFuncGetAttributes(&fa, b_delta);
+        cudaFuncGetAttributes(&fa, b_linquad);
+        cudaFuncGetAttributes(&fa, b_alpha);
+        cudaFuncGetAttributes(&fa, b_apply);
+        cudaFuncGetAttributes(&fa, b_error);
+        cudaFuncGetAttributes(&fa, b_l1);
+        cudaFuncGetAttributes(&fa, b_iter_partials);
+        cudaFuncGetAttributes(&fa, b_iter_final);
+        device_error_ptr();
+    }
+    P.el_grid = occupancy_grid(b_delta, 0, L.el_total);
+    P.sn_grid = occupancy_grid(b_linquad, 0, L.sn_total);
+    P.rc_grid = occupancy_grid(b_iter_partials, 0, L.sn_total + L.rc_total);
+    e = cudaGetLastError();
+    if (e != cudaSuccess) return set_cuda_error(e);
+    P.magic = BT_MAGIC;
+    std::memset(plan_out, 0, sizeof(*plan_out));
+    std::memcpy(plan_out, &P, sizeof(P));
+    return MBX_OK;
+}
+
+static const BatchedPlanHost *plan_of(const mbx_batched_plan *p) {
+    if (!p) return nullptr;
+    const BatchedPlanHost *P = reinterpret_cast<const BatchedPlanHost *>(p);
+    return P->magic == BT_MAGIC ? P : nullptr;
+}
+
+extern "C" int mbx_vcd_batched_step(const mbx_batched_plan *plan, int32_t step, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P || step < 0 || step >= P->num_steps) return MBX_ERR_INVALID_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    int *err = device_error_ptr();
+    const BatchedTables &T = P->t;
+    const int n = P->num_scans;
+    const int warp_blocks = (n + 7) / 8;
+    if (P->kind == MBX_GEOM_PARALLEL)
+        b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
+    else
+        b_bp<MBX_GEOM_CONE><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
+    note_launch();
+    b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err);
+    note_launch();
+    if (P->kind == MBX_GEOM_PARALLEL)
+        b_fp<MBX_GEOM_PARALLEL><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+    else
+        b_fp<MBX_GEOM_CONE><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+    note_launch();
+    b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
+    note_launch();
+    b_alpha<<<warp_blocks, 256, 0, st>>>(T, n, step);
+    note_launch();
+    b_apply<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total);
+    note_launch();
+    b_error<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
+    note_launch();
+    b_l1<<<warp_blocks, 256, 0, st>>>(T, n, step);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+}
+
+extern "C" int mbx_vcd_batched_iteration_stats(const mbx_batched_plan *plan, int32_t iteration, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P || iteration < 0 || iteration >= P->num_iterations) return MBX_ERR_INVALID_ARG;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const int n = P->num_scans;
+    b_iter_partials<<<P->rc_grid, BT_THREADS, 0, st>>>(P->t, n, P->sn_total, P->rc_total);
+    note_launch();
+    b_iter_final<<<(n + 7) / 8, 256, 0, st>>>(P->t, n, iteration, P->sn_total);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+}

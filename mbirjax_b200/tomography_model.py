@@ -296,33 +296,12 @@ class TomographyModel(ParameterHandler):
             raise NotImplementedError('prox_map is not on the mbirjax_b200 hot path')
         if self.get_params('positivity_flag'):
             raise NotImplementedError('positivity_flag=True is not on the mbirjax_b200 hot path')
+        state = self._vcd_setup(sinogram, weights, init_recon)
         recon_shape = self.get_params('recon_shape')
-        num_slices = recon_shape[2]
-        dev = self._device()
-        sino = self._dev(sinogram)
-        w = None if weights is None else self._dev(weights)
-        if init_recon is None:
-            init = self.direct_recon(sino)
-        elif isinstance(init_recon, int) and init_recon == 0:
-            init = torch.zeros(recon_shape, dtype=torch.float32, device=dev)
-        else:
-            init = self._dev(init_recon)
-        if tuple(init.shape) != tuple(recon_shape):
-            raise ValueError('init_recon does not have the correct shape. \nExpected {}, but got shape {} for '
-                             'init_recon shape.'.format(recon_shape, tuple(init.shape)))
-        # alpha minimising (1/2)||y - alpha A x||_W^2 (tomography_model.py:1137-1152)
-        error_sinogram = self.forward_project(init)
-        wes = error_sinogram if w is None else w * error_sinogram
-        norm = float(torch.sum(wes.double() * error_sinogram.double()))
-        alpha = float(torch.sum(wes.double() * sino.double())) / norm if norm > 0 else 1.0
-        error_sinogram = (sino - np.float32(alpha) * error_sinogram).contiguous()
-        flat_recon = (np.float32(alpha) * init).reshape((-1, num_slices)).contiguous()
-        del wes
-        sigma_y = float(self.get_params('sigma_y'))
-        fm_hessian = self.compute_hessian_diagonal(weights=w).reshape((-1, num_slices)).contiguous()
-        fm_constant = 1.0 / (sigma_y ** 2.0)
-        b, sigma_x, p, q, T = self._qggmrf_params()
-        qp = _capi.qggmrf_params(b, sigma_x, p, q, T)
+        dev = state['device']
+        w, flat_recon, error_sinogram = state['weights'], state['flat_recon'], state['error_sinogram']
+        fm_hessian, fm_constant, qp, sigma_y = (state['fm_hessian'], state['fm_constant'], state['qp'],
+                                                state['sigma_y'])
         geom = self._geometry()
         dev_partitions = [torch.as_tensor(part, device=dev, dtype=torch.int32).contiguous() for part in partitions]
         workspaces = {}
@@ -360,6 +339,38 @@ class TomographyModel(ParameterHandler):
         self.last_error_sinogram = error_sinogram
         return flat_recon.reshape(recon_shape), (fm_rmse[:num_iters], pm_loss[:num_iters], nmae_update[:num_iters],
                                                  alpha_values[:num_iters])
+
+    def _vcd_setup(self, sinogram, weights=None, init_recon=None):
+        """Device state for VCD iterations (tomography_model.py:1110-1192): initial recon (direct recon when
+        init_recon is None), alpha-rescaled error sinogram, Hessian diagonal, fm constant and qGGMRF record."""
+        recon_shape = self.get_params('recon_shape')
+        num_slices = recon_shape[2]
+        dev = self._device()
+        sino = self._dev(sinogram)
+        w = None if weights is None else self._dev(weights)
+        if init_recon is None:
+            init = self.direct_recon(sino)
+        elif isinstance(init_recon, int) and init_recon == 0:
+            init = torch.zeros(recon_shape, dtype=torch.float32, device=dev)
+        else:
+            init = self._dev(init_recon)
+        if tuple(init.shape) != tuple(recon_shape):
+            raise ValueError('init_recon does not have the correct shape. \nExpected {}, but got shape {} for '
+                             'init_recon shape.'.format(recon_shape, tuple(init.shape)))
+        # alpha minimising (1/2)||y - alpha A x||_W^2 (tomography_model.py:1137-1152)
+        error_sinogram = self.forward_project(init)
+        wes = error_sinogram if w is None else w * error_sinogram
+        norm = float(torch.sum(wes.double() * error_sinogram.double()))
+        alpha = float(torch.sum(wes.double() * sino.double())) / norm if norm > 0 else 1.0
+        error_sinogram = (sino - np.float32(alpha) * error_sinogram).contiguous()
+        flat_recon = (np.float32(alpha) * init).reshape((-1, num_slices)).contiguous()
+        del wes
+        sigma_y = float(self.get_params('sigma_y'))
+        fm_hessian = self.compute_hessian_diagonal(weights=w).reshape((-1, num_slices)).contiguous()
+        b, sigma_x, p, q, T = self._qggmrf_params()
+        return {'device': dev, 'weights': w, 'flat_recon': flat_recon, 'error_sinogram': error_sinogram,
+                'fm_hessian': fm_hessian, 'fm_constant': 1.0 / (sigma_y ** 2.0), 'sigma_y': sigma_y,
+                'qp': _capi.qggmrf_params(b, sigma_x, p, q, T)}
 
     # ------------------------------------------------------------------ misc reference helpers
     def gen_weights(self, sinogram, weight_type):

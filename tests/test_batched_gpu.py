@@ -1,0 +1,74 @@
+"""Batched VCD (persistent work-list kernels over many scans, all iterations in one CUDA graph) against the
+plain per-scan path and the oracle: same partitions, subset orders and qGGMRF parameters."""
+import numpy as np
+import pytest
+import torch
+
+import mbirjax_b200 as mb
+from mbirjax_b200.batched import BatchedVCD, morton_order
+from mbirjax_b200.utilities import gen_ellipsoid_phantom
+import oracle as O
+from cases import rel_l2
+
+pytestmark = pytest.mark.gpu
+
+
+def _scan(kind, views, rows, channels, seed):
+    ang = np.linspace(0, np.pi if kind == 'parallel' else 2 * np.pi, views, endpoint=False).astype(np.float32)
+    if kind == 'parallel':
+        model = mb.ParallelBeamModel((views, rows, channels), ang)
+        geom = O.parallel_geometry((views, rows, channels), ang)
+    else:
+        model = mb.ConeBeamModel((views, rows, channels), ang, 4.0 * channels, 4.0 * channels)
+        geom = O.cone_geometry((views, rows, channels), ang, 4.0 * channels, 4.0 * channels)
+    model.set_params(sharpness=0.0, granularity=[4], partition_sequence=[0], verbose=0)
+    ph = gen_ellipsoid_phantom(geom.recon_shape, 5, seed).numpy()
+    np.random.seed(seed)
+    sino = O.forward_project(geom, ph)
+    sino = (sino + np.random.default_rng(seed).normal(0, 0.01 * np.abs(sino).max(), sino.shape)).astype(np.float32)
+    return model, geom, sino
+
+
+def _plain(model, sino, seed, iters, w=None):
+    np.random.seed(seed)
+    rec, d = model.recon(sino, weights=w, max_iterations=iters, stop_threshold_change_pct=0, logfile_path=None,
+                         print_logs=False)
+    return rec.cpu().numpy(), d
+
+
+@pytest.mark.parametrize('use_graph', [True, False])
+def test_batched_matches_plain_and_oracle(cuda, use_graph):
+    shapes = [(40, 6, 48), (23, 9, 37), (61, 4, 64)]
+    seeds = [3, 4, 5]
+    items = [_scan('parallel', v, r, c, sd) for (v, r, c), sd in zip(shapes, seeds)]
+    models = [it[0] for it in items]
+    sinos = [it[2] for it in items]
+    recons, dicts = BatchedVCD(models, sinos, seeds=seeds).recon(max_iterations=4, use_graph=use_graph)
+    for (model, geom, sino), rec, d, sd in zip(items, recons, dicts, seeds):
+        plain, pd = _plain(model, sino, sd, 4)
+        assert rel_l2(rec.cpu().numpy(), plain) <= 1e-5
+        np.testing.assert_allclose(d['fm_rmse'], pd['recon_params']['fm_rmse'], rtol=1e-4)
+        np.testing.assert_allclose(d['alpha_values'], pd['recon_params']['alpha_values'], rtol=1e-4)
+    # one scan against the oracle
+    model, geom, sino = items[0]
+    np.random.seed(seeds[0])
+    ref, _ = O.vcd.recon(geom, sino, granularity=[4], partition_sequence=[0], max_iterations=4, sharpness=0.0,
+                         stop_threshold_change_pct=0)
+    assert rel_l2(recons[0].cpu().numpy(), ref) <= 1e-4
+
+
+def test_batched_cone_with_weights(cuda):
+    items = [_scan('cone', 24, 6, 32, 7), _scan('cone', 30, 8, 28, 8)]
+    models = [it[0] for it in items]
+    sinos = [it[2] for it in items]
+    ws = [np.exp(-s / s.max()).astype(np.float32) for s in sinos]
+    recons, dicts = BatchedVCD(models, sinos, weights=ws, seeds=[7, 8]).recon(max_iterations=3)
+    for (model, geom, sino), w, rec, sd in zip(items, ws, recons, [7, 8]):
+        plain, _ = _plain(model, sino, sd, 3, w)
+        assert rel_l2(rec.cpu().numpy(), plain) <= 1e-5
+
+
+def test_morton_order_is_a_permutation():
+    idx = np.sort(np.random.default_rng(0).choice(64 * 64, 500, replace=False)).astype(np.int32)
+    o = morton_order(idx, 64)
+    assert sorted(o.tolist()) == list(range(500))
