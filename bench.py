@@ -1,21 +1,28 @@
 #!/usr/bin/env python
 """Benchmark of the MBIR hot path on B200.
 
-Workload (default ``--workload cone``): plain cone-beam VCD on one scan -- sinogram 256 views x 128 rows x 256
-channels (views uniform on [0, 2pi)), source_detector_dist = source_iso_dist = 1024, unit detector pitch, recon
-256x256x128 (auto size), forward-projected from 20 seeded random ellipsoids (seed 1) with 1% Gaussian noise,
-qGGMRF p=2, q=1.2, T=1, sharpness 0, 4 pixel subsets, 20 VCD iterations with FDK initialisation.
-A step is one full ``ConeBeamModel.recon`` of that scan; the value is recons/s.
+Default workload (``--workload batched``): 24 independent parallel-beam scans of uneven geometry.  Scan i (seed i)
+draws views U{60..720} on [0, pi), det_rows U{8..64} and det_channels U{96..512}; its volume is channels x
+channels x rows holding 10 seeded random ellipsoids (centres in the inner 70%, semi-axes U[5,40] voxels,
+densities U[0.1,1], summed where they overlap), forward-projected with 1% Gaussian noise; qGGMRF p=2, q=1.2, T=1,
+sharpness 0, 4 pixel subsets, 10 VCD iterations with FBP initialisation.  A step is one reconstruction of all 24
+scans; the value is recons/s of the batched path (``mbirjax_b200.batched.BatchedVCD``: one persistent work-list
+kernel per stage over all scans, all iterations in one CUDA graph).  The same line reports the plain per-scan GPU
+path (``ParallelBeamModel.recon`` scan after scan) measured the same way, and their ratio.
+
+``--workload cone``: plain cone-beam VCD on one scan (256 views x 128 rows x 256 channels, sdd = sid = 1024,
+recon 256x256x128 from 20 ellipsoids, 20 iterations x 4 subsets, FDK init).
 
 Synthetic data stands in for measured scans (the reference publishes no benchmark dataset).
 Timing: W untimed warm-up steps, then exactly K steps between barriers + device synchronisations, timed with
-CUDA events on the launching stream; max over ranks.  The recon working set (about 70 MB) fits in L2, so L2 is
-flushed (a 256 MB write) before every step, inside the timed region.  SM clocks and throttle reasons are
-sampled with nvidia-smi during the timed region.  ``e2e`` repeats the measurement through the public API with
-the sinogram in pinned host memory and the recon copied back each step.  ``roofline`` times the dominant
-kernels (one VCD subset's back projection and forward projection) with CUDA events and divides their
-algorithmic bytes by the measured HBM copy bandwidth.  ``cpu_baseline`` times the oracle's restatement of the
-reference arithmetic on all host cores for one subset update and scales it to one recon.
+CUDA events on the launching stream; max over ranks.  L2 is flushed (a 256 MB write) before every step, inside
+the timed region (the batched inputs, about 1 GB, exceed L2 anyway).  SM clocks and throttle reasons are sampled
+with nvidia-smi during the timed region.  ``e2e`` repeats the measurement through the public API with the
+sinograms in pinned host memory and the recons copied back each step.  ``roofline`` times the dominant kernels
+(the back- and forward-projection stages of a subset update) live with CUDA events and divides their algorithmic
+bytes, 4 (V N S + V R C) summed over scans, by the measured HBM copy bandwidth.  ``cpu_baseline`` times the
+oracle's restatement of the reference arithmetic on all host cores for one subset update of one scan and scales
+it by the same work model to the whole workload.
 
 ``--impl reference`` times the reference arithmetic (the oracle port: JAX is not installable offline, so the
 reference's own JAX CPU path cannot run) on the host cores on the same workload and metric.
@@ -40,6 +47,7 @@ if ROOT not in sys.path:
 METRIC = 'batched vs plain recons/s at 1e-4 NRMSE; proj HBM GB/s; autograd/fwd time'
 CONE = dict(views=256, rows=128, channels=256, sdd=1024.0, sid=1024.0, ellipsoids=20, seed=1, subsets=4,
             iterations=20)
+BATCH = dict(num_scans=24, ellipsoids=10, subsets=4, iterations=10, cpu_sample_scan=0)
 
 
 def parse_args():
@@ -48,7 +56,7 @@ def parse_args():
     ap.add_argument('--steps', type=int, default=5)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='mbirjax_b200', choices=['mbirjax_b200', 'reference'])
-    ap.add_argument('--workload', default='cone', choices=['cone'])
+    ap.add_argument('--workload', default='batched', choices=['batched', 'cone'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     return ap.parse_args()
@@ -170,6 +178,115 @@ def recon_once(model, sino):
     return rec
 
 
+def build_batched_workload(device):
+    import mbirjax_b200 as mb
+    from mbirjax_b200.utilities import gen_ellipsoid_phantom, add_noise, batched_scan_shapes, uniform_angles
+    models, sinos = [], []
+    for i, (v, r, c) in enumerate(batched_scan_shapes(BATCH['num_scans'])):
+        model = mb.ParallelBeamModel((v, r, c), uniform_angles(v))
+        model.set_params(sharpness=0.0, snr_db=30.0, granularity=[BATCH['subsets']], partition_sequence=[0],
+                         verbose=0)
+        phantom = gen_ellipsoid_phantom(model.get_params('recon_shape'), BATCH['ellipsoids'], i, device=device)
+        np.random.seed(i)
+        sinos.append(add_noise(model.forward_project(phantom), 0.01, i).contiguous())
+        models.append(model)
+        del phantom
+    return models, sinos
+
+
+def batched_recon(models, sinos):
+    from mbirjax_b200.batched import BatchedVCD
+    recons, _ = BatchedVCD(models, sinos, seeds=list(range(len(models)))).recon(max_iterations=BATCH['iterations'])
+    return recons
+
+
+def plain_recon(models, sinos):
+    recons = []
+    for i, (model, sino) in enumerate(zip(models, sinos)):
+        np.random.seed(i)
+        rec, _ = model.recon(sino, max_iterations=BATCH['iterations'], stop_threshold_change_pct=0,
+                             logfile_path=None, print_logs=False)
+        recons.append(rec)
+    return recons
+
+
+def batched_roofline(models, sinos, peak_gbs, peak_kind):
+    """Average duration of the batched back- and forward-projection stages (CUDA events, 4 subset steps)."""
+    import torch
+    from mbirjax_b200 import _capi
+    from mbirjax_b200.batched import BatchedVCD
+    b = BatchedVCD(models, sinos, seeds=list(range(len(models))))
+    scans, sched = b._setup(1)
+    dev = b.states[0]['device']
+    n = len(scans)
+    step_stats = torch.zeros((sched.shape[0], n, 4), dtype=torch.float64, device=dev)
+    iter_stats = torch.zeros((1, n, 4), dtype=torch.float64, device=dev)
+    plan, ws = _capi.vcd_batched_prepare(scans, sched, 1, step_stats, iter_stats, dev)
+    times = {k: 0.0 for k in _capi.BATCHED_STAGES}
+    for step in range(sched.shape[0]):
+        for stage, name in enumerate(_capi.BATCHED_STAGES):
+            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+            s.record()
+            _capi.vcd_batched_stage(plan, step, stage)
+            e.record()
+            torch.cuda.synchronize()
+            times[name] += s.elapsed_time(e)
+    steps = sched.shape[0]
+    alg = 0.0
+    for m, sc in zip(models, scans):
+        V, R, C = m.get_params('sinogram_shape')
+        S = m.get_params('recon_shape')[2]
+        alg += 4.0 * (V * sc.subset_size * S + V * R * C)
+    res = {}
+    for name in ('bp', 'fp'):
+        ms = times[name] / steps
+        res[name] = {'ms': ms, 'gbs': alg / (ms * 1e-3) / 1e9}
+    dom = max(res, key=lambda k: res[k]['ms'])
+    traffic = profile_traffic('b_' + dom)
+    share = {k: round(v / sum(times.values()), 4) for k, v in times.items()}
+    return {'kernel': 'b_' + dom, 'bound': 'hbm', 'achieved': round(res[dom]['gbs'], 1), 'peak': peak_gbs,
+            'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': round(res[dom]['gbs'] / peak_gbs, 4),
+            'traffic': traffic, 'launch_ms': round(res[dom]['ms'], 4), 'alg_bytes_per_launch': alg,
+            'other': {'b_' + k: {'launch_ms': round(v['ms'], 4), 'achieved_gbs': round(v['gbs'], 1)}
+                      for k, v in res.items() if k != dom},
+            'stage_time_share': share}
+
+
+def cpu_batched_sample(workers=None):
+    """One VCD subset update of one scan of the batch with the oracle on all host cores; returns
+    (seconds, cores, scale) where scale converts it to the whole workload by the 4(VNS + VRC) work model."""
+    import oracle as O
+    from oracle.pool import OraclePool, vcd_subset_update_pooled
+    from mbirjax_b200.utilities import batched_scan_shapes, uniform_angles
+    shapes = batched_scan_shapes(BATCH['num_scans'])
+
+    def work(v, r, c):
+        m = int(np.ceil(np.sum(O.get_2d_ror_mask((c, c, r))) / BATCH['subsets']))
+        return v * (m * r + r * c)
+
+    i = BATCH['cpu_sample_scan']
+    v, r, c = shapes[i]
+    geom = O.parallel_geometry((v, r, c), uniform_angles(v))
+    nr, nc, ns = geom.recon_shape
+    rng = np.random.default_rng(0)
+    flat = rng.random((nr * nc, ns)).astype(np.float32) * 0.1
+    err = rng.standard_normal(geom.sinogram_shape).astype(np.float32)
+    hess = np.full((nr * nc, ns), 1000.0, dtype=np.float32)
+    np.random.seed(i)
+    subset = O.gen_pixel_partition(geom.recon_shape, BATCH['subsets'])[0]
+    params = (O.get_b_from_nbr_wts([1, 1, 1]), 0.05, 2.0, 1.2, 1.0)
+    pool = OraclePool(geom, workers)
+    try:
+        vcd_subset_update_pooled(pool, flat, err, None, hess, subset[:256], 100.0, params)  # start workers
+        t0 = time.perf_counter()
+        vcd_subset_update_pooled(pool, flat, err, None, hess, subset, 100.0, params)
+        dt = time.perf_counter() - t0
+    finally:
+        pool.close()
+    scale = sum(work(*sh) for sh in shapes) / work(v, r, c) * BATCH['subsets'] * BATCH['iterations']
+    return dt, pool.workers, scale
+
+
 def timed_steps(step_fn, steps, warmup, world, flush):
     import torch
     for _ in range(warmup):
@@ -275,30 +392,11 @@ def cpu_recons_per_s(subset_seconds):
 
 
 # ----------------------------------------------------------------------------------------------- arms
-def run_reference(args):
-    world = int(os.environ.get('WORLD_SIZE', '1'))
-    rank = int(os.environ.get('RANK', '0'))
-    if rank != 0:
-        return
-    samples = []
-    cores = None
-    for i in range(args.warmup + args.steps):
-        dt, cores = cpu_reference_sample()
-        if i >= args.warmup:
-            samples.append(dt)
-    mean = float(np.mean(samples))
-    value = cpu_recons_per_s(mean)
-    sample = ('one VCD subset update (1 of %d subsets, 1 of %d iterations) of the cone workload per step, oracle '
-              'port on %d processes; scaled x%d to one recon' % (CONE['subsets'], CONE['iterations'], cores,
-                                                                CONE['subsets'] * CONE['iterations']))
-    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'recons/s', 'n_gpus': args.gpus,
-            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean * 1e3, 'higher_is_better': True,
-            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': cone_config(world),
-            'cpu_baseline': {'value': value, 'unit': 'recons/s', 'cores': cores, 'kind': 'port', 'sample': sample},
-            'e2e': {'value': value, 'unit': 'recons/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
-            'note': 'reference JAX CPU path unavailable (jax not installable offline); oracle NumPy port timed'}
-    print(json.dumps(line), flush=True)
+def batched_config(world):
+    return {'workload': '24 uneven parallel-beam scans (views U{60..720}, rows U{8..64}, channels U{96..512}, '
+                        'seed i), 10 ellipsoids each, 10 VCD iterations x 4 subsets, FBP init; batched path',
+            'num_scans': BATCH['num_scans'], 'iterations': BATCH['iterations'], 'subsets': BATCH['subsets'],
+            'parallelism': 'replicas x%d' % world, 'l2': 'flushed before every step (inputs ~1 GB > L2)'}
 
 
 def cone_config(world):
@@ -308,69 +406,135 @@ def cone_config(world):
             'subsets': CONE['subsets'], 'parallelism': 'replicas x%d' % world, 'l2': 'flushed before every step'}
 
 
+def run_reference(args):
+    world = int(os.environ.get('WORLD_SIZE', '1'))
+    rank = int(os.environ.get('RANK', '0'))
+    if rank != 0:
+        return
+    samples, cores, scale = [], None, 1.0
+    for i in range(args.warmup + args.steps):
+        if args.workload == 'batched':
+            dt, cores, scale = cpu_batched_sample()
+        else:
+            dt, cores = cpu_reference_sample()
+            scale = CONE['subsets'] * CONE['iterations']
+        if i >= args.warmup:
+            samples.append(dt)
+    mean = float(np.mean(samples))
+    units = BATCH['num_scans'] if args.workload == 'batched' else 1
+    value = units / (mean * scale)
+    sample = ('one VCD subset update of %s per step, oracle NumPy port on %d processes, scaled x%.1f to the whole '
+              'workload' % ('scan %d of the batch' % BATCH['cpu_sample_scan'] if args.workload == 'batched'
+                            else 'the cone scan', cores, scale))
+    line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'recons/s', 'n_gpus': args.gpus,
+            'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean * 1e3, 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
+            'config': batched_config(world) if args.workload == 'batched' else cone_config(world),
+            'cpu_baseline': {'value': value, 'unit': 'recons/s', 'cores': cores, 'kind': 'port', 'sample': sample},
+            'e2e': {'value': value, 'unit': 'recons/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
+            'note': 'reference JAX CPU path unavailable (jax not installable offline); oracle NumPy port timed'}
+    print(json.dumps(line), flush=True)
+
+
 def run_gpu(args):
     import torch
-    import mbirjax_b200 as mb
     from mbirjax_b200 import _capi
     world, rank, local = dist_setup(args.gpus)
     device = torch.device('cuda', local)
     lib = _capi.load_library()
     peak_gbs, peak_kind = load_peaks()
-    model, sino, phantom = build_cone_workload(device)
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
     def flush():
         flush_buf.zero_()
 
-    # device-resident: sinogram already in HBM
-    def step():
-        recon_once(model, sino)
+    if args.workload == 'batched':
+        models, sinos = build_batched_workload(device)
+        units = BATCH['num_scans']
+        config = batched_config(world)
 
-    clocks = ClockSampler(local)
-    launches0 = None
+        def step():
+            batched_recon(models, sinos)
+    else:
+        model, sino, phantom = build_cone_workload(device)
+        units = 1
+        config = cone_config(world)
+
+        def step():
+            recon_once(model, sino)
+
     for _ in range(args.warmup):
         step()
     torch.cuda.synchronize()
+    clocks = ClockSampler(local)
     clocks.start()
     launches0 = lib.mbx_launch_count()
     ms = timed_steps(step, args.steps, 0, world, flush)
     launches = lib.mbx_launch_count() - launches0
     clk = clocks.stop()
     ms = max_over_ranks(ms, world)
-    ms_per_step = ms / args.steps
-    value = world * args.steps / (ms * 1e-3)
+    value = world * units * args.steps / (ms * 1e-3)
+    line = {'metric': METRIC, 'value': round(value, 4), 'unit': 'recons/s', 'n_gpus': world, 'steps': args.steps,
+            'warmup': args.warmup, 'ms_per_step': round(ms / args.steps, 3), 'higher_is_better': True,
+            'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': config,
+            'gpu_launches': int(launches), 'clocks': clk}
 
-    # accuracy of this recon against the phantom (sanity) is reported; parity vs the oracle is in the tests
-    rec = recon_once(model, sino)
-    nrmse_phantom = float(torch.linalg.norm(rec - phantom) / torch.linalg.norm(phantom))
-
-    line = {'metric': METRIC, 'value': round(value, 3), 'unit': 'recons/s', 'n_gpus': world, 'steps': args.steps,
-            'warmup': args.warmup, 'ms_per_step': round(ms_per_step, 3), 'higher_is_better': True, 'scaling': 'weak',
-            'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': cone_config(world),
-            'gpu_launches': int(launches), 'clocks': clk, 'nrmse_vs_phantom': round(nrmse_phantom, 4)}
+    if args.workload == 'batched':
+        # the plain per-scan GPU path on the same scans, measured the same way
+        for _ in range(1):
+            plain_recon(models, sinos)
+        p_ms = timed_steps(lambda: plain_recon(models, sinos), args.steps, 0, world, flush)
+        p_ms = max_over_ranks(p_ms, world)
+        plain_value = world * units * args.steps / (p_ms * 1e-3)
+        rb = batched_recon(models, sinos)
+        rp = plain_recon(models, sinos)
+        diff = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(rb, rp))
+        line['plain_recons_per_s'] = round(plain_value, 4)
+        line['batched_over_plain'] = round(value / plain_value, 3)
+        line['max_rel_l2_batched_vs_plain'] = diff
+        del rb, rp
 
     if not args.no_e2e:
-        host_sino = sino.cpu().pin_memory()
-        out_host = torch.empty(tuple(model.get_params('recon_shape')), dtype=torch.float32).pin_memory()
+        if args.workload == 'batched':
+            host_sinos = [s_.cpu().pin_memory() for s_ in sinos]
+            outs = [torch.empty(tuple(m.get_params('recon_shape')), dtype=torch.float32).pin_memory() for m in models]
 
-        def e2e_step():
-            r = recon_once(model, host_sino)          # H2D of the sinogram happens inside the public API call
-            out_host.copy_(r, non_blocking=True)      # D2H of the recon
+            def e2e_step():
+                recs = batched_recon(models, host_sinos)   # H2D of every sinogram inside the public API
+                for o, r in zip(outs, recs):
+                    o.copy_(r, non_blocking=True)            # D2H of every recon
+            h2d = sum(int(h.numel()) * 4 for h in host_sinos)
+            d2h = sum(int(o.numel()) * 4 for o in outs)
+        else:
+            host_sino = sino.cpu().pin_memory()
+            out_host = torch.empty(tuple(model.get_params('recon_shape')), dtype=torch.float32).pin_memory()
+
+            def e2e_step():
+                r = recon_once(model, host_sino)
+                out_host.copy_(r, non_blocking=True)
+            h2d, d2h = int(host_sino.numel()) * 4, int(out_host.numel()) * 4
         e_ms = timed_steps(e2e_step, args.steps, 1, world, flush)
         e_ms = max_over_ranks(e_ms, world)
-        line['e2e'] = {'value': round(world * args.steps / (e_ms * 1e-3), 3), 'unit': 'recons/s',
-                       'h2d_bytes_per_step': int(host_sino.numel() * 4),
-                       'd2h_bytes_per_step': int(out_host.numel() * 4)}
+        line['e2e'] = {'value': round(world * units * args.steps / (e_ms * 1e-3), 4), 'unit': 'recons/s',
+                       'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h}
 
-    line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind)
+    if args.workload == 'batched':
+        line['roofline'] = batched_roofline(models, sinos, peak_gbs, peak_kind)
+    else:
+        line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind)
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
-        dt, cores = cpu_reference_sample()
-        line['cpu_baseline'] = {'value': round(cpu_recons_per_s(dt), 6), 'unit': 'recons/s', 'cores': cores,
+        if args.workload == 'batched':
+            dt, cores, scale = cpu_batched_sample()
+        else:
+            dt, cores = cpu_reference_sample()
+            scale = CONE['subsets'] * CONE['iterations']
+        line['cpu_baseline'] = {'value': round(units / (dt * scale), 6), 'unit': 'recons/s', 'cores': cores,
                                 'kind': 'port',
-                                'sample': 'one VCD subset update of the workload (oracle NumPy port, %d processes), '
-                                          'scaled x%d to one recon; %.2f s measured' % (
-                                              cores, CONE['subsets'] * CONE['iterations'], dt)}
+                                'sample': 'one VCD subset update of %s (oracle NumPy port, %d processes), %.2f s, '
+                                          'scaled x%.1f to the workload' % (
+                                              'scan %d' % BATCH['cpu_sample_scan'] if args.workload == 'batched'
+                                              else 'the cone scan', cores, dt, scale)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -210,6 +210,13 @@ MBX_API int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans, co
  * (tomography_model.py:1343-1542) per scan. */
 MBX_API int mbx_vcd_batched_step(const mbx_batched_plan *plan, int32_t step, void *stream);
 
+/* Number of stages of one batched subset step, and one stage on its own (the step is stages 0..7 in order:
+ * back projection, delta, forward projection, line-search partials, alpha, recon update, error update, l1).
+ * Running the stages of a step one by one in order is the same as mbx_vcd_batched_step; it lets a caller
+ * time each stage with events. */
+#define MBX_BATCHED_STAGES 8
+MBX_API int mbx_vcd_batched_stage(const mbx_batched_plan *plan, int32_t step, int32_t stage, void *stream);
+
 /* Per-scan iteration statistics into iter_stats[iteration] (inputs of the reference's fm_rmse and NMAE,
  * tomography_model.py:1219-1220). */
 MBX_API int mbx_vcd_batched_iteration_stats(const mbx_batched_plan *plan, int32_t iteration, void *stream);

@@ -77,6 +77,7 @@ _SIGNATURES = {
                                                ctypes.POINTER(MbxBatchedPlan), c_void_p]),
     'mbx_vcd_batched_step': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_void_p]),
     'mbx_vcd_batched_iteration_stats': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_void_p]),
+    'mbx_vcd_batched_stage': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_int32, c_void_p]),
     'mbx_direct_filter': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p]),
 }
 
@@ -281,3 +282,11 @@ def vcd_batched_step(plan, step):
 def vcd_batched_iteration_stats(plan, iteration):
     _check(load_library().mbx_vcd_batched_iteration_stats(ctypes.byref(plan), int(iteration), _stream()),
            'mbx_vcd_batched_iteration_stats')
+
+
+BATCHED_STAGES = ('bp', 'delta', 'fp', 'linquad', 'alpha', 'apply', 'error', 'l1')
+
+
+def vcd_batched_stage(plan, step, stage):
+    _check(load_library().mbx_vcd_batched_stage(ctypes.byref(plan), int(step), int(stage), _stream()),
+           'mbx_vcd_batched_stage')

@@ -575,38 +575,51 @@ static const BatchedPlanHost *plan_of(const mbx_batched_plan *p) {
     return P->magic == BT_MAGIC ? P : nullptr;
 }
 
-extern "C" int mbx_vcd_batched_step(const mbx_batched_plan *plan, int32_t step, void *stream) {
-    const BatchedPlanHost *P = plan_of(plan);
-    if (!P || step < 0 || step >= P->num_steps) return MBX_ERR_INVALID_ARG;
-    cudaStream_t st = static_cast<cudaStream_t>(stream);
+static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStream_t st) {
     int *err = device_error_ptr();
     const BatchedTables &T = P->t;
     const int n = P->num_scans;
     const int warp_blocks = (n + 7) / 8;
-    if (P->kind == MBX_GEOM_PARALLEL)
-        b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
-    else
-        b_bp<MBX_GEOM_CONE><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
-    note_launch();
-    b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err);
-    note_launch();
-    if (P->kind == MBX_GEOM_PARALLEL)
-        b_fp<MBX_GEOM_PARALLEL><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
-    else
-        b_fp<MBX_GEOM_CONE><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
-    note_launch();
-    b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
-    note_launch();
-    b_alpha<<<warp_blocks, 256, 0, st>>>(T, n, step);
-    note_launch();
-    b_apply<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total);
-    note_launch();
-    b_error<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
-    note_launch();
-    b_l1<<<warp_blocks, 256, 0, st>>>(T, n, step);
+    switch (stage) {
+        case 0:
+            if (P->kind == MBX_GEOM_PARALLEL)
+                b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
+            else
+                b_bp<MBX_GEOM_CONE><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
+            break;
+        case 1: b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err); break;
+        case 2:
+            if (P->kind == MBX_GEOM_PARALLEL)
+                b_fp<MBX_GEOM_PARALLEL><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+            else
+                b_fp<MBX_GEOM_CONE><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+            break;
+        case 3: b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;
+        case 4: b_alpha<<<warp_blocks, 256, 0, st>>>(T, n, step); break;
+        case 5: b_apply<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total); break;
+        case 6: b_error<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;
+        case 7: b_l1<<<warp_blocks, 256, 0, st>>>(T, n, step); break;
+        default: return MBX_ERR_INVALID_ARG;
+    }
     note_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+}
+
+extern "C" int mbx_vcd_batched_step(const mbx_batched_plan *plan, int32_t step, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P || step < 0 || step >= P->num_steps) return MBX_ERR_INVALID_ARG;
+    for (int stage = 0; stage < MBX_BATCHED_STAGES; ++stage) {
+        const int rc = launch_stage(P, step, stage, static_cast<cudaStream_t>(stream));
+        if (rc != MBX_OK) return rc;
+    }
+    return MBX_OK;
+}
+
+extern "C" int mbx_vcd_batched_stage(const mbx_batched_plan *plan, int32_t step, int32_t stage, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P || step < 0 || step >= P->num_steps || stage < 0 || stage >= MBX_BATCHED_STAGES) return MBX_ERR_INVALID_ARG;
+    return launch_stage(P, step, stage, static_cast<cudaStream_t>(stream));
 }
 
 extern "C" int mbx_vcd_batched_iteration_stats(const mbx_batched_plan *plan, int32_t iteration, void *stream) {
