@@ -77,28 +77,39 @@ inline CbPlan plan_fp_cb(const mbx_geom &g) {
     return pl;
 }
 
+// Fractional centre channel n_p of one pixel (the same arithmetic as cb_footprint, so both agree on round(n_p)).
+template <int KIND>
+__device__ __forceinline__ float cb_channel(const mbx_geom &g, float cs, float sn, float xt, float yt, float inv_d,
+                                            float &mag) {
+    const float inv_dc = 1.0f / g.delta_det_channel;
+    const float det_center_channel = 0.5f * (float)(g.num_det_channels - 1);
+    const float x_p = cs * xt - sn * yt;
+    if (KIND == MBX_GEOM_PARALLEL) {
+        mag = 1.0f;
+        return (x_p + g.det_channel_offset) * inv_dc + det_center_channel;
+    }
+    const float y_p = sn * xt + cs * yt;
+    mag = 1.0f / (1.0f / g.magnification - y_p * inv_d);
+    return (mag * x_p + g.det_channel_offset) * inv_dc + det_center_channel;
+}
+
 // Channel footprint of one pixel (trig-free for cone beam); also the cone vertical constants.
 template <int KIND>
 __device__ __forceinline__ void cb_footprint(const mbx_geom &g, float cs, float sn, float xt, float yt, int &nc,
                                              float &a0, float &a1, float &a2, float &imd, float &wr, float &mdz,
                                              float &mz0) {
     const float inv_dc = 1.0f / g.delta_det_channel;
-    const float det_center_channel = 0.5f * (float)(g.num_det_channels - 1);
-    float n_p, w, scale;
+    const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
+    float mag;
+    const float n_p = cb_channel<KIND>(g, cs, sn, xt, yt, inv_d, mag);
+    float w, scale;
     if (KIND == MBX_GEOM_PARALLEL) {
-        const float x = cs * xt - sn * yt;
-        n_p = (x + g.det_channel_offset) * inv_dc + det_center_channel;
         const float cos_alpha = fmaxf(fabsf(cs), fabsf(sn));
         w = (g.delta_voxel * inv_dc) * cos_alpha;
         scale = g.delta_voxel / cos_alpha;
         imd = wr = mdz = mz0 = 0.0f;
     } else {
-        const float x_p = cs * xt - sn * yt;
-        const float y_p = sn * xt + cs * yt;
-        const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
-        const float mag = 1.0f / (1.0f / g.magnification - y_p * inv_d);
-        const float u = mag * x_p;
-        n_p = (u + g.det_channel_offset) * inv_dc + det_center_channel;
+        const float u = mag * (cs * xt - sn * yt);
         const float t = u * inv_d;
         const float cos_tp = rsqrtf(fmaf(t, t, 1.0f));
         const float sin_tp = t * cos_tp;
@@ -174,6 +185,8 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     const float angle = view_ok ? g.angles[vi] : 0.0f;
     const float cs = cosf(angle), sn = sinf(angle);
     const float kconst = 0.5f * (float)(num_slices - 1) - g.recon_slice_offset / g.delta_voxel;
+    const float inv_cols = 1.0f / (float)g.num_recon_cols;
+    const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
 
     __syncthreads();  // previous tile of this CTA (batched use) is finished with shared memory
     for (size_t i = tid; i < tile_words; i += CB_THREADS) tile[i] = 0.0f;
@@ -199,20 +212,19 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     while (scan < num_pixels) {
         // ---- 1. compaction of the pixels that touch this channel block (ordered)
         int count = 0;
-        __syncthreads();
+        __syncthreads();  // the previous pass is done with the list
+        const int count0 = count;
         while (scan < num_pixels && count <= CB_CAP - CB_THREADS) {
             const long long p = scan + tid;
             bool take = false;
-            int nc = 0;
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f, imd = 0.f, wr = 0.f, mdz = 0.f, mz0 = 0.f;
             if (p < num_pixels) {
                 const int idx = A.pix[p];
                 if (idx < 0 || idx >= npix_grid) {
                     if (cb == 0 && j == 0) flag_error(err, MBX_ERRFLAG_PIXEL);
                 } else {
-                    float xt, yt;
-                    pixel_tilde(g, idx, xt, yt);
-                    cb_footprint<KIND>(g, cs, sn, xt, yt, nc, a0, a1, a2, imd, wr, mdz, mz0);
+                    float xt, yt, mag;
+                    pixel_tilde_fast(g, idx, inv_cols, xt, yt);
+                    const int nc = (int)rintf(cb_channel<KIND>(g, cs, sn, xt, yt, inv_d, mag));
                     take = nc + 1 >= n0 && nc - 1 < n0 + CB_NB;
                 }
             }
@@ -223,22 +235,31 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             for (int w = 0; w < warp; ++w) base += s_misc[w];
             int total = 0;
             for (int w = 0; w < 8; ++w) total += s_misc[w];
-            if (take) {
-                const int pos = base + __popc(ballot & ((1u << lane) - 1u));
-                L.p[pos] = A.vox_by_index ? A.pix[p] : (int)p;  // row of vox holding this pixel's cylinder
-                L.nc[pos] = nc;
-                L.a0[pos] = a0;
-                L.a1[pos] = a1;
-                L.a2[pos] = a2;
-                L.imd[pos] = imd;
-                L.wr[pos] = wr;
-                L.mdz[pos] = mdz;
-                L.mz0[pos] = mz0;
-            }
+            if (take) L.p[base + __popc(ballot & ((1u << lane) - 1u))] = (int)p;
             count += total;
             scan += CB_THREADS;
             __syncthreads();
         }
+        // footprints of the kept pixels only (dense, no divergence)
+        for (int i = count0 + tid; i < count; i += CB_THREADS) {
+            const int p = L.p[i];
+            const int idx = A.pix[p];
+            float xt, yt;
+            pixel_tilde_fast(g, idx, inv_cols, xt, yt);
+            int nc;
+            float a0, a1, a2, imd, wr, mdz, mz0;
+            cb_footprint<KIND>(g, cs, sn, xt, yt, nc, a0, a1, a2, imd, wr, mdz, mz0);
+            L.p[i] = A.vox_by_index ? idx : p;  // row of vox holding this pixel's cylinder
+            L.nc[i] = nc;
+            L.a0[i] = a0;
+            L.a1[i] = a1;
+            L.a2[i] = a2;
+            L.imd[i] = imd;
+            L.wr[i] = wr;
+            L.mdz[i] = mdz;
+            L.mz0[i] = mz0;
+        }
+        __syncthreads();
         // ---- 2. accumulation into the private copy of each lane group
         for (int rg = lg / copies; rg < row_groups; rg += (pl.groups >= row_groups ? row_groups : pl.groups)) {
             // with copies > 1 the lane groups of a row group split the pixel list; else each group walks them all

@@ -36,6 +36,23 @@ __device__ __forceinline__ void pixel_tilde(const mbx_geom &g, int idx, float &x
     x_tilde = g.delta_voxel * ((float)col - 0.5f * (float)(g.num_recon_cols - 1));
 }
 
+// Same, with the row / column split of the flat index done by a float reciprocal (inv_cols = 1/num_recon_cols)
+// and an exact integer correction instead of an integer division.
+__device__ __forceinline__ void pixel_tilde_fast(const mbx_geom &g, int idx, float inv_cols, float &x_tilde,
+                                                 float &y_tilde) {
+    int row = __float2int_rz(__int2float_rz(idx) * inv_cols);
+    int col = idx - row * g.num_recon_cols;
+    if (col < 0) {
+        --row;
+        col += g.num_recon_cols;
+    } else if (col >= g.num_recon_cols) {
+        ++row;
+        col -= g.num_recon_cols;
+    }
+    y_tilde = g.delta_voxel * ((float)row - 0.5f * (float)(g.num_recon_rows - 1));
+    x_tilde = g.delta_voxel * ((float)col - 0.5f * (float)(g.num_recon_cols - 1));
+}
+
 // Horizontal (channel) footprint of one pixel in one view: fractional channel n_p, centre channel,
 // projected width W (in channels) and cos(alpha).
 struct ChannelFootprint {

@@ -4,7 +4,9 @@
 // vcd.cu).  Batching replaces one launch per scan per stage with ONE persistent launch per stage for all scans:
 // each stage kernel walks a packed work list -- the concatenation of every scan's tiles, described by
 // per-stage prefix offsets over scans -- with a grid sized to the resident CTAs of the device, and decodes each
-// tile into (scan, local tile) by binary search.  Stages of one subset step:
+// tile into (scan, local tile) by binary search.  The two projection stages hand tiles out dynamically (an
+// atomic counter reset by a memset before each launch) over a work list ordered by decreasing per-tile cost,
+// so scans of very different size finish together.  Stages of one subset step:
 //   b_bp      back projection of W*e at each scan's current subset (bp_fast tiles)
 //   b_delta   qGGMRF gradient/Hessian + delta; float64 partials of the prior terms, one per tile
 //   b_fp      forward projection of delta (channel-block tiles of fp_cb)
@@ -54,6 +56,8 @@ struct BatchedTables {
     int *bp_off, *fp_off, *el_off, *sn_off, *rc_off;  // [num_scans + 1] tile prefix offsets
     int *fp_cblocks;    // [num_scans]
     int *bp_gx;         // [num_scans]
+    int *bp_scan, *fp_scan;  // [num_scans]: scan at each position of the (cost-sorted) bp / fp work lists
+    int *counters;      // [2]: next bp / fp tile to hand out (reset before each launch)
     int *schedule;      // [num_steps][num_scans]
     double *p_prior, *p_fwd, *p_l1, *p_iter;
     float *alpha;       // [num_scans]
@@ -103,12 +107,22 @@ __device__ __forceinline__ void tile_reduce(const double (&v)[NV], double *slot)
     __syncthreads();
 }
 
+// Next tile of a dynamically scheduled work list (one atomic per CTA per tile).
+__device__ __forceinline__ int fetch_tile(int *counter) {
+    __shared__ int s_next;
+    __syncthreads();  // every thread is done with the previous tile index
+    if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
+    __syncthreads();
+    return s_next;
+}
+
 template <int KIND>
 __global__ void __launch_bounds__(BPF_THREADS, 2) b_bp(BatchedTables T, int num_scans, int step, int total, int *err) {
     extern __shared__ __align__(16) float smb[];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int s = find_scan(T.bp_off, num_scans, t);
-        const int local = t - __ldg(T.bp_off + s);
+    for (int t = fetch_tile(T.counters); t < total; t = fetch_tile(T.counters)) {
+        const int k = find_scan(T.bp_off, num_scans, t);
+        const int s = __ldg(T.bp_scan + k);
+        const int local = t - __ldg(T.bp_off + k);
         const int sub = __ldg(T.schedule + step * num_scans + s);
         const int K = T.scans[s].K;
         const int gx = __ldg(T.bp_gx + s);
@@ -119,9 +133,10 @@ __global__ void __launch_bounds__(BPF_THREADS, 2) b_bp(BatchedTables T, int num_
 template <int KIND>
 __global__ void __launch_bounds__(CB_THREADS, 2) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
     extern __shared__ __align__(16) float smf2[];
-    for (int t = blockIdx.x; t < total; t += gridDim.x) {
-        const int s = find_scan(T.fp_off, num_scans, t);
-        const int local = t - __ldg(T.fp_off + s);
+    for (int t = fetch_tile(T.counters + 1); t < total; t = fetch_tile(T.counters + 1)) {
+        const int k = find_scan(T.fp_off, num_scans, t);
+        const int s = __ldg(T.fp_scan + k);
+        const int local = t - __ldg(T.fp_off + k);
         const int sub = __ldg(T.schedule + step * num_scans + s);
         const int K = T.scans[s].K;
         const int cbs = __ldg(T.fp_cblocks + s);
@@ -334,7 +349,8 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
 }
 
 struct Layout {
-    size_t scans, bpargs, fpargs, offs, cblocks, gx, sched, p_prior, p_fwd, p_l1, p_iter, alpha, bufs, total;
+    size_t scans, bpargs, fpargs, offs, cblocks, gx, scan_of, counters, sched, p_prior, p_fwd, p_l1, p_iter, alpha,
+        bufs, total;
     int bp_total, fp_total, el_total, sn_total, rc_total;
     std::vector<size_t> buf_off;  // per scan: bp, delta, dsino
 };
@@ -364,6 +380,8 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
     L.offs = take(sizeof(int) * 5 * (n + 1));
     L.cblocks = take(sizeof(int) * n);
     L.gx = take(sizeof(int) * n);
+    L.scan_of = take(sizeof(int) * 2 * n);
+    L.counters = take(sizeof(int) * 2);
     L.sched = take(sizeof(int) * (size_t)num_steps * n);
     L.p_prior = take(sizeof(double) * 2 * (size_t)L.el_total);
     L.p_fwd = take(sizeof(double) * 2 * (size_t)L.sn_total);
@@ -422,6 +440,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
         }
     char *base = static_cast<char *>(workspace);
     std::vector<char> host(L.sched + sizeof(int) * (size_t)num_steps * num_scans, 0);
+    int *hscan_of = reinterpret_cast<int *>(host.data() + L.scan_of);
     VcdScan *hs = reinterpret_cast<VcdScan *>(host.data() + L.scans);
     BpArgs *hb = reinterpret_cast<BpArgs *>(host.data() + L.bpargs);
     FpArgs *hf = reinterpret_cast<FpArgs *>(host.data() + L.fpargs);
@@ -490,11 +509,35 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
         smem_fp = std::max(smem_fp, z.fpp.smem);
         hcb[s] = z.fpp.cblocks;
         hgx[s] = z.bp_gx;
-        o_bp[s + 1] = o_bp[s] + z.bp_tiles;
-        o_fp[s + 1] = o_fp[s] + z.fp_tiles;
         o_el[s + 1] = o_el[s] + z.el_tiles;
         o_sn[s + 1] = o_sn[s] + z.sn_tiles;
         o_rc[s + 1] = o_rc[s] + z.rc_tiles;
+    }
+    // bp / fp work lists: scans in decreasing order of per-tile cost, so that the dynamically scheduled tail of
+    // a launch is made of the cheapest tiles
+    {
+        std::vector<int> ord(num_scans);
+        std::vector<double> cost(num_scans);
+        for (int s = 0; s < num_scans; ++s) {
+            const mbx_geom &g = scans[s].geom;
+            cost[s] = (double)g.num_views * std::min(g.num_recon_slices, BPF_ST * zs[s].bpp.nsl) * 32.0 * zs[s].bpp.npg;
+            ord[s] = s;
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        for (int k = 0; k < num_scans; ++k) {
+            hscan_of[k] = ord[k];
+            o_bp[k + 1] = o_bp[k] + zs[ord[k]].bp_tiles;
+        }
+        for (int s = 0; s < num_scans; ++s) {
+            const mbx_geom &g = scans[s].geom;
+            cost[s] = ((double)scans[s].subset_size * (CB_NB + 2) / g.num_det_channels + 1.0) * g.num_det_rows;
+            ord[s] = s;
+        }
+        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
+        for (int k = 0; k < num_scans; ++k) {
+            hscan_of[num_scans + k] = ord[k];
+            o_fp[k + 1] = o_fp[k] + zs[ord[k]].fp_tiles;
+        }
     }
     std::memcpy(hsched, schedule, sizeof(int) * (size_t)num_steps * num_scans);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
@@ -515,6 +558,9 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     P.t.rc_off = doff + 4 * n1;
     P.t.fp_cblocks = reinterpret_cast<int *>(base + L.cblocks);
     P.t.bp_gx = reinterpret_cast<int *>(base + L.gx);
+    P.t.bp_scan = reinterpret_cast<int *>(base + L.scan_of);
+    P.t.fp_scan = P.t.bp_scan + num_scans;
+    P.t.counters = reinterpret_cast<int *>(base + L.counters);
     P.t.schedule = reinterpret_cast<int *>(base + L.sched);
     P.t.p_prior = reinterpret_cast<double *>(base + L.p_prior);
     P.t.p_fwd = reinterpret_cast<double *>(base + L.p_fwd);
@@ -582,6 +628,10 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
     const int warp_blocks = (n + 7) / 8;
     switch (stage) {
         case 0:
+            {
+                const cudaError_t me = cudaMemsetAsync(T.counters, 0, sizeof(int), st);
+                if (me != cudaSuccess) return set_cuda_error(me);
+            }
             if (P->kind == MBX_GEOM_PARALLEL)
                 b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
             else
@@ -589,6 +639,10 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
             break;
         case 1: b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err); break;
         case 2:
+            {
+                const cudaError_t me = cudaMemsetAsync(T.counters + 1, 0, sizeof(int), st);
+                if (me != cudaSuccess) return set_cuda_error(me);
+            }
             if (P->kind == MBX_GEOM_PARALLEL)
                 b_fp<MBX_GEOM_PARALLEL><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
             else
