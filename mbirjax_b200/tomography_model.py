@@ -87,7 +87,8 @@ class TomographyModel(ParameterHandler):
         return _cuda_device()
 
     def _geometry(self):
-        """The mbx_geom record for the current parameters (device angle table kept alive on the model)."""
+        """The mbx_geom record for the current parameters.  Its angle pointer refers to a device tensor owned by
+        this model, so the record is valid only while the model is alive and its geometry parameters unchanged."""
         if self._geom is None:
             dev = self._device()
             sinogram_shape, recon_shape = self.get_params(['sinogram_shape', 'recon_shape'])
