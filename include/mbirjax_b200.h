@@ -127,6 +127,23 @@ MBX_API int mbx_sparse_back_project(const mbx_geom *g, const float *sinogram, co
                             int32_t num_views_sel, int32_t coeff_power, float scale, float *out,
                             void *workspace, size_t workspace_bytes, void *stream);
 
+/* Size of the static device array behind mbx_sparse_back_project_noalloc (16 MiB). */
+#define MBX_NOALLOC_SCRATCH_BYTES (16u << 20)
+
+/* mbx_sparse_back_project without a workspace argument, for callers that cannot allocate GPU memory at call
+ * time (for example code running inside JAX, which the mbirjax reference configures to take 98% of the GPU
+ * for its own allocator, or pipelines that reserve all device memory up front).  This entry point has no
+ * counterpart in the reference.  It calls no cudaMalloc, cudaFree or other allocating routine.  The scratch
+ * for the split view sums lives in a static device array of MBX_NOALLOC_SCRATCH_BYTES: every GPU on which the
+ * entry point is used holds that array until the process exits.  Its address is looked up on the first call on
+ * each device, so make that first call before any stream capture.  All calls on a device share the array, so
+ * calls whose GPU work overlaps race and must be serialised by the caller.  A call whose sizes would need more
+ * scratch than the array holds returns MBX_ERR_WORKSPACE before any launch. */
+MBX_API int mbx_sparse_back_project_noalloc(const mbx_geom *g, const float *sinogram, const float *weights,
+                                            const int32_t *pixel_indices, int64_t num_pixels,
+                                            const int32_t *view_indices, int32_t num_views_sel, int32_t coeff_power,
+                                            float scale, float *out, void *stream);
+
 /* ---- qGGMRF prior ----------------------------------------------------------------------------- */
 
 /* Surrogate gradient and Hessian diagonal at pixel_indices (num_pixels, S) each.

@@ -62,6 +62,9 @@ _SIGNATURES = {
     'mbx_sparse_back_project': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p, c_int64,
                                                c_void_p, c_int32, c_int32, c_float, c_void_p, c_void_p, c_size_t,
                                                c_void_p]),
+    'mbx_sparse_back_project_noalloc': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p,
+                                                       c_int64, c_void_p, c_int32, c_int32, c_float, c_void_p,
+                                                       c_void_p]),
     'mbx_qggmrf_grad_hess': (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int64,
                                             ctypes.POINTER(MbxQggmrfParams), c_void_p, c_void_p, c_void_p]),
     'mbx_qggmrf_loss_grad_workspace_bytes': (c_size_t, [c_int32, c_int32, c_int32]),
@@ -186,6 +189,24 @@ def back_project(geom, sinogram, pixel_indices, view_indices=None, coeff_power=1
                                      _ptr(view_indices), nv, int(coeff_power), float(scale), _ptr(out), _ptr(ws),
                                      nbytes, _stream())
     _check(rc, 'mbx_sparse_back_project')
+    return out
+
+
+def back_project_noalloc(geom, sinogram, pixel_indices, view_indices=None, coeff_power=1, weights=None, scale=1.0,
+                         out=None):
+    """Same result as back_project, through the entry point that allocates nothing: its scratch is a static
+    device array inside the library (for callers that cannot allocate GPU memory at call time).  Calls whose GPU
+    work overlaps share that array and must not run concurrently."""
+    lib = load_library()
+    _require_cuda(sinogram, pixel_indices, view_indices, weights)
+    n = int(pixel_indices.shape[0])
+    nv = int(view_indices.shape[0]) if view_indices is not None else geom.num_views
+    if out is None:
+        out = torch.empty((n, geom.num_recon_slices), dtype=torch.float32, device=sinogram.device)
+    rc = lib.mbx_sparse_back_project_noalloc(ctypes.byref(geom), _ptr(sinogram), _ptr(weights), _ptr(pixel_indices),
+                                             n, _ptr(view_indices), nv, int(coeff_power), float(scale), _ptr(out),
+                                             _stream())
+    _check(rc, 'mbx_sparse_back_project_noalloc')
     return out
 
 
