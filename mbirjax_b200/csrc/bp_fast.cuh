@@ -231,13 +231,35 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             const float *view = sino + (long long)vi * num_rows * num_channels;
             const float *wview = wts ? wts + (long long)vi * num_rows * num_channels : nullptr;
             if (KIND == MBX_GEOM_PARALLEL) {
-                const float *row = view + (long long)s0 * num_channels;
-                const float *wrow = wview ? wview + (long long)s0 * num_channels : nullptr;
+                const long long rowoff = (long long)s0 * num_channels;
+                if (nc >= 1 && nc + 1 < num_channels && ns == BPF_ST) {
+                    // all three taps on the detector and a full slice tile: one pointer, constant tap offsets
+                    const float *p = view + rowoff + (nc - 1);
+                    if (wview) {
+                        const float *q = wview + rowoff + (nc - 1);
 #pragma unroll
-                for (int s = 0; s < BPF_ST; ++s) {
-                    if (s < ns) acc[s] += bpf_row(row, wrow, n0, n1, n2, a0, a1, a2);
-                    row += num_channels;
-                    if (wrow) wrow += num_channels;
+                        for (int s = 0; s < BPF_ST; ++s) {
+                            acc[s] = fmaf(a0, __ldg(p) * __ldg(q),
+                                          fmaf(a1, __ldg(p + 1) * __ldg(q + 1), fmaf(a2, __ldg(p + 2) * __ldg(q + 2), acc[s])));
+                            p += num_channels;
+                            q += num_channels;
+                        }
+                    } else {
+#pragma unroll
+                        for (int s = 0; s < BPF_ST; ++s) {
+                            acc[s] = fmaf(a0, __ldg(p), fmaf(a1, __ldg(p + 1), fmaf(a2, __ldg(p + 2), acc[s])));
+                            p += num_channels;
+                        }
+                    }
+                } else {
+                    const float *row = view + rowoff;
+                    const float *wrow = wview ? wview + rowoff : nullptr;
+#pragma unroll
+                    for (int s = 0; s < BPF_ST; ++s) {
+                        if (s < ns) acc[s] += bpf_row(row, wrow, n0, n1, n2, a0, a1, a2);
+                        row += num_channels;
+                        if (wrow) wrow += num_channels;
+                    }
                 }
             } else {
                 const float A0 = sh.A0[f], A1 = sh.A1[f], c2 = sh.c2[f];
