@@ -229,7 +229,7 @@ static cudaError_t launch_fp_cb(const FpArgs &A, cudaStream_t st) {
 int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, long long num_pixels,
                     const int32_t *views, int num_views_sel, float *out, void *ws, size_t ws_bytes,
                     cudaStream_t st) {
-    const CbPlan cpl = plan_fp_cb(g);
+    const CbPlan cpl = plan_fp_cb(g, num_views_sel, 4LL * num_sms());
     if (cpl.ok) {
         FpArgs A;
         A.g = g;

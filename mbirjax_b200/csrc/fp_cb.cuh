@@ -1,20 +1,27 @@
 // Forward projector for psf_radius == 1 (and bp_psf_radius == 1 for cone beam), parallel and cone beam:
-// channel-block gather, no atomics, deterministic.  Same contract and arithmetic as the general fp_kernel
-// (forward_project.cu), which replaces Projectors.sparse_forward_project (projectors.py:61-129) over
-// parallel_beam.py:138-178 and cone_beam.py:189-377.
+// channel-block gather with a per-block counting sort, register accumulation, no atomics on data, deterministic.
+// Same contract and arithmetic as the general fp_kernel (forward_project.cu), which replaces
+// Projectors.sparse_forward_project (projectors.py:61-129) over parallel_beam.py:138-178 and cone_beam.py:189-377.
 //
-// One CTA owns an output block: one view x CB_NB consecutive channels x all detector rows.
-//  1. Scan: the 256 threads walk the pixel list 256 at a time, compute each pixel's channel footprint
-//     (centre channel, three coefficients; trig-free for cone beam) and keep, by an ordered ballot/prefix
-//     compaction into shared memory, the pixels with a tap inside the block (at most CB_CAP per pass).
-//  2. Accumulate: threads are grouped into "lane groups" of RL lanes (RL = rows handled at once, lanes run
-//     along detector rows, so each voxel-cylinder read is contiguous).  Every lane group owns a private copy
-//     of the tile rows it handles and walks a strided share of the compacted pixels, adding the three
-//     channel taps into its copy with plain shared-memory read-modify-writes: within a group lanes hold
-//     distinct rows, and no two groups share a copy, so there are no races and no atomics.  For cone beam
-//     each lane first evaluates the detector-row-centric vertical fan of the reference (cone_beam.py:347-372,
-//     including the 128-row batch anchor) for its row, reading the cylinder directly (L1-resident).
-//  3. Reduce: the private copies of each tile row are summed in a fixed order and written, coalesced.
+// One CTA owns an output block: one view x nb consecutive channels (nb = 32, 64 or 128) x all detector rows.
+// It walks the caller's pixel list in passes of at most `cap` kept pixels:
+//  1. Scan: the 256 threads compute each pixel's centre channel n_c (trig-free for cone beam) and keep, by an
+//     ordered ballot compaction, the pixels with a tap inside the block; bin = n_c - n0 + 1 in [0, nb + 1].
+//  2. Sort: a stable counting sort by bin (shared-memory histogram, warp-aggregated ranks from
+//     __match_any_sync), during which the kept pixels' footprints are computed and stored as sorted records.
+//     Each bin is padded to a multiple of 4 records with zero-weight copies of its first record, so the
+//     accumulation loop below reads records four at a time with no bounds tests.
+//  3. Accumulate: the bins are split into 8 contiguous ranges of about equal record counts, one per warp
+//     (at least two bins each).  Lanes run along detector rows (contiguous voxel-cylinder reads); when a
+//     block has fewer rows than a warp has lanes, the warp splits into ppw sub-groups that take different
+//     records of each group of four, each with a private tile copy.  A bin's records all tap the same three
+//     channels, so a lane sums them in three registers and, at the end of the bin, channel bin-2 is complete:
+//     it is added to the shared tile once per pass, not once per tap.  The first two and the last two channels
+//     of a warp's range also receive taps from the neighbouring warp; those partial sums are added in two
+//     phases (even warps, barrier, odd warps), so no channel has two writers at once.
+//  4. Write: the copies of each tile element are summed in a fixed order and written, coalesced.
+// For cone beam each lane evaluates the detector-row-centric vertical fan of the reference
+// (cone_beam.py:347-372, including the 128-row batch anchor) for its row, reading the cylinder directly.
 #pragma once
 
 #include <climits>
@@ -26,48 +33,96 @@
 namespace mbx {
 
 constexpr int CB_THREADS = 256;
-constexpr int CB_NB = 32;          // channels per block
-constexpr int CB_PITCH = CB_NB + 1;
-constexpr int CB_CAP = 1024;       // compacted pixels per pass
+constexpr int CB_WARPS = CB_THREADS / 32;
+constexpr int CB_QUAD = 4;  // bins are padded to a multiple of this many records
 
 struct CbPlan {
-    int rl;        // rows per lane group (power of two <= 32)
-    int lg_per_warp, groups;   // lane groups per warp, lane groups per CTA
-    int row_groups;            // ceil(R / rl)
-    int copies;                // private copies per row group (>= 1)
-    int cblocks;               // channel blocks per view
+    int nb;          // channels per block
+    int rl;          // lanes per record = rows per chunk (8, 16 or 32)
+    int ppw;         // sub-groups per warp = 32 / rl
+    int row_chunks;  // ceil(R / rl)
+    int rpad;        // row_chunks * rl
+    int pitch;       // tile row pitch (nb + 1)
+    int cap;         // records per pass, padding included
+    int fill;        // the scan stops adding pixels once a pass holds more than this many
+    int nbins;       // nb + 2
+    int cblocks;     // channel blocks per view
+    // shared-memory layout (4-byte words)
+    int o_rec, o_rec2, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_cone, o_misc;
     size_t smem;
     bool ok;
 };
 
-// Per compacted pixel record (structure of arrays in shared memory).
-struct CbList {
-    int *p;       // pixel position in the caller's list
-    int *nc;      // centre channel
-    float *a0, *a1, *a2;
-    float *imd;   // cone: 1 / (mag * delta_voxel)
-    float *wr;    // cone: W_r
-    float *mdz;   // cone: (mag / D) * delta_voxel
-    float *mz0;   // cone: (mag / D) * z_0
-};
+inline size_t cb_layout(CbPlan &pl, int kind, int R) {
+    size_t o = (size_t)pl.ppw * pl.rpad * pl.pitch;
+    o = (o + 3) & ~(size_t)3;
+    pl.o_rec = (int)o;
+    o += 4 * (size_t)pl.cap;
+    pl.o_rec2 = (int)o;
+    if (kind == MBX_GEOM_CONE) o += 4 * (size_t)pl.cap;
+    pl.o_ulist = (int)o;
+    o += pl.cap;
+    pl.o_ubin = (int)o;
+    o += pl.cap;
+    pl.o_bstart = (int)o;
+    o += pl.nbins + 1;
+    pl.o_run = (int)o;
+    o += pl.nbins;
+    pl.o_wcnt = (int)o;
+    o += (size_t)CB_WARPS * pl.nbins;
+    pl.o_cone = (int)o;
+    if (kind == MBX_GEOM_CONE) o += 3 * (size_t)R;
+    pl.o_misc = (int)o;
+    o += 2 * CB_WARPS;
+    return o * 4;
+}
 
-inline CbPlan plan_fp_cb(const mbx_geom &g) {
-    CbPlan pl;
+// num_views_sel: views per call (0 = all); min_blocks: CTAs wanted per call (a narrower channel block is
+// chosen to reach it); 0 = widest block.
+inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min_blocks = 0) {
+    CbPlan pl = {};
     pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || g.bp_psf_radius == 1);
-    const int R = g.num_det_rows;
-    int rl = 1;
-    while (rl < R && rl < 32) rl <<= 1;
-    pl.rl = rl;
-    pl.lg_per_warp = 32 / rl;
-    pl.groups = 8 * pl.lg_per_warp;
-    pl.row_groups = ceil_div(R, rl);
-    pl.copies = pl.groups >= pl.row_groups ? pl.groups / pl.row_groups : 1;
-    pl.cblocks = ceil_div(g.num_det_channels, CB_NB);
-    const size_t tile_words = (size_t)pl.row_groups * pl.copies * rl * CB_PITCH;
-    const size_t list_words = (size_t)CB_CAP * 9;
-    const size_t table_words = (g.kind == MBX_GEOM_CONE) ? (size_t)3 * R : 0;
-    pl.smem = (tile_words + list_words + table_words + 64) * 4;
-    if (pl.smem > 200 * 1024) pl.ok = false;
+    const int R = g.num_det_rows, C = g.num_det_channels;
+    // lanes per record: padded rows, weighted by the cost of ppw sub-groups
+    double best = 1e300;
+    for (int rl = 32; rl >= 8; rl >>= 1) {
+        const int ppw = 32 / rl;
+        const double over = ppw == 1 ? 1.0 : (ppw == 2 ? 1.15 : 1.4);
+        const double cost = (double)ceil_div(R, rl) * rl * over;
+        if (cost < best - 1e-9) {
+            best = cost;
+            pl.rl = rl;
+        }
+    }
+    pl.ppw = 32 / pl.rl;
+    pl.row_chunks = ceil_div(R, pl.rl);
+    pl.rpad = pl.row_chunks * pl.rl;
+    // widest channel block, then largest pass, that fit the shared-memory tier (2, then 1 CTA per SM: the
+    // registers of the accumulation loop allow no more than 2); a pass must hold at least 256 pixels after
+    // the padding and the last scan chunk are set aside
+    static const size_t tiers[2] = {112 * 1024, 200 * 1024};
+    bool found = false;
+    for (int t = 0; t < 2 && !found; ++t) {
+        for (int nb = 128; nb >= 32 && !found; nb >>= 1) {
+            const long long nv = num_views_sel > 0 ? num_views_sel : g.num_views;
+            if (nb > 32 && min_blocks > 0 && (long long)ceil_div(C, nb) * nv < min_blocks) continue;
+            for (int cap = 2048; cap >= 512 && !found; cap >>= 1) {
+                CbPlan q = pl;
+                q.nb = nb;
+                q.pitch = nb + 1;
+                q.cap = cap;
+                q.nbins = nb + 2;
+                q.fill = cap - CB_THREADS - (CB_QUAD - 1) * q.nbins;
+                q.cblocks = ceil_div(C, nb);
+                q.smem = cb_layout(q, g.kind, R);
+                if (q.fill >= 256 && q.smem <= tiers[t]) {
+                    pl = q;
+                    found = true;
+                }
+            }
+        }
+    }
+    if (!found) pl.ok = false;
     if (g.kind == MBX_GEOM_CONE) {
         const double half_r = 0.5 * (g.num_recon_rows - 1), half_c = 0.5 * (g.num_recon_cols - 1);
         const double rho = g.delta_voxel * std::sqrt(half_r * half_r + half_c * half_c);
@@ -77,7 +132,7 @@ inline CbPlan plan_fp_cb(const mbx_geom &g) {
     return pl;
 }
 
-// Fractional centre channel n_p of one pixel (the same arithmetic as cb_footprint, so both agree on round(n_p)).
+// Fractional centre channel n_p of one pixel.
 template <int KIND>
 __device__ __forceinline__ float cb_channel(const mbx_geom &g, float cs, float sn, float xt, float yt, float inv_d,
                                             float &mag) {
@@ -93,9 +148,10 @@ __device__ __forceinline__ float cb_channel(const mbx_geom &g, float cs, float s
     return (mag * x_p + g.det_channel_offset) * inv_dc + det_center_channel;
 }
 
-// Channel footprint of one pixel (trig-free for cone beam); also the cone vertical constants.
+// Channel footprint of one pixel whose centre channel nc was fixed by the scan (trig-free for cone beam);
+// also the cone vertical constants.
 template <int KIND>
-__device__ __forceinline__ void cb_footprint(const mbx_geom &g, float cs, float sn, float xt, float yt, int &nc,
+__device__ __forceinline__ void cb_footprint(const mbx_geom &g, float cs, float sn, float xt, float yt, int nc,
                                              float &a0, float &a1, float &a2, float &imd, float &wr, float &mdz,
                                              float &mz0) {
     const float inv_dc = 1.0f / g.delta_det_channel;
@@ -124,7 +180,6 @@ __device__ __forceinline__ void cb_footprint(const mbx_geom &g, float cs, float 
         mdz = mdd * g.delta_voxel;
         mz0 = mdd * z0;
     }
-    nc = (int)rintf(n_p);
     const float half_w = (w + 1.0f) * 0.5f, l_max = fminf(1.0f, w), d = n_p - (float)nc;
     float c[3];
 #pragma unroll
@@ -151,33 +206,147 @@ struct FpArgs {
     CbPlan plan;
 };
 
+// Detector-row constants of the cone vertical fan (one per lane).
+struct CbRow {
+    float vm, vb;
+    int b0;
+};
+
+// Value of one record for detector row m: the voxel itself (parallel) or the cone vertical fan.
+template <int KIND>
+__device__ __forceinline__ float cb_value(const float *cyl, int m, int num_slices, const float4 &cv,
+                                          const CbRow &rw, float kconst) {
+    if (KIND == MBX_GEOM_PARALLEL) return __ldg(cyl + m);
+    const float w_r = cv.y;
+    const float k_m = fmaf(rw.vm, cv.x, kconst);
+    const float k_m0 = fmaf(rw.vb, cv.x, kconst);
+    const int k_c = (int)rintf(k_m);
+    const float dm = fmaf(w_r, (float)k_c - k_m0, (float)(rw.b0 - m));
+    const float half_w = (w_r + 1.0f) * 0.5f, l_max = fminf(1.0f, w_r);
+    float val = 0.0f;
+#pragma unroll
+    for (int ko = -1; ko <= 1; ++ko) {
+        const int k = k_c + ko;
+        if (k >= 0 && k < num_slices) {
+            const float a = fminf(fmaxf(half_w - fabsf(fmaf(w_r, (float)ko, dm)), 0.0f), l_max);
+            const float t = fmaf((float)k, cv.z, cv.w);
+            const float q = fmaf(t, t, 1.0f);
+            val = fmaf(a, __ldg(cyl + k) * (q * rsqrtf(q)), val);
+        }
+    }
+    return val;
+}
+
+// What one warp needs to accumulate one pass.
+struct CbPass {
+    const float4 *rec, *rec2;  // sorted records (rec2: cone only)
+    const int *bstart;         // padded bin starts
+    float *tile;
+    const float *s_vm, *s_vb;  // cone row tables
+    const int *s_b0;
+    int b_lo, b_hi;            // this warp's bins
+};
+
+// Accumulation of one pass by one warp (PPW sub-groups of 32/PPW rows each), then the edge writes.
+template <int KIND, int PPW>
+__device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, int warp, int lane, float kconst) {
+    const mbx_geom &g = A.g;
+    const CbPlan &pl = A.plan;
+    constexpr int RL = 32 / PPW;
+    constexpr int U = CB_QUAD / PPW;  // records of a quad per lane
+    constexpr int QU = PPW;           // quads per iteration: U * QU = 4 loads in flight per lane
+    const int sub = lane / RL, lr = lane % RL;
+    const int num_rows = g.num_det_rows, num_slices = g.num_recon_slices, nb = pl.nb;
+    for (int rc = 0; rc < pl.row_chunks; ++rc) {
+        const int m = rc * RL + lr;
+        const int mc = min(m, num_rows - 1);  // rows past R read a valid row; their tile rows are never written out
+        CbRow rw = {0.f, 0.f, 0};
+        if (KIND == MBX_GEOM_CONE) {
+            rw.vm = P.s_vm[mc];
+            rw.vb = P.s_vb[mc];
+            rw.b0 = P.s_b0[mc];
+        }
+        float *trow = P.tile + ((size_t)sub * pl.rpad + m) * pl.pitch;
+        // before bin b: x = sum for channel b-2, y = sum for channel b-1; bin b adds s0/s1/s2 to b-2/b-1/b
+        float x = 0.f, y = 0.f, e0 = 0.f, e1 = 0.f;
+        for (int b = P.b_lo; b < P.b_hi; ++b) {
+            const int q0 = P.bstart[b], q1 = P.bstart[b + 1];
+            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
+            for (int i = q0; i < q1; i += CB_QUAD * QU) {
+                float4 rq[U * QU];
+                float vq[U * QU];
+#pragma unroll
+                for (int qq = 0; qq < QU; ++qq) {
+#pragma unroll
+                    for (int u = 0; u < U; ++u) {
+                        const int k = qq * U + u;
+                        const int ii = i + qq * CB_QUAD + sub * U + u;
+                        if (QU == 1 || i + qq * CB_QUAD < q1) {
+                            rq[k] = P.rec[ii];
+                            const float *cyl = A.vox + (long long)__float_as_int(rq[k].x) * num_slices;
+                            float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
+                            if (KIND == MBX_GEOM_CONE) cv = P.rec2[ii];
+                            vq[k] = cb_value<KIND>(cyl, mc, num_slices, cv, rw, kconst);
+                        } else {
+                            rq[k] = make_float4(0.f, 0.f, 0.f, 0.f);
+                            vq[k] = 0.0f;
+                        }
+                    }
+                }
+#pragma unroll
+                for (int k = 0; k < U * QU; ++k) {
+                    s0 = fmaf(rq[k].y, vq[k], s0);
+                    s1 = fmaf(rq[k].z, vq[k], s1);
+                    s2 = fmaf(rq[k].w, vq[k], s2);
+                }
+            }
+            // bin b is done: channel b-2 has all its taps from this warp's bins
+            const float done = x + s0;
+            x = y + s1;
+            y = s2;
+            const int f = b - P.b_lo;
+            if (f == 0)
+                e0 = done;
+            else if (f == 1)
+                e1 = done;
+            else
+                trow[b - 2] += done;  // interior channel: b_lo <= b-2 <= b_hi-3 < nb, one writer
+        }
+        // edge channels b_lo-2, b_lo-1 (partial: the warp below adds its part) and b_hi-2, b_hi-1 (partial: the
+        // warp above adds its part): even warps first, then odd warps, so no channel has two writers at once
+#pragma unroll
+        for (int ph = 0; ph < 2; ++ph) {
+            if (ph == 1) __syncthreads();
+            if ((warp & 1) == ph) {
+                if (P.b_lo >= 2) trow[P.b_lo - 2] += e0;
+                if (P.b_lo >= 1) trow[P.b_lo - 1] += e1;
+                if (P.b_hi - 2 < nb) trow[P.b_hi - 2] += x;
+                if (P.b_hi - 1 < nb) trow[P.b_hi - 1] += y;
+            }
+        }
+    }
+}
+
 template <int KIND>
 __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) {
     const mbx_geom &g = A.g;
     const CbPlan &pl = A.plan;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int num_rows = g.num_det_rows, num_channels = g.num_det_channels, num_slices = g.num_recon_slices;
-    const int n0 = cb * CB_NB;
-    const int rl = pl.rl;
-    const int row_groups = pl.row_groups, copies = pl.copies;
+    const int nb = pl.nb, nbins = pl.nbins, n0 = cb * nb;
 
-    float *tile = sm;  // [row_group][copy][rl][CB_PITCH]
-    const size_t tile_words = (size_t)row_groups * copies * rl * CB_PITCH;
-    CbList L;
-    L.p = reinterpret_cast<int *>(sm + tile_words);
-    L.nc = L.p + CB_CAP;
-    L.a0 = reinterpret_cast<float *>(L.nc + CB_CAP);
-    L.a1 = L.a0 + CB_CAP;
-    L.a2 = L.a1 + CB_CAP;
-    L.imd = L.a2 + CB_CAP;
-    L.wr = L.imd + CB_CAP;
-    L.mdz = L.wr + CB_CAP;
-    L.mz0 = L.mdz + CB_CAP;
-    float *s_vm = L.mz0 + CB_CAP;             // cone: [R] detector height of each row centre
-    float *s_vb = s_vm + num_rows;            // cone: [R] same at the row's 128-row batch start
-    int *s_b0 = reinterpret_cast<int *>(s_vb + num_rows);  // cone: [R] batch start row
-    int *s_misc = (KIND == MBX_GEOM_CONE) ? s_b0 + num_rows : reinterpret_cast<int *>(s_vm);
-    // s_misc[0..7]: warp counts, [8]: list count
+    float *tile = sm;  // [ppw][rpad][pitch]
+    float4 *rec = reinterpret_cast<float4 *>(sm + pl.o_rec);    // sorted {vox row (int bits), a0, a1, a2}
+    float4 *rec2 = reinterpret_cast<float4 *>(sm + pl.o_rec2);  // cone: sorted {imd, W_r, mdz, mz0}
+    int *ulist = reinterpret_cast<int *>(sm + pl.o_ulist);      // kept pixel positions, scan order
+    int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // their bins
+    int *bstart = reinterpret_cast<int *>(sm + pl.o_bstart);    // [nbins + 1] padded start of each bin
+    int *run = reinterpret_cast<int *>(sm + pl.o_run);          // [nbins] histogram, then placement cursor
+    int *wcnt = reinterpret_cast<int *>(sm + pl.o_wcnt);        // [warps][nbins] per-warp counts of a chunk
+    float *s_vm = sm + pl.o_cone;                               // cone: [R] detector height of each row centre
+    float *s_vb = s_vm + num_rows;                              // cone: [R] same at the row's 128-row batch start
+    int *s_b0 = reinterpret_cast<int *>(s_vb + num_rows);       // cone: [R] batch start row
+    int *s_misc = reinterpret_cast<int *>(sm + pl.o_misc);      // [2][warps]: warp counts, double-buffered
 
     const int vi = A.views ? A.views[j] : j;
     const bool view_ok = vi >= 0 && vi < g.num_views;
@@ -189,7 +358,9 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
 
     __syncthreads();  // previous tile of this CTA (batched use) is finished with shared memory
-    for (size_t i = tid; i < tile_words; i += CB_THREADS) tile[i] = 0.0f;
+    const int tile_words = pl.ppw * pl.rpad * pl.pitch;
+    for (int i = tid; i < tile_words; i += CB_THREADS) tile[i] = 0.0f;
+    for (int i = tid; i < CB_WARPS * nbins; i += CB_THREADS) wcnt[i] = 0;
     if (KIND == MBX_GEOM_CONE) {
         int rows_per_batch = g.entries_per_cylinder_batch;
         if (rows_per_batch > num_rows) rows_per_batch = num_rows;
@@ -202,21 +373,20 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
         }
     }
 
-    // lane group of this thread
-    const int lg = warp * pl.lg_per_warp + lane / rl;   // 0 .. groups-1
-    const int lr = lane % rl;                            // row within the group
     const int npix_grid = g.num_recon_rows * g.num_recon_cols;
     long long scan = 0;
     const long long num_pixels = view_ok ? A.num_pixels : 0;
 
     while (scan < num_pixels) {
-        // ---- 1. compaction of the pixels that touch this channel block (ordered)
-        int count = 0;
-        __syncthreads();  // the previous pass is done with the list
-        const int count0 = count;
-        while (scan < num_pixels && count <= CB_CAP - CB_THREADS) {
+        __syncthreads();  // the previous pass is done with every list
+        for (int b = tid; b < nbins; b += CB_THREADS) run[b] = 0;
+        __syncthreads();
+        // ---- 1. ordered compaction of the pixels that touch this channel block
+        int count = 0, par = 0;
+        while (scan < num_pixels && count <= pl.fill) {
             const long long p = scan + tid;
             bool take = false;
+            int bin = 0;
             if (p < num_pixels) {
                 const int idx = A.pix[p];
                 if (idx < 0 || idx >= npix_grid) {
@@ -225,101 +395,160 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
                     float xt, yt, mag;
                     pixel_tilde_fast(g, idx, inv_cols, xt, yt);
                     const int nc = (int)rintf(cb_channel<KIND>(g, cs, sn, xt, yt, inv_d, mag));
-                    take = nc + 1 >= n0 && nc - 1 < n0 + CB_NB;
+                    bin = nc - n0 + 1;
+                    take = bin >= 0 && bin < nbins;
                 }
             }
             const unsigned ballot = __ballot_sync(0xffffffffu, take);
-            if (lane == 0) s_misc[warp] = __popc(ballot);
+            int *wc = s_misc + par * CB_WARPS;  // the other buffer is still being read by slower warps
+            if (lane == 0) wc[warp] = __popc(ballot);
             __syncthreads();
-            int base = count;
-            for (int w = 0; w < warp; ++w) base += s_misc[w];
-            int total = 0;
-            for (int w = 0; w < 8; ++w) total += s_misc[w];
-            if (take) L.p[base + __popc(ballot & ((1u << lane) - 1u))] = (int)p;
+            int base = count, total = 0;
+#pragma unroll
+            for (int w = 0; w < CB_WARPS; ++w) {
+                const int c = wc[w];
+                base += (w < warp) ? c : 0;
+                total += c;
+            }
+            if (take) {
+                const int pos = base + __popc(ballot & ((1u << lane) - 1u));
+                ulist[pos] = (int)p;
+                ubin[pos] = bin;
+                atomicAdd(run + bin, 1);  // integer histogram: order-independent
+            }
             count += total;
             scan += CB_THREADS;
-            __syncthreads();
-        }
-        // footprints of the kept pixels only (dense, no divergence)
-        for (int i = count0 + tid; i < count; i += CB_THREADS) {
-            const int p = L.p[i];
-            const int idx = A.pix[p];
-            float xt, yt;
-            pixel_tilde_fast(g, idx, inv_cols, xt, yt);
-            int nc;
-            float a0, a1, a2, imd, wr, mdz, mz0;
-            cb_footprint<KIND>(g, cs, sn, xt, yt, nc, a0, a1, a2, imd, wr, mdz, mz0);
-            L.p[i] = A.vox_by_index ? idx : p;  // row of vox holding this pixel's cylinder
-            L.nc[i] = nc;
-            L.a0[i] = a0;
-            L.a1[i] = a1;
-            L.a2[i] = a2;
-            L.imd[i] = imd;
-            L.wr[i] = wr;
-            L.mdz[i] = mdz;
-            L.mz0[i] = mz0;
+            par ^= 1;
         }
         __syncthreads();
-        // ---- 2. accumulation into the private copy of each lane group
-        for (int rg = lg / copies; rg < row_groups; rg += (pl.groups >= row_groups ? row_groups : pl.groups)) {
-            // with copies > 1 the lane groups of a row group split the pixel list; else each group walks them all
-            const int copy = (pl.groups >= row_groups) ? lg % copies : 0;
-            if (pl.groups >= row_groups && lg >= row_groups * copies) break;
-            const int m = rg * rl + lr;
-            float *trow = tile + (((size_t)rg * copies + copy) * rl + lr) * CB_PITCH;
-            if (m < num_rows) {
-                float vm = 0.f, vb = 0.f;
-                int b0 = 0;
-                if (KIND == MBX_GEOM_CONE) {
-                    vm = s_vm[m];
-                    vb = s_vb[m];
-                    b0 = s_b0[m];
-                }
-                for (int i = copy; i < count; i += copies) {
-                    const int nc = L.nc[i];
-                    const float *cyl = A.vox + (long long)L.p[i] * num_slices;
-                    float val;
-                    if (KIND == MBX_GEOM_PARALLEL) {
-                        val = __ldg(cyl + m);
-                    } else {
-                        const float imd = L.imd[i], w_r = L.wr[i];
-                        const float k_m = fmaf(vm, imd, kconst);
-                        const float k_m0 = fmaf(vb, imd, kconst);
-                        const int k_c = (int)rintf(k_m);
-                        const float dm = fmaf(w_r, (float)k_c - k_m0, (float)(b0 - m));
-                        const float half_w = (w_r + 1.0f) * 0.5f, l_max = fminf(1.0f, w_r);
-                        const float mdz = L.mdz[i], mz0 = L.mz0[i];
-                        val = 0.0f;
+        if (count == 0) continue;
+        // ---- 2a. padded bin starts: exclusive scan of the rounded-up histogram (warp 0); run[] becomes the
+        //          placement cursor
+        if (warp == 0) {
+            const int per = (nbins + 31) / 32;
+            int loc = 0;
+            for (int k = 0; k < per; ++k) {
+                const int b = lane * per + k;
+                if (b < nbins) loc += (run[b] + CB_QUAD - 1) & ~(CB_QUAD - 1);
+            }
+            int incl = loc;
 #pragma unroll
-                        for (int ko = -1; ko <= 1; ++ko) {
-                            const int k = k_c + ko;
-                            if (k >= 0 && k < num_slices) {
-                                const float a = fminf(fmaxf(half_w - fabsf(fmaf(w_r, (float)ko, dm)), 0.0f), l_max);
-                                const float t = fmaf((float)k, mdz, mz0);
-                                const float q = fmaf(t, t, 1.0f);
-                                val = fmaf(a, __ldg(cyl + k) * (q * rsqrtf(q)), val);
-                            }
-                        }
-                    }
-                    const int c = nc - n0;  // column of the centre tap
-                    if (c - 1 >= 0 && c - 1 < CB_NB) trow[c - 1] = fmaf(L.a0[i], val, trow[c - 1]);
-                    if (c >= 0 && c < CB_NB) trow[c] = fmaf(L.a1[i], val, trow[c]);
-                    if (c + 1 >= 0 && c + 1 < CB_NB) trow[c + 1] = fmaf(L.a2[i], val, trow[c + 1]);
+            for (int off = 1; off < 32; off <<= 1) {
+                const int t = __shfl_up_sync(0xffffffffu, incl, off);
+                if (lane >= off) incl += t;
+            }
+            int acc = incl - loc;
+            for (int k = 0; k < per; ++k) {
+                const int b = lane * per + k;
+                if (b < nbins) {
+                    const int h = run[b];
+                    bstart[b] = acc;
+                    run[b] = acc;
+                    acc += (h + CB_QUAD - 1) & ~(CB_QUAD - 1);
                 }
             }
-            if (pl.groups >= row_groups) break;
+            if (lane == 31) bstart[nbins] = incl;
         }
+        __syncthreads();
+        // ---- 2b. stable placement by bin, computing the footprints on the way
+        for (int base = 0; base < count; base += CB_THREADS) {
+            const int i = base + tid;
+            const bool valid = i < count;
+            const int b = valid ? ubin[i] : -1;
+            const unsigned peers = __match_any_sync(0xffffffffu, b);
+            const int rank = __popc(peers & ((1u << lane) - 1u));
+            if (valid && rank == 0) wcnt[warp * nbins + b] = __popc(peers);
+            __syncthreads();
+            if (valid) {
+                int pos = run[b] + rank;
+                for (int w = 0; w < warp; ++w) pos += wcnt[w * nbins + b];
+                const int p = ulist[i];
+                const int idx = A.pix[p];
+                float xt, yt;
+                pixel_tilde_fast(g, idx, inv_cols, xt, yt);
+                float a0, a1, a2, imd, wr, mdz, mz0;
+                cb_footprint<KIND>(g, cs, sn, xt, yt, n0 + b - 1, a0, a1, a2, imd, wr, mdz, mz0);
+                rec[pos] = make_float4(__int_as_float(A.vox_by_index ? idx : p), a0, a1, a2);
+                if (KIND == MBX_GEOM_CONE) rec2[pos] = make_float4(imd, wr, mdz, mz0);
+            }
+            __syncthreads();
+            for (int bb = tid; bb < nbins; bb += CB_THREADS) {
+                int t = 0;
+                for (int w = 0; w < CB_WARPS; ++w) {
+                    t += wcnt[w * nbins + bb];
+                    wcnt[w * nbins + bb] = 0;
+                }
+                run[bb] += t;
+            }
+            __syncthreads();
+        }
+        // ---- 2c. padding: zero-weight copies of each bin's first record up to the next multiple of 4
+        for (int b = tid; b < nbins; b += CB_THREADS) {
+            const int d0 = run[b], d1 = bstart[b + 1];
+            if (d0 < d1) {
+                const float4 r0 = rec[bstart[b]];
+                for (int d = d0; d < d1; ++d) rec[d] = make_float4(r0.x, 0.f, 0.f, 0.f);
+                if (KIND == MBX_GEOM_CONE) {
+                    const float4 c0 = rec2[bstart[b]];
+                    for (int d = d0; d < d1; ++d) rec2[d] = c0;
+                }
+            }
+        }
+        __syncthreads();
+        // ---- 3. warp ranges of bins with about equal record counts, at least two bins each:
+        //         B_v = 2v + max_{u<=v}(lb_u - 2u), then B_v <= nbins - 2(8 - v); lb_v = first bin starting at or
+        //         after v/8 of the records
+        CbPass P;
+        {
+            const int tot = bstart[nbins];
+            int lb = 0;
+            if (lane <= CB_WARPS) {
+                const int target = (int)(((long long)lane * tot) / CB_WARPS);
+                int lo = 0, hi = nbins;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (bstart[mid] >= target)
+                        hi = mid;
+                    else
+                        lo = mid + 1;
+                }
+                lb = lo;
+            }
+            int t = (lane <= CB_WARPS) ? lb - 2 * lane : INT_MIN / 2;
+#pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, t, off);
+                if (lane >= off) t = max(t, u);
+            }
+            int bv = min(2 * lane + t, nbins - 2 * (CB_WARPS - lane));
+            if (lane == CB_WARPS) bv = nbins;
+            P.b_lo = __shfl_sync(0xffffffffu, bv, warp);
+            P.b_hi = __shfl_sync(0xffffffffu, bv, warp + 1);
+        }
+        P.rec = rec;
+        P.rec2 = rec2;
+        P.bstart = bstart;
+        P.tile = tile;
+        P.s_vm = s_vm;
+        P.s_vb = s_vb;
+        P.s_b0 = s_b0;
+        if (pl.ppw == 1)
+            cb_accumulate<KIND, 1>(A, P, warp, lane, kconst);
+        else if (pl.ppw == 2)
+            cb_accumulate<KIND, 2>(A, P, warp, lane, kconst);
+        else
+            cb_accumulate<KIND, 4>(A, P, warp, lane, kconst);
     }
     __syncthreads();
-    // ---- 3. fixed-order sum of the private copies, coalesced write
-    const int nch = min(CB_NB, num_channels - n0);
+    // ---- 4. fixed-order sum of the sub-group copies, coalesced write
+    const int nch = min(nb, num_channels - n0);
+    const int ppw = pl.ppw;
     float *out = A.out + (long long)j * num_rows * num_channels + n0;
-    for (int e = tid; e < num_rows * CB_NB; e += CB_THREADS) {
-        const int m = e / CB_NB, c = e - (e / CB_NB) * CB_NB;
+    for (int e = tid; e < num_rows * nb; e += CB_THREADS) {
+        const int m = e / nb, c = e - (e / nb) * nb;
         if (c >= nch) continue;
-        const int rg = m / rl, lr2 = m - rg * rl;
         float s = 0.0f;
-        for (int cp = 0; cp < copies; ++cp) s += tile[(((size_t)rg * copies + cp) * rl + lr2) * CB_PITCH + c];
+        for (int k = 0; k < ppw; ++k) s += tile[((size_t)k * pl.rpad + m) * pl.pitch + c];
         out[(long long)m * num_channels + c] = s;
     }
 }

@@ -530,7 +530,8 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
         }
         for (int s = 0; s < num_scans; ++s) {
             const mbx_geom &g = scans[s].geom;
-            cost[s] = ((double)scans[s].subset_size * (CB_NB + 2) / g.num_det_channels + 1.0) * g.num_det_rows;
+            cost[s] = (double)scans[s].subset_size *
+                      (2.0 + (double)(zs[s].fpp.nb + 2) * zs[s].fpp.rpad / g.num_det_channels);
             ord[s] = s;
         }
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
