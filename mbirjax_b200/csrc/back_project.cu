@@ -52,9 +52,7 @@ static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const fl
     A.out = dst;
     A.split_stride = ss;
     A.out_by_index = 0;
-    A.nsl = pl.nsl;
-    A.npg = pl.npg;
-    A.vc = pl.vc;
+    A.plan = pl;
     dim3 grid(pl.gx, pl.gy, pl.splits);
     kern<<<grid, BPF_THREADS, pl.smem, st>>>(A, device_error_ptr());
     note_launch();

@@ -2,18 +2,21 @@
 // detector pitch at the magnification), for parallel and cone beam.  Same contract and arithmetic as the
 // general bp_kernel (back_project.cuh); organised to minimise instructions per (pixel, slice, view):
 //
-//  * CTA = 256 threads = 8 warps; lanes run along 32 pixels, warps along slice tiles of ST slices (or along
-//    further pixel groups when the cylinder has fewer than 8 tiles).  Accumulators stay in registers.
-//  * Per chunk of views, each (pixel, view) footprint is computed once, by one thread, into shared memory and
-//    read by every warp of that pixel: centre channel, the three channel coefficients (already raised to
-//    coeff_power) and, for cone beam, the affine map slice -> detector row m_p(k) = A0 + k*A1 and the
-//    vertical-angle factor c2 = (mag/D)^2 so that 1/cos(phi_k) = sqrt(1 + c2 z_k^2).  The cone footprint is
-//    trig-free: cos/sin(theta - theta_p) and 1/cos(theta_p) come from the per-view cos/sin and
-//    rsqrt(D^2 + u^2) instead of atan2/cos/sin per pixel.
+//  * CTA = 256 threads = 8 warps; lanes run along 32 pixels, warps along slice tiles (or along further pixel
+//    groups when the cylinder has fewer than 8 tiles).  The tile height ts <= 16 is chosen so that the tiles
+//    split the slices evenly over a power-of-two number of warps; accumulators stay in registers.
+//  * Per chunk of views, each (pixel, view) footprint is computed once, by one thread, into shared memory as
+//    one float4 and read by every warp of that pixel: the first of three consecutive detector channels that
+//    hold every nonzero tap and their coefficients (already raised to coeff_power; at the detector edges the
+//    taps are shifted onto in-range channels with a zero coefficient, so every gather is three loads at
+//    constant offsets from one pointer), plus for cone beam the affine map slice -> detector row
+//    m_p(k) = A0 + k*A1 and the vertical-angle factor c2 = (mag/D)^2 so that 1/cos(phi_k) = sqrt(1 + c2 z_k^2).
+//    The cone footprint is trig-free: cos/sin(theta - theta_p) and 1/cos(theta_p) come from the per-view
+//    cos/sin and rsqrt(D^2 + u^2) instead of atan2/cos/sin per pixel.
 //  * Cone: every detector row a warp's slice tile touches is gathered once per view into the thread's column
 //    of a shared-memory row cache ([row][thread], conflict-free), rows outside the detector cached as 0; the
 //    vertical fan then reads three cached rows per slice with no bounds tests.  plan_bp_fast admits a geometry
-//    only when the rows of a slice tile (ST * max |dm/dk| + 4) fit the cache.
+//    only when the rows of a slice tile (ts * max |dm/dk| + 4) fit the cache.
 #pragma once
 
 #include "back_project.cuh"
@@ -21,38 +24,44 @@
 namespace mbx {
 
 constexpr int BPF_THREADS = 256;
-constexpr int BPF_ST = 16;          // slices per thread
-constexpr int BPF_CACHE_ROWS = 48;  // row-cache depth per thread (cone): ST * max|dm/dk| + 4 must fit
+constexpr int BPF_ST = 16;          // most slices per thread
+constexpr int BPF_CACHE_ROWS = 48;  // row-cache depth per thread (cone): ts * max|dm/dk| + 4 must fit
+#ifndef MBX_BPF_CHUNK_PARALLEL
+#define MBX_BPF_CHUNK_PARALLEL 1024     // footprints staged per view chunk, parallel beam
+#endif
+#ifndef MBX_BPF_CHUNK_CONE
+#define MBX_BPF_CHUNK_CONE 512          // same, cone beam (its row cache takes most of the shared memory)
+#endif
 
 struct BpfPlan {
-    int nsl;    // slice tiles per CTA (warps per pixel group)
-    int npg;    // pixel groups of 32 per CTA
-    int vc;     // views per footprint chunk
+    int nsl;      // slice tiles per CTA (warps per pixel group)
+    int npg;      // pixel groups of 32 per CTA
+    int lg_pcta;  // log2(32 * npg)
+    int chunk;    // footprints staged per view chunk (a multiple of BPF_THREADS)
+    int vc;       // views per chunk = chunk / (32 * npg)
+    int ts;       // slices per tile (<= BPF_ST)
+    int tiles;    // ceil(S / ts)
     int gx, gy, splits, views_per_split;
     size_t smem, workspace;
     bool ok;
 };
 
-// Footprint record in shared memory (structure of arrays, [vc][pixels]).
-struct BpfShared {
-    int *nc;
-    float *a0, *a1, *a2, *A0, *A1, *c2;
-};
-
+// Footprint of one (pixel, view): fa = {first channel (int bits; -1: no tap), c0, c1, c2} for the channels
+// first, first+1, first+2; fb (cone) = {A0, A1, c2 = (mag/D)^2, 0}.
 template <int KIND>
 __device__ __forceinline__ void bpf_footprint(const mbx_geom &g, float cs, float sn, float x_tilde, float y_tilde,
-                                              int coeff_power, int &nc, float &a0, float &a1, float &a2, float &A0,
-                                              float &A1, float &c2) {
+                                              int coeff_power, float4 &fa, float4 &fb) {
     const float inv_dc = 1.0f / g.delta_det_channel;
-    const float det_center_channel = 0.5f * (float)(g.num_det_channels - 1);
+    const int num_channels = g.num_det_channels;
+    const float det_center_channel = 0.5f * (float)(num_channels - 1);
     float n_p, w, scale;  // scale = delta_voxel / cos_alpha
+    fb = make_float4(0.f, 0.f, 0.f, 0.f);
     if (KIND == MBX_GEOM_PARALLEL) {
         const float x = cs * x_tilde - sn * y_tilde;
         n_p = (x + g.det_channel_offset) * inv_dc + det_center_channel;
         const float cos_alpha = fmaxf(fabsf(cs), fabsf(sn));
         w = (g.delta_voxel * inv_dc) * cos_alpha;
         scale = g.delta_voxel / cos_alpha;
-        A0 = A1 = c2 = 0.0f;
     } else {
         const float x_p = cs * x_tilde - sn * y_tilde;
         const float y_p = sn * x_tilde + cs * y_tilde;
@@ -72,38 +81,35 @@ __device__ __forceinline__ void bpf_footprint(const mbx_geom &g, float cs, float
         const float inv_dr = 1.0f / g.delta_det_row;
         const float center_slice = 0.5f * (float)(g.num_recon_slices - 1);
         const float z0 = g.recon_slice_offset - g.delta_voxel * center_slice;
-        A1 = mag * g.delta_voxel * inv_dr;
-        A0 = (mag * z0 + g.det_row_offset) * inv_dr + 0.5f * (float)(g.num_det_rows - 1);
         const float mr = mag * inv_d;
-        c2 = mr * mr;
+        fb.x = (mag * z0 + g.det_row_offset) * inv_dr + 0.5f * (float)(g.num_det_rows - 1);
+        fb.y = mag * g.delta_voxel * inv_dr;
+        fb.z = mr * mr;
     }
-    nc = (int)rintf(n_p);
+    const int nc = (int)rintf(n_p);
     const float half_w = (w + 1.0f) * 0.5f;
     const float l_max = fminf(1.0f, w);
     const float d = n_p - (float)nc;
-    float c[3];
+    float a[3];
 #pragma unroll
     for (int k = -1; k <= 1; ++k) {
         const int n = nc + k;
-        float a = scale * fminf(fmaxf(half_w - fabsf(d - (float)k), 0.0f), l_max);
-        if (n < 0 || n >= g.num_det_channels) a = 0.0f;
-        c[k + 1] = (coeff_power == 2) ? a * a : a;
+        float v = scale * fminf(fmaxf(half_w - fabsf(d - (float)k), 0.0f), l_max);
+        if (n < 0 || n >= num_channels) v = 0.0f;
+        a[k + 1] = (coeff_power == 2) ? v * v : v;
     }
-    a0 = c[0];
-    a1 = c[1];
-    a2 = c[2];
-}
-
-// sum_k a_k * (w * sino)[row, nc + k], the three taps gathered with clamped (in-range) addresses.
-__device__ __forceinline__ float bpf_row(const float *__restrict__ row, const float *__restrict__ wrow, int n0, int n1,
-                                         int n2, float a0, float a1, float a2) {
-    float v0 = __ldg(row + n0), v1 = __ldg(row + n1), v2 = __ldg(row + n2);
-    if (wrow) {
-        v0 *= __ldg(wrow + n0);
-        v1 *= __ldg(wrow + n1);
-        v2 *= __ldg(wrow + n2);
+    // channels first..first+2 on the detector; tap k of the pixel sits at position k - (first - (nc - 1))
+    const int lo = nc - 1;
+    const int first = min(max(lo, 0), num_channels - 3);
+    const int sh = first - lo;
+    float c[3];
+#pragma unroll
+    for (int k = 0; k < 3; ++k) {
+        const int j = k + sh;
+        c[k] = (j == 0) ? a[0] : ((j == 1) ? a[1] : ((j == 2) ? a[2] : 0.0f));
     }
-    return fmaf(a0, v0, fmaf(a1, v1, a2 * v2));
+    const bool any = c[0] != 0.0f || c[1] != 0.0f || c[2] != 0.0f;
+    fa = make_float4(__int_as_float(any ? first : -1), c[0], c[1], c[2]);
 }
 
 // Arguments of one back projection (one scan).
@@ -120,50 +126,44 @@ struct BpArgs {
     float *out;                // (num_pixels, S) in list order, or a flat recon when out_by_index
     long long split_stride;    // 0: final output; else partial-sum workspace stride
     int out_by_index;
-    int nsl, npg, vc;
+    BpfPlan plan;
 };
 
 template <int KIND>
 __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf, int *err) {
     const mbx_geom &g = A.g;
+    const BpfPlan &P = A.plan;
     const float *__restrict__ sino = A.sino;
     const float *__restrict__ wts = A.wts;
     const int32_t *__restrict__ pix = A.pix;
     const long long num_pixels = A.num_pixels;
     const int32_t *__restrict__ views = A.views;
     const int num_views_sel = A.num_views_sel, views_per_split = A.views_per_split, coeff_power = A.coeff_power;
-    const int nsl = A.nsl, npg = A.npg, vc = A.vc;
-    const int pcta = 32 * npg;                       // pixels per CTA
-    const int nfp = vc * pcta;                       // footprints per chunk
-    BpfShared sh;
-    sh.nc = reinterpret_cast<int *>(smf);
-    sh.a0 = smf + nfp;
-    sh.a1 = smf + 2 * nfp;
-    sh.a2 = smf + 3 * nfp;
-    sh.A0 = smf + 4 * nfp;
-    sh.A1 = smf + 5 * nfp;
-    sh.c2 = smf + 6 * nfp;
-    float *s_cs = smf + 7 * nfp;
+    const int nsl = P.nsl, vc = P.vc, lg_pcta = P.lg_pcta, chunk = P.chunk;
+    const int pcta = 1 << lg_pcta;                  // pixels per CTA
+    float4 *s_fa = reinterpret_cast<float4 *>(smf);  // [chunk] = [view in chunk][pixel]
+    float4 *s_fb = s_fa + chunk;                     // cone: [chunk]
+    float *s_cs = reinterpret_cast<float *>(s_fa + (KIND == MBX_GEOM_CONE ? 2 : 1) * chunk);
     float *s_sn = s_cs + vc;
     int *s_vi = reinterpret_cast<int *>(s_sn + vc);
     float *cache = reinterpret_cast<float *>(s_vi + vc);  // [BPF_CACHE_ROWS][BPF_THREADS] (cone)
-    // 16-byte alignment of the cache is not needed (scalar accesses)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pg = warp / nsl, stl = warp - pg * nsl;
     const int pl = pg * 32 + lane;                                   // pixel within CTA
     const long long slot = (long long)bx * pcta + pl;
     const long long p = (A.order && slot < num_pixels) ? A.order[slot] : slot;  // list entry of this thread
-    const int s0 = (by * nsl + stl) * BPF_ST;
+    const int s0 = (by * nsl + stl) * P.ts;
     const int num_rows = g.num_det_rows, num_channels = g.num_det_channels, num_slices = g.num_recon_slices;
-    const int ns = min(BPF_ST, num_slices - s0);
+    const int ns = min(P.ts, num_slices - s0);
     const int split = bz;
     const int v_begin = split * views_per_split;
     const int v_end = min(num_views_sel, v_begin + views_per_split);
     const int npix_grid = g.num_recon_rows * g.num_recon_cols;
+    const long long view_stride = (long long)num_rows * num_channels;
 
-    // pixel geometry of the pixel this thread computes footprints for (pixel tid % pcta)
-    const int fpl = tid % pcta;
+    // pixel geometry of the pixel this thread computes footprints for (pixel tid % pcta of every view)
+    const int fpl = tid & (pcta - 1);
     const long long fp_slot = (long long)bx * pcta + fpl;
     const long long fp_pixel = (A.order && fp_slot < num_pixels) ? A.order[fp_slot] : fp_slot;
     float fxt = 0.0f, fyt = 0.0f;
@@ -203,66 +203,53 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             s_sn[tid] = sinf(ang);
         }
         __syncthreads();
-        for (int f = tid; f < nv * pcta; f += BPF_THREADS) {
-            const int t = f / pcta;
-            int nc = INT_MIN;
-            float a0 = 0.f, a1 = 0.f, a2 = 0.f, A0 = 0.f, A1 = 0.f, c2 = 0.f;
-            if (fvalid && s_vi[t] >= 0)
-                bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, nc, a0, a1, a2, A0, A1, c2);
-            sh.nc[f] = nc;
-            sh.a0[f] = a0;
-            sh.a1[f] = a1;
-            sh.a2[f] = a2;
-            sh.A0[f] = A0;
-            sh.A1[f] = A1;
-            sh.c2[f] = c2;
+        for (int f = tid; f < chunk; f += BPF_THREADS) {
+            const int t = f >> lg_pcta;
+            if (t < nv) {
+                float4 fa = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f), fb = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (fvalid && s_vi[t] >= 0) bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb);
+                s_fa[f] = fa;
+                if (KIND == MBX_GEOM_CONE) s_fb[f] = fb;
+            }
         }
         __syncthreads();
         if (!active) continue;
         for (int t = 0; t < nv; ++t) {
-            const int f = t * pcta + pl;
-            const int nc = sh.nc[f];
-            if (nc == INT_MIN) continue;
-            const int vi = s_vi[t];
-            const float a0 = sh.a0[f], a1 = sh.a1[f], a2 = sh.a2[f];
-            const int n0 = min(max(nc - 1, 0), num_channels - 1);
-            const int n1 = min(max(nc, 0), num_channels - 1);
-            const int n2 = min(max(nc + 1, 0), num_channels - 1);
-            const float *view = sino + (long long)vi * num_rows * num_channels;
-            const float *wview = wts ? wts + (long long)vi * num_rows * num_channels : nullptr;
+            const int f = (t << lg_pcta) + pl;
+            const float4 fa = s_fa[f];
+            const int first = __float_as_int(fa.x);
+            if (first < 0) continue;
+            const long long voff = (long long)s_vi[t] * view_stride;
             if (KIND == MBX_GEOM_PARALLEL) {
-                const long long rowoff = (long long)s0 * num_channels;
-                if (nc >= 1 && nc + 1 < num_channels && ns == BPF_ST) {
-                    // all three taps on the detector and a full slice tile: one pointer, constant tap offsets
-                    const float *p = view + rowoff + (nc - 1);
-                    if (wview) {
-                        const float *q = wview + rowoff + (nc - 1);
-#pragma unroll
-                        for (int s = 0; s < BPF_ST; ++s) {
-                            acc[s] = fmaf(a0, __ldg(p) * __ldg(q),
-                                          fmaf(a1, __ldg(p + 1) * __ldg(q + 1), fmaf(a2, __ldg(p + 2) * __ldg(q + 2), acc[s])));
-                            p += num_channels;
-                            q += num_channels;
-                        }
-                    } else {
-#pragma unroll
-                        for (int s = 0; s < BPF_ST; ++s) {
-                            acc[s] = fmaf(a0, __ldg(p), fmaf(a1, __ldg(p + 1), fmaf(a2, __ldg(p + 2), acc[s])));
-                            p += num_channels;
-                        }
-                    }
-                } else {
-                    const float *row = view + rowoff;
-                    const float *wrow = wview ? wview + rowoff : nullptr;
+                // three taps at constant offsets from one pointer, one detector row per slice
+                const long long off = voff + (long long)s0 * num_channels + first;
+                const float *q = sino + off;
+                if (wts) {
+                    const float *qw = wts + off;
 #pragma unroll
                     for (int s = 0; s < BPF_ST; ++s) {
-                        if (s < ns) acc[s] += bpf_row(row, wrow, n0, n1, n2, a0, a1, a2);
-                        row += num_channels;
-                        if (wrow) wrow += num_channels;
+                        if (s < ns)
+                            acc[s] = fmaf(fa.y, __ldg(q) * __ldg(qw),
+                                          fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fmaf(fa.w, __ldg(q + 2) * __ldg(qw + 2), acc[s])));
+                        q += num_channels;
+                        qw += num_channels;
+                    }
+                } else if (ns == BPF_ST) {  // full tile: no guards
+#pragma unroll
+                    for (int s = 0; s < BPF_ST; ++s) {
+                        acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
+                        q += num_channels;
+                    }
+                } else {
+#pragma unroll
+                    for (int s = 0; s < BPF_ST; ++s) {
+                        if (s < ns) acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
+                        q += num_channels;
                     }
                 }
             } else {
-                const float A0 = sh.A0[f], A1 = sh.A1[f], c2 = sh.c2[f];
+                const float4 fb = s_fb[f];
+                const float A0 = fb.x, A1 = fb.y, c2 = fb.z;
                 const float half_w = (A1 + 1.0f) * 0.5f;
                 const float l_max = fminf(1.0f, A1);
                 const int mc_first = (int)rintf(fmaf((float)s0, A1, A0));
@@ -276,8 +263,14 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 for (int m = m_lo; m <= m_hi; ++m) {
                     float c = 0.0f;
                     if (m >= 0 && m < num_rows) {
-                        const long long off = (long long)m * num_channels;
-                        c = bpf_row(view + off, wview ? wview + off : nullptr, n0, n1, n2, a0, a1, a2);
+                        const long long off = voff + (long long)m * num_channels + first;
+                        const float *q = sino + off;
+                        if (wts) {
+                            const float *qw = wts + off;
+                            c = fmaf(fa.y, __ldg(q) * __ldg(qw), fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fa.w * (__ldg(q + 2) * __ldg(qw + 2))));
+                        } else {
+                            c = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fa.w * __ldg(q + 2)));
+                        }
                     }
                     mycache[(m - m_lo) * BPF_THREADS] = c;
                 }
@@ -328,23 +321,38 @@ __global__ void __launch_bounds__(BPF_THREADS, 3) bp_fast_kernel(const BpArgs A,
 
 inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_views_sel) {
     BpfPlan pl;
-    pl.ok = (g.psf_radius == 1);
+    pl.ok = (g.psf_radius == 1) && g.num_det_channels >= 3;
     const int S = g.num_recon_slices;
-    const int tiles = ceil_div(S, BPF_ST);
-    pl.nsl = tiles >= 8 ? 8 : (tiles >= 4 ? 4 : (tiles >= 2 ? 2 : 1));
+    // tile height: the fewest tiles of <= BPF_ST slices, rounded up to a power of two (<= 8) or a multiple of 8,
+    // then the slices spread evenly over them
+    const int t0 = ceil_div(S, BPF_ST);
+    int T = 1;
+    if (t0 <= 8) {
+        while (T < t0) T <<= 1;
+    } else {
+        T = ceil_div(t0, 8) * 8;
+    }
+    pl.ts = ceil_div(S, T);
+    pl.tiles = ceil_div(S, pl.ts);
+    pl.nsl = 1;
+    while (pl.nsl < pl.tiles && pl.nsl < 8) pl.nsl <<= 1;
     pl.npg = 8 / pl.nsl;
-    pl.vc = pl.nsl;  // footprints per chunk = 256
+    pl.lg_pcta = 5;
+    while ((1 << pl.lg_pcta) < 32 * pl.npg) ++pl.lg_pcta;
     const int pcta = 32 * pl.npg;
+    pl.chunk = (g.kind == MBX_GEOM_CONE) ? MBX_BPF_CHUNK_CONE : MBX_BPF_CHUNK_PARALLEL;
+    if (pl.chunk < pcta) pl.chunk = pcta;
+    pl.vc = pl.chunk / pcta;
     pl.gx = ceil_div(num_pixels > 0 ? num_pixels : 1, pcta);
-    pl.gy = ceil_div(tiles, pl.nsl);
+    pl.gy = ceil_div(pl.tiles, pl.nsl);
     if (g.kind == MBX_GEOM_CONE) {
-        // the row cache must hold the rows of a slice tile: BPF_ST * max |dm/dk| + 4
+        // the row cache must hold the rows of a slice tile: ts * max |dm/dk| + 4
         const double half_r = 0.5 * (g.num_recon_rows - 1), half_c = 0.5 * (g.num_recon_cols - 1);
         const double rho = g.delta_voxel * std::sqrt(half_r * half_r + half_c * half_c);
         const double inv = 1.0 / g.magnification - (std::isinf(g.source_detector_dist) ? 0.0 : rho / g.source_detector_dist);
         const double max_mag = inv > 1e-6 ? 1.0 / inv : 1e6;
         const double slope = max_mag * g.delta_voxel / g.delta_det_row;
-        if (BPF_ST * slope + 4 > BPF_CACHE_ROWS) pl.ok = false;
+        if (pl.ts * slope + 4 > BPF_CACHE_ROWS) pl.ok = false;
     }
     const long long base = (long long)pl.gx * pl.gy;
     const int sms = num_sms();
@@ -358,8 +366,8 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
     }
     pl.views_per_split = ceil_div(num_views_sel, splits);
     pl.splits = ceil_div(num_views_sel, pl.views_per_split);
-    const size_t nfp = (size_t)pl.vc * pcta;
-    pl.smem = nfp * 7 * 4 + (size_t)pl.vc * 12 + (g.kind == MBX_GEOM_CONE ? (size_t)BPF_CACHE_ROWS * BPF_THREADS * 4 : 0);
+    pl.smem = (size_t)pl.chunk * 16 * (g.kind == MBX_GEOM_CONE ? 2 : 1) + (size_t)pl.vc * 12 +
+              (g.kind == MBX_GEOM_CONE ? (size_t)BPF_CACHE_ROWS * BPF_THREADS * 4 : 0);
     pl.workspace = pl.splits > 1 ? align256((size_t)pl.splits * num_pixels * S * 4) : 0;
     return pl;
 }

@@ -32,6 +32,10 @@
 
 namespace mbx {
 
+#ifndef MBX_FPCB_SMEM_TIER0
+#define MBX_FPCB_SMEM_TIER0 (112 * 1024)  // shared memory a plan first tries to fit (2 CTAs per SM)
+#endif
+
 constexpr int CB_THREADS = 256;
 constexpr int CB_WARPS = CB_THREADS / 32;
 constexpr int CB_QUAD = 4;  // bins are padded to a multiple of this many records
@@ -100,7 +104,7 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
     // widest channel block, then largest pass, that fit the shared-memory tier (2, then 1 CTA per SM: the
     // registers of the accumulation loop allow no more than 2); a pass must hold at least 256 pixels after
     // the padding and the last scan chunk are set aside
-    static const size_t tiers[2] = {112 * 1024, 200 * 1024};
+    static const size_t tiers[2] = {MBX_FPCB_SMEM_TIER0, 200 * 1024};
     bool found = false;
     for (int t = 0; t < 2 && !found; ++t) {
         for (int nb = 128; nb >= 32 && !found; nb >>= 1) {
@@ -554,7 +558,10 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(CB_THREADS, 2) fp_cb_kernel(const FpArgs A, int *err) {
+#ifndef MBX_FPCB_MIN_BLOCKS
+#define MBX_FPCB_MIN_BLOCKS 2  // resident CTAs per SM the forward projection is compiled for
+#endif
+__global__ void __launch_bounds__(CB_THREADS, MBX_FPCB_MIN_BLOCKS) fp_cb_kernel(const FpArgs A, int *err) {
     extern __shared__ __align__(16) float smcb[];
     fp_cb_tile<KIND>(A, blockIdx.x, blockIdx.y, smcb, err);
 }

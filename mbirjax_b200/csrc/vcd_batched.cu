@@ -117,7 +117,10 @@ __device__ __forceinline__ int fetch_tile(int *counter) {
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(BPF_THREADS, 2) b_bp(BatchedTables T, int num_scans, int step, int total, int *err) {
+#ifndef MBX_BBP_MIN_BLOCKS
+#define MBX_BBP_MIN_BLOCKS 3  // resident CTAs per SM the batched back projection is compiled for
+#endif
+__global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(BatchedTables T, int num_scans, int step, int total, int *err) {
     extern __shared__ __align__(16) float smb[];
     for (int t = fetch_tile(T.counters); t < total; t = fetch_tile(T.counters)) {
         const int k = find_scan(T.bp_off, num_scans, t);
@@ -131,7 +134,10 @@ __global__ void __launch_bounds__(BPF_THREADS, 2) b_bp(BatchedTables T, int num_
 }
 
 template <int KIND>
-__global__ void __launch_bounds__(CB_THREADS, 2) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
+#ifndef MBX_BFP_MIN_BLOCKS
+#define MBX_BFP_MIN_BLOCKS 2  // resident CTAs per SM the batched forward projection is compiled for
+#endif
+__global__ void __launch_bounds__(CB_THREADS, MBX_BFP_MIN_BLOCKS) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
     extern __shared__ __align__(16) float smf2[];
     for (int t = fetch_tile(T.counters + 1); t < total; t = fetch_tile(T.counters + 1)) {
         const int k = find_scan(T.fp_off, num_scans, t);
@@ -490,9 +496,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
             a.out = v.bp;
             a.split_stride = 0;
             a.out_by_index = 0;
-            a.nsl = z.bpp.nsl;
-            a.npg = z.bpp.npg;
-            a.vc = z.bpp.vc;
+            a.plan = z.bpp;
             FpArgs &f = hf[ki];
             f.g = sc.geom;
             f.vox = v.delta;
@@ -520,7 +524,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
         std::vector<double> cost(num_scans);
         for (int s = 0; s < num_scans; ++s) {
             const mbx_geom &g = scans[s].geom;
-            cost[s] = (double)g.num_views * std::min(g.num_recon_slices, BPF_ST * zs[s].bpp.nsl) * 32.0 * zs[s].bpp.npg;
+            cost[s] = (double)g.num_views * std::min(g.num_recon_slices, zs[s].bpp.ts * zs[s].bpp.nsl) * 32.0 * zs[s].bpp.npg;
             ord[s] = s;
         }
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
