@@ -145,8 +145,8 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
     float4 *s_fb = s_fa + chunk;                     // cone: [chunk]
     float *s_cs = reinterpret_cast<float *>(s_fa + (KIND == MBX_GEOM_CONE ? 2 : 1) * chunk);
     float *s_sn = s_cs + vc;
-    int *s_vi = reinterpret_cast<int *>(s_sn + vc);
-    float *cache = reinterpret_cast<float *>(s_vi + vc);  // [BPF_CACHE_ROWS][BPF_THREADS] (cone)
+    int *s_voff = reinterpret_cast<int *>(s_sn + vc);      // element offset of each view (-1: invalid view)
+    float *cache = reinterpret_cast<float *>(s_voff + vc);  // [BPF_CACHE_ROWS][BPF_THREADS] (cone)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pg = warp / nsl, stl = warp - pg * nsl;
@@ -160,7 +160,8 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
     const int v_begin = split * views_per_split;
     const int v_end = min(num_views_sel, v_begin + views_per_split);
     const int npix_grid = g.num_recon_rows * g.num_recon_cols;
-    const long long view_stride = (long long)num_rows * num_channels;
+    const int view_stride = num_rows * num_channels;  // plan_bp_fast admits sinograms of < 2^31 elements
+    const int s0c = s0 * num_channels;
 
     // pixel geometry of the pixel this thread computes footprints for (pixel tid % pcta of every view)
     const int fpl = tid & (pcta - 1);
@@ -198,7 +199,7 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             const bool ok = vi >= 0 && vi < g.num_views;
             if (!ok && bx == 0 && by == 0) flag_error(err, MBX_ERRFLAG_VIEW);
             const float ang = ok ? g.angles[vi] : 0.0f;
-            s_vi[tid] = ok ? vi : -1;
+            s_voff[tid] = ok ? vi * view_stride : -1;
             s_cs[tid] = cosf(ang);
             s_sn[tid] = sinf(ang);
         }
@@ -207,7 +208,7 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             const int t = f >> lg_pcta;
             if (t < nv) {
                 float4 fa = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f), fb = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (fvalid && s_vi[t] >= 0) bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb);
+                if (fvalid && s_voff[t] >= 0) bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb);
                 s_fa[f] = fa;
                 if (KIND == MBX_GEOM_CONE) s_fb[f] = fb;
             }
@@ -219,32 +220,35 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             const float4 fa = s_fa[f];
             const int first = __float_as_int(fa.x);
             if (first < 0) continue;
-            const long long voff = (long long)s_vi[t] * view_stride;
+            const int voff = s_voff[t];
             if (KIND == MBX_GEOM_PARALLEL) {
-                // three taps at constant offsets from one pointer, one detector row per slice
-                const long long off = voff + (long long)s0 * num_channels + first;
-                const float *q = sino + off;
+                // three taps at constant offsets from one 32-bit element offset, one detector row per slice
+                int o = voff + s0c + first;
                 if (wts) {
-                    const float *qw = wts + off;
 #pragma unroll
                     for (int s = 0; s < BPF_ST; ++s) {
-                        if (s < ns)
+                        if (s < ns) {
+                            const float *q = sino + o, *qw = wts + o;
                             acc[s] = fmaf(fa.y, __ldg(q) * __ldg(qw),
                                           fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fmaf(fa.w, __ldg(q + 2) * __ldg(qw + 2), acc[s])));
-                        q += num_channels;
-                        qw += num_channels;
+                        }
+                        o += num_channels;
                     }
                 } else if (ns == BPF_ST) {  // full tile: no guards
 #pragma unroll
                     for (int s = 0; s < BPF_ST; ++s) {
+                        const float *q = sino + o;
                         acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
-                        q += num_channels;
+                        o += num_channels;
                     }
                 } else {
 #pragma unroll
                     for (int s = 0; s < BPF_ST; ++s) {
-                        if (s < ns) acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
-                        q += num_channels;
+                        if (s < ns) {
+                            const float *q = sino + o;
+                            acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
+                        }
+                        o += num_channels;
                     }
                 }
             } else {
@@ -263,10 +267,10 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 for (int m = m_lo; m <= m_hi; ++m) {
                     float c = 0.0f;
                     if (m >= 0 && m < num_rows) {
-                        const long long off = voff + (long long)m * num_channels + first;
-                        const float *q = sino + off;
+                        const int o = voff + m * num_channels + first;
+                        const float *q = sino + o;
                         if (wts) {
-                            const float *qw = wts + off;
+                            const float *qw = wts + o;
                             c = fmaf(fa.y, __ldg(q) * __ldg(qw), fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fa.w * (__ldg(q + 2) * __ldg(qw + 2))));
                         } else {
                             c = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fa.w * __ldg(q + 2)));
@@ -321,7 +325,9 @@ __global__ void __launch_bounds__(BPF_THREADS, 3) bp_fast_kernel(const BpArgs A,
 
 inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_views_sel) {
     BpfPlan pl;
-    pl.ok = (g.psf_radius == 1) && g.num_det_channels >= 3;
+    // 32-bit element offsets address the sinogram
+    pl.ok = (g.psf_radius == 1) && g.num_det_channels >= 3 &&
+            (long long)g.num_views * g.num_det_rows * g.num_det_channels < (1LL << 31);
     const int S = g.num_recon_slices;
     // tile height: the fewest tiles of <= BPF_ST slices, rounded up to a power of two (<= 8) or a multiple of 8,
     // then the slices spread evenly over them

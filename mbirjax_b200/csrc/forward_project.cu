@@ -207,7 +207,7 @@ static cudaError_t launch_fp_kind(const mbx_geom &g, const FpPlan &pl, const flo
 }
 
 size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel) {
-    if (plan_fp_cb(g).ok) return 0;
+    if (plan_fp_cb(g).ok && num_pixels * g.num_recon_slices < (1LL << 31)) return 0;
     return plan_fp(g, num_pixels, num_views_sel).workspace;
 }
 
@@ -230,7 +230,7 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
                     const int32_t *views, int num_views_sel, float *out, void *ws, size_t ws_bytes,
                     cudaStream_t st) {
     const CbPlan cpl = plan_fp_cb(g, num_views_sel, 4LL * num_sms());
-    if (cpl.ok) {
+    if (cpl.ok && num_pixels * g.num_recon_slices < (1LL << 31)) {  // 32-bit cylinder offsets
         FpArgs A;
         A.g = g;
         A.vox = vox;

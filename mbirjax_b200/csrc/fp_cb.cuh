@@ -8,20 +8,20 @@
 //  1. Scan: the 256 threads compute each pixel's centre channel n_c (trig-free for cone beam) and keep, by an
 //     ordered ballot compaction, the pixels with a tap inside the block; bin = n_c - n0 + 1 in [0, nb + 1].
 //  2. Sort: a stable counting sort by bin (shared-memory histogram, warp-aggregated ranks from
-//     __match_any_sync), during which the kept pixels' footprints are computed and stored as sorted records.
-//     Each bin is padded to a multiple of 4 records with zero-weight copies of its first record, so the
-//     accumulation loop below reads records four at a time with no bounds tests.
-//  3. Accumulate: the bins are split into 8 contiguous ranges of about equal record counts, one per warp
-//     (at least two bins each).  Lanes run along detector rows (contiguous voxel-cylinder reads); when a
-//     block has fewer rows than a warp has lanes, the warp splits into ppw sub-groups that take different
-//     records of each group of four, each with a private tile copy.  A bin's records all tap the same three
-//     channels, so a lane sums them in three registers and, at the end of the bin, channel bin-2 is complete:
-//     it is added to the shared tile once per pass, not once per tap.  The first two and the last two channels
-//     of a warp's range also receive taps from the neighbouring warp; those partial sums are added in two
-//     phases (even warps, barrier, odd warps), so no channel has two writers at once.
+//     __match_any_sync), during which the kept pixels' footprints are computed and stored as sorted records
+//     {cylinder offset, three channel coefficients} plus the bin.
+//  3. Accumulate: the bins are split into 8 contiguous ranges of about equal record counts, one per warp (at
+//     least two bins each).  A warp's lanes form ppw sub-groups of 32/ppw lanes; each sub-group walks an
+//     equal contiguous share of the warp's records, and each lane carries rpl detector rows (contiguous
+//     voxel-cylinder reads, rows rl apart).  The walk is flat and software-pipelined (8 loads in flight per
+//     lane); because the records are sorted by centre channel, a lane keeps three running channel sums per
+//     row in registers and, when the bin changes, channel bin-2 is done and is added once to the sub-group's
+//     private tile copy.  Channels at the ends of a warp's range also receive taps from the neighbouring
+//     warp; those partial sums are added in two phases (even warps, barrier, odd warps), so no tile element
+//     has two writers at once.
 //  4. Write: the copies of each tile element are summed in a fixed order and written, coalesced.
 // For cone beam each lane evaluates the detector-row-centric vertical fan of the reference
-// (cone_beam.py:347-372, including the 128-row batch anchor) for its row, reading the cylinder directly.
+// (cone_beam.py:347-372, including the 128-row batch anchor) for its rows, reading the cylinder directly.
 #pragma once
 
 #include <climits>
@@ -38,21 +38,22 @@ namespace mbx {
 
 constexpr int CB_THREADS = 256;
 constexpr int CB_WARPS = CB_THREADS / 32;
-constexpr int CB_QUAD = 4;  // bins are padded to a multiple of this many records
+constexpr int CB_LOADS = 8;  // loads in flight per lane in the accumulation walk
 
 struct CbPlan {
     int nb;          // channels per block
-    int rl;          // lanes per record = rows per chunk (8, 16 or 32)
-    int ppw;         // sub-groups per warp = 32 / rl
-    int row_chunks;  // ceil(R / rl)
-    int rpad;        // row_chunks * rl
+    int ppw;         // sub-groups per warp (1, 2 or 4)
+    int rl;          // lanes per sub-group = 32 / ppw
+    int rpl;         // detector rows per lane per row pass (1..4)
+    int row_passes;  // ceil(R / (rl * rpl))
+    int rpad;        // row_passes * rl * rpl
     int pitch;       // tile row pitch (nb + 1)
-    int cap;         // records per pass, padding included
+    int cap;         // records per pass
     int fill;        // the scan stops adding pixels once a pass holds more than this many
     int nbins;       // nb + 2
     int cblocks;     // channel blocks per view
     // shared-memory layout (4-byte words)
-    int o_rec, o_rec2, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_cone, o_misc;
+    int o_rec, o_rec2, o_sbin, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_cone, o_misc;
     size_t smem;
     bool ok;
 };
@@ -64,6 +65,8 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
     o += 4 * (size_t)pl.cap;
     pl.o_rec2 = (int)o;
     if (kind == MBX_GEOM_CONE) o += 4 * (size_t)pl.cap;
+    pl.o_sbin = (int)o;
+    o += pl.cap;
     pl.o_ulist = (int)o;
     o += pl.cap;
     pl.o_ubin = (int)o;
@@ -81,29 +84,34 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
     return o * 4;
 }
 
+#ifndef MBX_FPCB_SMEM_TIER0
+#define MBX_FPCB_SMEM_TIER0 (112 * 1024)  // shared memory a plan first tries to fit (2 CTAs per SM)
+#endif
+
 // num_views_sel: views per call (0 = all); min_blocks: CTAs wanted per call (a narrower channel block is
 // chosen to reach it); 0 = widest block.
 inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min_blocks = 0) {
     CbPlan pl = {};
     pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || g.bp_psf_radius == 1);
     const int R = g.num_det_rows, C = g.num_det_channels;
-    // lanes per record: padded rows, weighted by the cost of ppw sub-groups
+    // lane layout: padded rows weighted by the cost of ppw diverging sub-groups, plus a small cost per pass
+    static const int combos[10][2] = {{1, 1}, {1, 2}, {1, 3}, {1, 4}, {2, 1}, {2, 2}, {2, 3}, {2, 4}, {4, 1}, {4, 2}};
     double best = 1e300;
-    for (int rl = 32; rl >= 8; rl >>= 1) {
-        const int ppw = 32 / rl;
-        const double over = ppw == 1 ? 1.0 : (ppw == 2 ? 1.15 : 1.4);
-        const double cost = (double)ceil_div(R, rl) * rl * over;
+    for (const auto &cb : combos) {
+        const int ppw = cb[0], rpl = cb[1], rows = (32 / ppw) * rpl;
+        const int passes = ceil_div(R, rows);
+        const double f = ppw == 1 ? 1.0 : (ppw == 2 ? 1.15 : 1.35);
+        const double cost = (double)passes * rows * f + 2.0 * passes;
         if (cost < best - 1e-9) {
             best = cost;
-            pl.rl = rl;
+            pl.ppw = ppw;
+            pl.rpl = rpl;
         }
     }
-    pl.ppw = 32 / pl.rl;
-    pl.row_chunks = ceil_div(R, pl.rl);
-    pl.rpad = pl.row_chunks * pl.rl;
-    // widest channel block, then largest pass, that fit the shared-memory tier (2, then 1 CTA per SM: the
-    // registers of the accumulation loop allow no more than 2); a pass must hold at least 256 pixels after
-    // the padding and the last scan chunk are set aside
+    pl.rl = 32 / pl.ppw;
+    pl.row_passes = ceil_div(R, pl.rl * pl.rpl);
+    pl.rpad = pl.row_passes * pl.rl * pl.rpl;
+    // widest channel block, then largest pass, that fit the shared-memory tier (2, then 1 CTA per SM)
     static const size_t tiers[2] = {MBX_FPCB_SMEM_TIER0, 200 * 1024};
     bool found = false;
     for (int t = 0; t < 2 && !found; ++t) {
@@ -116,10 +124,10 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
                 q.pitch = nb + 1;
                 q.cap = cap;
                 q.nbins = nb + 2;
-                q.fill = cap - CB_THREADS - (CB_QUAD - 1) * q.nbins;
+                q.fill = cap - CB_THREADS;
                 q.cblocks = ceil_div(C, nb);
                 q.smem = cb_layout(q, g.kind, R);
-                if (q.fill >= 256 && q.smem <= tiers[t]) {
+                if (q.smem <= tiers[t]) {
                     pl = q;
                     found = true;
                 }
@@ -216,11 +224,12 @@ struct CbRow {
     int b0;
 };
 
-// Value of one record for detector row m: the voxel itself (parallel) or the cone vertical fan.
+// Value of one record for detector row m: the voxel itself (parallel: cyl already points at slice m) or the
+// cone vertical fan (cyl points at the start of the cylinder).
 template <int KIND>
 __device__ __forceinline__ float cb_value(const float *cyl, int m, int num_slices, const float4 &cv,
                                           const CbRow &rw, float kconst) {
-    if (KIND == MBX_GEOM_PARALLEL) return __ldg(cyl + m);
+    if (KIND == MBX_GEOM_PARALLEL) return __ldg(cyl);
     const float w_r = cv.y;
     const float k_m = fmaf(rw.vm, cv.x, kconst);
     const float k_m0 = fmaf(rw.vb, cv.x, kconst);
@@ -244,88 +253,121 @@ __device__ __forceinline__ float cb_value(const float *cyl, int m, int num_slice
 // What one warp needs to accumulate one pass.
 struct CbPass {
     const float4 *rec, *rec2;  // sorted records (rec2: cone only)
-    const int *bstart;         // padded bin starts
+    const int *sbin;           // bin of each sorted record
+    const int *bstart;         // bin starts
     float *tile;
     const float *s_vm, *s_vb;  // cone row tables
     const int *s_b0;
     int b_lo, b_hi;            // this warp's bins
 };
 
-// Accumulation of one pass by one warp (PPW sub-groups of 32/PPW rows each), then the edge writes.
-template <int KIND, int PPW>
+// Accumulation of one pass by one warp: PPW sub-groups, RPL rows per lane; then the edge writes.
+template <int KIND, int PPW, int RPL>
 __device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, int warp, int lane, float kconst) {
     const mbx_geom &g = A.g;
     const CbPlan &pl = A.plan;
     constexpr int RL = 32 / PPW;
-    constexpr int U = CB_QUAD / PPW;  // records of a quad per lane
-    constexpr int QU = PPW;           // quads per iteration: U * QU = 4 loads in flight per lane
+    constexpr int U = (CB_LOADS / RPL) > 0 ? (CB_LOADS / RPL) : 1;  // records prefetched per lane
     const int sub = lane / RL, lr = lane % RL;
     const int num_rows = g.num_det_rows, num_slices = g.num_recon_slices, nb = pl.nb;
-    for (int rc = 0; rc < pl.row_chunks; ++rc) {
-        const int m = rc * RL + lr;
-        const int mc = min(m, num_rows - 1);  // rows past R read a valid row; their tile rows are never written out
-        CbRow rw = {0.f, 0.f, 0};
-        if (KIND == MBX_GEOM_CONE) {
-            rw.vm = P.s_vm[mc];
-            rw.vb = P.s_vb[mc];
-            rw.b0 = P.s_b0[mc];
+    // this sub-group's share of the warp's records
+    const int w_lo = P.bstart[P.b_lo], w_hi = P.bstart[P.b_hi];
+    const int r_a = w_lo + (int)(((long long)(w_hi - w_lo) * sub) / PPW);
+    const int r_b = w_lo + (int)(((long long)(w_hi - w_lo) * (sub + 1)) / PPW);
+    // edge channels of the warp's range: E0, E1 (shared with the warp below), E2, E3 (with the warp above)
+    const int E0 = P.b_lo - 2, E1 = P.b_lo - 1, E2 = P.b_hi - 2, E3 = P.b_hi - 1;
+    for (int rp = 0; rp < pl.row_passes; ++rp) {
+        int m[RPL], mcl[RPL];
+        const float *vb[RPL];
+        float *trow[RPL];
+        CbRow rw[RPL];
+#pragma unroll
+        for (int j = 0; j < RPL; ++j) {
+            m[j] = (rp * RPL + j) * RL + lr;
+            const int mc = min(m[j], num_rows - 1);  // rows past R read a valid row; never written out
+            mcl[j] = mc;
+            vb[j] = A.vox + (KIND == MBX_GEOM_PARALLEL ? mc : 0);
+            trow[j] = P.tile + ((size_t)sub * pl.rpad + m[j]) * pl.pitch;
+            rw[j].vm = rw[j].vb = 0.f;
+            rw[j].b0 = 0;
+            if (KIND == MBX_GEOM_CONE) {
+                rw[j].vm = P.s_vm[mc];
+                rw[j].vb = P.s_vb[mc];
+                rw[j].b0 = P.s_b0[mc];
+            }
         }
-        float *trow = P.tile + ((size_t)sub * pl.rpad + m) * pl.pitch;
-        // before bin b: x = sum for channel b-2, y = sum for channel b-1; bin b adds s0/s1/s2 to b-2/b-1/b
-        float x = 0.f, y = 0.f, e0 = 0.f, e1 = 0.f;
-        for (int b = P.b_lo; b < P.b_hi; ++b) {
-            const int q0 = P.bstart[b], q1 = P.bstart[b + 1];
-            float s0 = 0.f, s1 = 0.f, s2 = 0.f;
-            for (int i = q0; i < q1; i += CB_QUAD * QU) {
-                float4 rq[U * QU];
-                float vq[U * QU];
+        // before bin bc: x = sum for channel bc-2, y = sum for channel bc-1; bin bc adds s0/s1/s2 to them and bc
+        float x[RPL], y[RPL], s0[RPL], s1[RPL], s2[RPL], e0[RPL], e1[RPL], e2[RPL], e3[RPL];
 #pragma unroll
-                for (int qq = 0; qq < QU; ++qq) {
+        for (int j = 0; j < RPL; ++j) x[j] = y[j] = s0[j] = s1[j] = s2[j] = e0[j] = e1[j] = e2[j] = e3[j] = 0.0f;
+        int bc = (r_a < r_b) ? P.sbin[r_a] : 0;
+        // bin bc is complete: channel bc-2 receives its sum
+        auto finish = [&]() {
+            const int c = bc - 2;
+            const bool interior = c >= P.b_lo && c <= P.b_hi - 3;
 #pragma unroll
-                    for (int u = 0; u < U; ++u) {
-                        const int k = qq * U + u;
-                        const int ii = i + qq * CB_QUAD + sub * U + u;
-                        if (QU == 1 || i + qq * CB_QUAD < q1) {
-                            rq[k] = P.rec[ii];
-                            const float *cyl = A.vox + (long long)__float_as_int(rq[k].x) * num_slices;
-                            float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
-                            if (KIND == MBX_GEOM_CONE) cv = P.rec2[ii];
-                            vq[k] = cb_value<KIND>(cyl, mc, num_slices, cv, rw, kconst);
-                        } else {
-                            rq[k] = make_float4(0.f, 0.f, 0.f, 0.f);
-                            vq[k] = 0.0f;
-                        }
-                    }
-                }
-#pragma unroll
-                for (int k = 0; k < U * QU; ++k) {
-                    s0 = fmaf(rq[k].y, vq[k], s0);
-                    s1 = fmaf(rq[k].z, vq[k], s1);
-                    s2 = fmaf(rq[k].w, vq[k], s2);
+            for (int j = 0; j < RPL; ++j) {
+                const float v = x[j] + s0[j];
+                x[j] = y[j] + s1[j];
+                y[j] = s2[j];
+                s0[j] = s1[j] = s2[j] = 0.0f;
+                if (interior) {
+                    trow[j][c] += v;
+                } else {
+                    e0[j] += (c == E0) ? v : 0.0f;
+                    e1[j] += (c == E1) ? v : 0.0f;
+                    e2[j] += (c == E2) ? v : 0.0f;
+                    e3[j] += (c == E3) ? v : 0.0f;
                 }
             }
-            // bin b is done: channel b-2 has all its taps from this warp's bins
-            const float done = x + s0;
-            x = y + s1;
-            y = s2;
-            const int f = b - P.b_lo;
-            if (f == 0)
-                e0 = done;
-            else if (f == 1)
-                e1 = done;
-            else
-                trow[b - 2] += done;  // interior channel: b_lo <= b-2 <= b_hi-3 < nb, one writer
+            ++bc;
+        };
+        for (int i = r_a; i < r_b; i += U) {
+            float4 rq[U];
+            int bq[U];
+            float vq[U][RPL];
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                const int ii = min(i + u, r_b - 1);  // past the end: reread the last record, contribute nothing
+                rq[u] = P.rec[ii];
+                bq[u] = P.sbin[ii];
+                float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
+                if (KIND == MBX_GEOM_CONE) cv = P.rec2[ii];
+                const int off = __float_as_int(rq[u].x);  // 32-bit element offset of the cylinder
+#pragma unroll
+                for (int j = 0; j < RPL; ++j)
+                    vq[u][j] = cb_value<KIND>(vb[j] + off, mcl[j], num_slices, cv, rw[j], kconst);
+            }
+#pragma unroll
+            for (int u = 0; u < U; ++u) {
+                if (i + u < r_b) {
+                    while (bc < bq[u]) finish();
+#pragma unroll
+                    for (int j = 0; j < RPL; ++j) {
+                        s0[j] = fmaf(rq[u].y, vq[u][j], s0[j]);
+                        s1[j] = fmaf(rq[u].z, vq[u][j], s1[j]);
+                        s2[j] = fmaf(rq[u].w, vq[u][j], s2[j]);
+                    }
+                }
+            }
         }
-        // edge channels b_lo-2, b_lo-1 (partial: the warp below adds its part) and b_hi-2, b_hi-1 (partial: the
-        // warp above adds its part): even warps first, then odd warps, so no channel has two writers at once
+        if (r_a < r_b) {  // the last bin and the two channels above it
+            finish();
+            finish();
+            finish();
+        }
+        // edge channels: even warps first, then odd warps
 #pragma unroll
         for (int ph = 0; ph < 2; ++ph) {
             if (ph == 1) __syncthreads();
             if ((warp & 1) == ph) {
-                if (P.b_lo >= 2) trow[P.b_lo - 2] += e0;
-                if (P.b_lo >= 1) trow[P.b_lo - 1] += e1;
-                if (P.b_hi - 2 < nb) trow[P.b_hi - 2] += x;
-                if (P.b_hi - 1 < nb) trow[P.b_hi - 1] += y;
+#pragma unroll
+                for (int j = 0; j < RPL; ++j) {
+                    if (E0 >= 0) trow[j][E0] += e0[j];
+                    if (E1 >= 0) trow[j][E1] += e1[j];
+                    if (E2 < nb) trow[j][E2] += e2[j];
+                    if (E3 < nb) trow[j][E3] += e3[j];
+                }
             }
         }
     }
@@ -340,8 +382,9 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     const int nb = pl.nb, nbins = pl.nbins, n0 = cb * nb;
 
     float *tile = sm;  // [ppw][rpad][pitch]
-    float4 *rec = reinterpret_cast<float4 *>(sm + pl.o_rec);    // sorted {vox row (int bits), a0, a1, a2}
+    float4 *rec = reinterpret_cast<float4 *>(sm + pl.o_rec);    // sorted {cylinder offset (int bits), a0, a1, a2}
     float4 *rec2 = reinterpret_cast<float4 *>(sm + pl.o_rec2);  // cone: sorted {imd, W_r, mdz, mz0}
+    int *sbin = reinterpret_cast<int *>(sm + pl.o_sbin);        // bin of each sorted record
     int *ulist = reinterpret_cast<int *>(sm + pl.o_ulist);      // kept pixel positions, scan order
     int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // their bins
     int *bstart = reinterpret_cast<int *>(sm + pl.o_bstart);    // [nbins + 1] padded start of each bin
@@ -426,14 +469,13 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
         }
         __syncthreads();
         if (count == 0) continue;
-        // ---- 2a. padded bin starts: exclusive scan of the rounded-up histogram (warp 0); run[] becomes the
-        //          placement cursor
+        // ---- 2a. bin starts: exclusive scan of the histogram (warp 0); run[] becomes the placement cursor
         if (warp == 0) {
             const int per = (nbins + 31) / 32;
             int loc = 0;
             for (int k = 0; k < per; ++k) {
                 const int b = lane * per + k;
-                if (b < nbins) loc += (run[b] + CB_QUAD - 1) & ~(CB_QUAD - 1);
+                if (b < nbins) loc += run[b];
             }
             int incl = loc;
 #pragma unroll
@@ -448,7 +490,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
                     const int h = run[b];
                     bstart[b] = acc;
                     run[b] = acc;
-                    acc += (h + CB_QUAD - 1) & ~(CB_QUAD - 1);
+                    acc += h;
                 }
             }
             if (lane == 31) bstart[nbins] = incl;
@@ -472,8 +514,10 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
                 pixel_tilde_fast(g, idx, inv_cols, xt, yt);
                 float a0, a1, a2, imd, wr, mdz, mz0;
                 cb_footprint<KIND>(g, cs, sn, xt, yt, n0 + b - 1, a0, a1, a2, imd, wr, mdz, mz0);
-                rec[pos] = make_float4(__int_as_float(A.vox_by_index ? idx : p), a0, a1, a2);
+                // element offset of the pixel's cylinder (the host admits vox buffers of < 2^31 elements)
+                rec[pos] = make_float4(__int_as_float((A.vox_by_index ? idx : p) * num_slices), a0, a1, a2);
                 if (KIND == MBX_GEOM_CONE) rec2[pos] = make_float4(imd, wr, mdz, mz0);
+                sbin[pos] = b;
             }
             __syncthreads();
             for (int bb = tid; bb < nbins; bb += CB_THREADS) {
@@ -486,19 +530,6 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             }
             __syncthreads();
         }
-        // ---- 2c. padding: zero-weight copies of each bin's first record up to the next multiple of 4
-        for (int b = tid; b < nbins; b += CB_THREADS) {
-            const int d0 = run[b], d1 = bstart[b + 1];
-            if (d0 < d1) {
-                const float4 r0 = rec[bstart[b]];
-                for (int d = d0; d < d1; ++d) rec[d] = make_float4(r0.x, 0.f, 0.f, 0.f);
-                if (KIND == MBX_GEOM_CONE) {
-                    const float4 c0 = rec2[bstart[b]];
-                    for (int d = d0; d < d1; ++d) rec2[d] = c0;
-                }
-            }
-        }
-        __syncthreads();
         // ---- 3. warp ranges of bins with about equal record counts, at least two bins each:
         //         B_v = 2v + max_{u<=v}(lb_u - 2u), then B_v <= nbins - 2(8 - v); lb_v = first bin starting at or
         //         after v/8 of the records
@@ -531,17 +562,24 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
         }
         P.rec = rec;
         P.rec2 = rec2;
+        P.sbin = sbin;
         P.bstart = bstart;
         P.tile = tile;
         P.s_vm = s_vm;
         P.s_vb = s_vb;
         P.s_b0 = s_b0;
-        if (pl.ppw == 1)
-            cb_accumulate<KIND, 1>(A, P, warp, lane, kconst);
-        else if (pl.ppw == 2)
-            cb_accumulate<KIND, 2>(A, P, warp, lane, kconst);
-        else
-            cb_accumulate<KIND, 4>(A, P, warp, lane, kconst);
+        switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
+            case 9: cb_accumulate<KIND, 1, 1>(A, P, warp, lane, kconst); break;
+            case 10: cb_accumulate<KIND, 1, 2>(A, P, warp, lane, kconst); break;
+            case 11: cb_accumulate<KIND, 1, 3>(A, P, warp, lane, kconst); break;
+            case 12: cb_accumulate<KIND, 1, 4>(A, P, warp, lane, kconst); break;
+            case 17: cb_accumulate<KIND, 2, 1>(A, P, warp, lane, kconst); break;
+            case 18: cb_accumulate<KIND, 2, 2>(A, P, warp, lane, kconst); break;
+            case 19: cb_accumulate<KIND, 2, 3>(A, P, warp, lane, kconst); break;
+            case 20: cb_accumulate<KIND, 2, 4>(A, P, warp, lane, kconst); break;
+            case 33: cb_accumulate<KIND, 4, 1>(A, P, warp, lane, kconst); break;
+            default: cb_accumulate<KIND, 4, 2>(A, P, warp, lane, kconst); break;
+        }
     }
     __syncthreads();
     // ---- 4. fixed-order sum of the sub-group copies, coalesced write
