@@ -14,25 +14,7 @@ import numpy as np
 import torch
 
 from . import _capi
-from .vcd_utils import gen_set_of_pixel_partitions, gen_partition_sequence
-
-
-def morton_order(pixel_indices, num_cols):
-    """Positions of pixel_indices sorted by the Z-order (Morton) code of (row, col): neighbouring positions are
-    spatially close, so the channel gathers of a warp of the back projector stay within a few sectors."""
-    idx = np.asarray(pixel_indices, dtype=np.int64)
-    row, col = idx // num_cols, idx % num_cols
-
-    def spread(v):
-        v = v.astype(np.uint64) & np.uint64(0xFFFF)
-        v = (v | (v << np.uint64(8))) & np.uint64(0x00FF00FF)
-        v = (v | (v << np.uint64(4))) & np.uint64(0x0F0F0F0F)
-        v = (v | (v << np.uint64(2))) & np.uint64(0x33333333)
-        v = (v | (v << np.uint64(1))) & np.uint64(0x55555555)
-        return v
-
-    code = spread(row) | (spread(col) << np.uint64(1))
-    return np.argsort(code, kind='stable').astype(np.int32)
+from .vcd_utils import gen_set_of_pixel_partitions, gen_partition_sequence, morton_order, morton_sorted_partition
 
 
 class BatchedVCD:
@@ -74,9 +56,8 @@ class BatchedVCD:
             state = model._vcd_setup(self.sinograms[i], self.weights[i], self.init_recons[i])
             schedules.append(np.stack([np.random.permutation(num_subsets) for _ in range(max_iterations)]))
             dev = state['device']
+            part = morton_sorted_partition(part, recon_shape[1])  # spatially coherent processing order
             part_d = torch.as_tensor(part, device=dev, dtype=torch.int32).contiguous()
-            order = np.stack([morton_order(p, recon_shape[1]) for p in part])
-            order_d = torch.as_tensor(order, device=dev, dtype=torch.int32).contiguous()
             rec = _capi.MbxScan()
             rec.geom = model._geometry()
             rec.flat_recon = state['flat_recon'].data_ptr()
@@ -84,12 +65,12 @@ class BatchedVCD:
             rec.weights = state['weights'].data_ptr() if state['weights'] is not None else None
             rec.fm_hessian = state['fm_hessian'].data_ptr()
             rec.partition = part_d.data_ptr()
-            rec.partition_order = order_d.data_ptr()
+            rec.partition_order = None
             rec.num_subsets = int(part.shape[0])
             rec.subset_size = int(part.shape[1])
             rec.fm_constant = float(state['fm_constant'])
             rec.qp = state['qp']
-            state['partition_d'], state['order_d'] = part_d, order_d
+            state['partition_d'] = part_d
             scans.append(rec)
             self.states.append(state)
             self.partitions.append(part)

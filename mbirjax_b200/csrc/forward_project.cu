@@ -207,7 +207,7 @@ static cudaError_t launch_fp_kind(const mbx_geom &g, const FpPlan &pl, const flo
 }
 
 size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel) {
-    if (plan_fp_cb(g).ok && num_pixels * g.num_recon_slices < (1LL << 31)) return 0;
+    if (plan_fp_cb(g).ok && num_pixels * g.num_recon_slices < (1LL << 31)) return fp_chunk_box_bytes(num_pixels);
     return plan_fp(g, num_pixels, num_views_sel).workspace;
 }
 
@@ -241,6 +241,17 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
         A.out = out;
         A.vox_by_index = 0;
         A.plan = cpl;
+        // bounding boxes of the list's chunks, so that each channel block skips the chunks that miss it
+        const size_t need = fp_chunk_box_bytes(num_pixels);
+        if (need > 0 && (ws == nullptr || ws_bytes < need)) return MBX_ERR_WORKSPACE;
+        A.chunk_box = num_pixels > 0 ? static_cast<const int4 *>(ws) : nullptr;
+        if (num_pixels > 0) {
+            fp_chunk_bounds_kernel<<<(unsigned)((num_pixels + CB_CHUNK - 1) / CB_CHUNK), CB_CHUNK, 0, st>>>(
+                pix, num_pixels, g.num_recon_rows, g.num_recon_cols, static_cast<int4 *>(ws));
+            note_launch();
+            cudaError_t e0 = cudaGetLastError();
+            if (e0 != cudaSuccess) return set_cuda_error(e0);
+        }
         cudaError_t e = (g.kind == MBX_GEOM_PARALLEL) ? launch_fp_cb<MBX_GEOM_PARALLEL>(A, st)
                                                        : launch_fp_cb<MBX_GEOM_CONE>(A, st);
         return e == cudaSuccess ? MBX_OK : set_cuda_error(e);

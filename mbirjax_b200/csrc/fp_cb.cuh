@@ -53,7 +53,7 @@ struct CbPlan {
     int nbins;       // nb + 2
     int cblocks;     // channel blocks per view
     // shared-memory layout (4-byte words)
-    int o_rec, o_rec2, o_sbin, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_cone, o_misc;
+    int o_rec, o_rec2, o_sbin, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_wstart, o_cone, o_hl, o_misc;
     size_t smem;
     bool ok;
 };
@@ -77,16 +77,16 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
     o += pl.nbins;
     pl.o_wcnt = (int)o;
     o += (size_t)CB_WARPS * pl.nbins;
+    pl.o_wstart = (int)o;
+    o += (size_t)CB_WARPS * pl.nbins;
     pl.o_cone = (int)o;
     if (kind == MBX_GEOM_CONE) o += 3 * (size_t)R;
+    pl.o_hl = (int)o;
+    o += CB_THREADS;
     pl.o_misc = (int)o;
-    o += 2 * CB_WARPS;
+    o += 3 * CB_WARPS;
     return o * 4;
 }
-
-#ifndef MBX_FPCB_SMEM_TIER0
-#define MBX_FPCB_SMEM_TIER0 (112 * 1024)  // shared memory a plan first tries to fit (2 CTAs per SM)
-#endif
 
 // num_views_sel: views per call (0 = all); min_blocks: CTAs wanted per call (a narrower channel block is
 // chosen to reach it); 0 = widest block.
@@ -135,6 +135,7 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
         }
     }
     if (!found) pl.ok = false;
+    if ((long long)g.num_recon_rows * g.num_recon_cols > (1LL << 24)) pl.ok = false;  // bin and index share a word
     if (g.kind == MBX_GEOM_CONE) {
         const double half_r = 0.5 * (g.num_recon_rows - 1), half_c = 0.5 * (g.num_recon_cols - 1);
         const double rho = g.delta_voxel * std::sqrt(half_r * half_r + half_c * half_c);
@@ -215,10 +216,87 @@ struct FpArgs {
     int num_views_sel;
     float *out;                // (num_views_sel, R, C)
     int vox_by_index;          // 0: vox is (num_pixels, S) in list order; 1: vox is a flat recon indexed by pixel
+    const int4 *chunk_box;     // optional: per 256 list entries {row min, row max, col min, col max}, or
+                               // row min -1 when the chunk holds an index off the grid (never skipped)
     CbPlan plan;
 };
 
-// Detector-row constants of the cone vertical fan (one per lane).
+constexpr int CB_CHUNK = 256;  // list entries per chunk of chunk_box (= the scan step)
+static_assert(CB_CHUNK == CB_THREADS, "the scan walks the list one chunk per step");
+
+inline size_t fp_chunk_box_bytes(long long num_pixels) {
+    return align256((size_t)((num_pixels + CB_CHUNK - 1) / CB_CHUNK) * sizeof(int4));
+}
+
+// Bounding box of the grid pixels of each CB_CHUNK list entries (one CTA of CB_CHUNK threads per chunk).
+static __global__ void __launch_bounds__(CB_CHUNK) fp_chunk_bounds_kernel(const int32_t *__restrict__ pix,
+                                                                    long long num_pixels, int num_rows, int num_cols,
+                                                                    int4 *__restrict__ box) {
+    __shared__ int red[4][CB_CHUNK / 32];
+    const long long p = (long long)blockIdx.x * CB_CHUNK + threadIdx.x;
+    int rmin = INT_MAX, rmax = INT_MIN, cmin = INT_MAX, cmax = INT_MIN, bad = 0;
+    if (p < num_pixels) {
+        const int idx = pix[p];
+        if (idx < 0 || idx >= num_rows * num_cols) {
+            bad = 1;
+        } else {
+            const int r = idx / num_cols, c = idx - (idx / num_cols) * num_cols;
+            rmin = rmax = r;
+            cmin = cmax = c;
+        }
+    }
+    rmin = min(rmin, bad ? -1 : rmin);
+#pragma unroll
+    for (int off = 16; off > 0; off >>= 1) {
+        rmin = min(rmin, __shfl_xor_sync(0xffffffffu, rmin, off));
+        rmax = max(rmax, __shfl_xor_sync(0xffffffffu, rmax, off));
+        cmin = min(cmin, __shfl_xor_sync(0xffffffffu, cmin, off));
+        cmax = max(cmax, __shfl_xor_sync(0xffffffffu, cmax, off));
+    }
+    const int warp = threadIdx.x >> 5, lane = threadIdx.x & 31;
+    if (lane == 0) {
+        red[0][warp] = rmin;
+        red[1][warp] = rmax;
+        red[2][warp] = cmin;
+        red[3][warp] = cmax;
+    }
+    __syncthreads();
+    if (threadIdx.x == 0) {
+        for (int w = 1; w < CB_CHUNK / 32; ++w) {
+            rmin = min(rmin, red[0][w]);
+            rmax = max(rmax, red[1][w]);
+            cmin = min(cmin, red[2][w]);
+            cmax = max(cmax, red[3][w]);
+        }
+        if (rmin < 0) rmin = -1;  // an off-grid index: the projector must see every entry to flag it
+        box[blockIdx.x] = make_int4(rmin, rmax, cmin, cmax);
+    }
+}
+
+// True when no pixel of the box can have a centre channel in [n0 - 1, n0 + nb] (one rounding step of slack
+// on each side).  The channel is a linear (parallel) or linear-fractional (cone, denominator of one sign) function
+// of the pixel position, so its extremes over the box are at the corners.
+template <int KIND>
+__device__ __forceinline__ bool cb_box_misses(const mbx_geom &g, int4 bx, float cs, float sn, float inv_d, int n0,
+                                              int nb) {
+    if (bx.x < 0) return false;
+    float lo = 3.0e38f, hi = -3.0e38f;
+#pragma unroll
+    for (int corner = 0; corner < 4; ++corner) {
+        const int r = (corner & 1) ? bx.y : bx.x;
+        const int c = (corner & 2) ? bx.w : bx.z;
+        const float yt = g.delta_voxel * ((float)r - 0.5f * (float)(g.num_recon_rows - 1));
+        const float xt = g.delta_voxel * ((float)c - 0.5f * (float)(g.num_recon_cols - 1));
+        float mag;
+        const float np = cb_channel<KIND>(g, cs, sn, xt, yt, inv_d, mag);
+        lo = fminf(lo, np);
+        hi = fmaxf(hi, np);
+    }
+    const float nlo = rintf(lo) - 1.0f, nhi = rintf(hi) + 1.0f;  // centre channels of the box lie in [nlo, nhi]
+    return nhi < (float)(n0 - 1) || nlo > (float)(n0 + nb);
+}
+
+// Detector-row constants of the cone vertical fan (one per lane and row).
 struct CbRow {
     float vm, vb;
     int b0;
@@ -386,14 +464,17 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     float4 *rec2 = reinterpret_cast<float4 *>(sm + pl.o_rec2);  // cone: sorted {imd, W_r, mdz, mz0}
     int *sbin = reinterpret_cast<int *>(sm + pl.o_sbin);        // bin of each sorted record
     int *ulist = reinterpret_cast<int *>(sm + pl.o_ulist);      // kept pixel positions, scan order
-    int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // their bins
+    int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // their bin << 24 | pixel index
     int *bstart = reinterpret_cast<int *>(sm + pl.o_bstart);    // [nbins + 1] padded start of each bin
     int *run = reinterpret_cast<int *>(sm + pl.o_run);          // [nbins] histogram, then placement cursor
     int *wcnt = reinterpret_cast<int *>(sm + pl.o_wcnt);        // [warps][nbins] per-warp counts of a chunk
+    int *wstart = reinterpret_cast<int *>(sm + pl.o_wstart);    // [warps][nbins] per-warp start positions
     float *s_vm = sm + pl.o_cone;                               // cone: [R] detector height of each row centre
     float *s_vb = s_vm + num_rows;                              // cone: [R] same at the row's 128-row batch start
     int *s_b0 = reinterpret_cast<int *>(s_vb + num_rows);       // cone: [R] batch start row
-    int *s_misc = reinterpret_cast<int *>(sm + pl.o_misc);      // [2][warps]: warp counts, double-buffered
+    int *hl = reinterpret_cast<int *>(sm + pl.o_hl);            // chunks of the current segment that can hit
+    int *s_misc = reinterpret_cast<int *>(sm + pl.o_misc);      // [2][warps]: warp counts, double-buffered;
+                                                                // [2][warps]: hit counts of a segment
 
     const int vi = A.views ? A.views[j] : j;
     const bool view_ok = vi >= 0 && vi < g.num_views;
@@ -421,21 +502,63 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     }
 
     const int npix_grid = g.num_recon_rows * g.num_recon_cols;
-    long long scan = 0;
     const long long num_pixels = view_ok ? A.num_pixels : 0;
+    const long long nchunks = (num_pixels + CB_CHUNK - 1) / CB_CHUNK;
+    long long seg = 0;    // first chunk of the next segment of CB_THREADS chunks to test
+    int nh = 0, hp = 0;   // chunks of the current segment that can reach the block (in hl), next one to scan
+    int idx_next = -1;    // prefetched pixel index of entry tid of chunk hl[hp]
+    bool more = num_pixels > 0;
 
-    while (scan < num_pixels) {
+    while (more) {
         __syncthreads();  // the previous pass is done with every list
         for (int b = tid; b < nbins; b += CB_THREADS) run[b] = 0;
         __syncthreads();
         // ---- 1. ordered compaction of the pixels that touch this channel block
         int count = 0, par = 0;
-        while (scan < num_pixels && count <= pl.fill) {
-            const long long p = scan + tid;
+        while (count <= pl.fill) {
+            if (hp == nh) {
+                if (seg >= nchunks) {
+                    more = false;
+                    break;
+                }
+                // next segment: ordered list of its chunks whose bounding box can reach the block
+                __syncthreads();  // everyone is done with hl
+                const long long c = seg + tid;
+                bool hit = false;
+                if (c < nchunks)
+                    hit = !A.chunk_box || !cb_box_misses<KIND>(g, __ldg(A.chunk_box + c), cs, sn, inv_d, n0, nb);
+                const unsigned hb = __ballot_sync(0xffffffffu, hit);
+                int *hw = s_misc + 2 * CB_WARPS;
+                if (lane == 0) hw[warp] = __popc(hb);
+                __syncthreads();
+                int hbase = 0, htot = 0;
+#pragma unroll
+                for (int w = 0; w < CB_WARPS; ++w) {
+                    const int k = hw[w];
+                    hbase += (w < warp) ? k : 0;
+                    htot += k;
+                }
+                if (hit) hl[hbase + __popc(hb & ((1u << lane) - 1u))] = (int)c;
+                __syncthreads();
+                nh = htot;
+                hp = 0;
+                seg += CB_THREADS;
+                if (nh > 0) {
+                    const long long p0 = (long long)hl[0] * CB_CHUNK + tid;
+                    idx_next = p0 < num_pixels ? A.pix[p0] : -1;
+                }
+                continue;
+            }
+            const long long p = (long long)hl[hp] * CB_CHUNK + tid;
+            const int idx = idx_next;
+            ++hp;
+            if (hp < nh) {  // prefetch the next chunk's entry while this one is compacted
+                const long long pn = (long long)hl[hp] * CB_CHUNK + tid;
+                idx_next = pn < num_pixels ? A.pix[pn] : -1;
+            }
             bool take = false;
             int bin = 0;
             if (p < num_pixels) {
-                const int idx = A.pix[p];
                 if (idx < 0 || idx >= npix_grid) {
                     if (cb == 0 && j == 0) flag_error(err, MBX_ERRFLAG_PIXEL);
                 } else {
@@ -460,11 +583,10 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             if (take) {
                 const int pos = base + __popc(ballot & ((1u << lane) - 1u));
                 ulist[pos] = (int)p;
-                ubin[pos] = bin;
+                ubin[pos] = (int)(((unsigned)bin << 24) | (unsigned)idx);
                 atomicAdd(run + bin, 1);  // integer histogram: order-independent
             }
             count += total;
-            scan += CB_THREADS;
             par ^= 1;
         }
         __syncthreads();
@@ -496,20 +618,33 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             if (lane == 31) bstart[nbins] = incl;
         }
         __syncthreads();
-        // ---- 2b. stable placement by bin, computing the footprints on the way
+        // ---- 2b. stable placement by bin, computing the footprints on the way.  Per chunk of 256 kept pixels:
+        //          per-warp bin counts (ranks from __match_any_sync), then each bin's per-warp start positions
+        //          (cursor + counts of the warps before), then the records.
         for (int base = 0; base < count; base += CB_THREADS) {
             const int i = base + tid;
             const bool valid = i < count;
-            const int b = valid ? ubin[i] : -1;
+            const unsigned ub = valid ? (unsigned)ubin[i] : 0u;
+            const int b = valid ? (int)(ub >> 24) : -1;  // bins reach nb + 1 = 129: unsigned unpacking
             const unsigned peers = __match_any_sync(0xffffffffu, b);
             const int rank = __popc(peers & ((1u << lane) - 1u));
             if (valid && rank == 0) wcnt[warp * nbins + b] = __popc(peers);
             __syncthreads();
+            for (int bb = tid; bb < nbins; bb += CB_THREADS) {
+                int acc = run[bb];
+                for (int w = 0; w < CB_WARPS; ++w) {
+                    const int c = wcnt[w * nbins + bb];
+                    wstart[w * nbins + bb] = acc;
+                    wcnt[w * nbins + bb] = 0;
+                    acc += c;
+                }
+                run[bb] = acc;
+            }
+            __syncthreads();
             if (valid) {
-                int pos = run[b] + rank;
-                for (int w = 0; w < warp; ++w) pos += wcnt[w * nbins + b];
+                const int pos = wstart[warp * nbins + b] + rank;
                 const int p = ulist[i];
-                const int idx = A.pix[p];
+                const int idx = (int)(ub & 0xFFFFFFu);
                 float xt, yt;
                 pixel_tilde_fast(g, idx, inv_cols, xt, yt);
                 float a0, a1, a2, imd, wr, mdz, mz0;
@@ -519,17 +654,10 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
                 if (KIND == MBX_GEOM_CONE) rec2[pos] = make_float4(imd, wr, mdz, mz0);
                 sbin[pos] = b;
             }
-            __syncthreads();
-            for (int bb = tid; bb < nbins; bb += CB_THREADS) {
-                int t = 0;
-                for (int w = 0; w < CB_WARPS; ++w) {
-                    t += wcnt[w * nbins + bb];
-                    wcnt[w * nbins + bb] = 0;
-                }
-                run[bb] += t;
-            }
-            __syncthreads();
+            // the next chunk's counts go to wcnt (cleared above); its starts overwrite wstart only after the
+            // barrier that follows, which every thread reaches after reading its start here
         }
+        __syncthreads();
         // ---- 3. warp ranges of bins with about equal record counts, at least two bins each:
         //         B_v = 2v + max_{u<=v}(lb_u - 2u), then B_v <= nbins - 2(8 - v); lb_v = first bin starting at or
         //         after v/8 of the records

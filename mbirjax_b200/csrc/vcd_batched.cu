@@ -360,6 +360,7 @@ struct Layout {
         bufs, total;
     int bp_total, fp_total, el_total, sn_total, rc_total;
     std::vector<size_t> buf_off;  // per scan: bp, delta, dsino
+    std::vector<size_t> box_off;  // per scan: chunk bounding boxes of its subsets, [K][chunks]
 };
 
 static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::vector<ScanSizes> &zs) {
@@ -401,6 +402,9 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
         L.buf_off[3 * s + 1] = take(4 * (size_t)zs[s].ncyl);
         L.buf_off[3 * s + 2] = take(4 * (size_t)zs[s].nsino);
     }
+    L.box_off.resize(n);
+    for (int s = 0; s < n; ++s)
+        L.box_off[s] = take((size_t)scans[s].num_subsets * fp_chunk_box_bytes(scans[s].subset_size));
     L.total = off;
     return MBX_OK;
 }
@@ -508,6 +512,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
             f.out = v.dsino;
             f.vox_by_index = 0;
             f.plan = z.fpp;
+            f.chunk_box = reinterpret_cast<const int4 *>(base + L.box_off[s] + (size_t)k * fp_chunk_box_bytes(sc.subset_size));
         }
         // bp_fast smem without view splits
         smem_bp = std::max(smem_bp, z.bpp.smem);
@@ -548,6 +553,18 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     std::memcpy(hsched, schedule, sizeof(int) * (size_t)num_steps * num_scans);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemcpyAsync(base, host.data(), host.size(), cudaMemcpyHostToDevice, st);
+    // chunk bounding boxes of every subset (the forward projection skips chunks that miss its channel block)
+    for (int s = 0; s < num_scans && e == cudaSuccess; ++s) {
+        const mbx_scan &sc = scans[s];
+        const unsigned nch = (unsigned)((sc.subset_size + CB_CHUNK - 1) / CB_CHUNK);
+        for (int k = 0; k < sc.num_subsets && e == cudaSuccess; ++k) {
+            int4 *box = reinterpret_cast<int4 *>(base + L.box_off[s] + (size_t)k * fp_chunk_box_bytes(sc.subset_size));
+            fp_chunk_bounds_kernel<<<nch, CB_CHUNK, 0, st>>>(sc.partition + (size_t)k * sc.subset_size, sc.subset_size,
+                                                             sc.geom.num_recon_rows, sc.geom.num_recon_cols, box);
+            note_launch();
+            e = cudaGetLastError();
+        }
+    }
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error(e);
 

@@ -20,7 +20,7 @@ import torch
 
 from . import _capi
 from .parameter_handler import ParameterHandler
-from .vcd_utils import gen_full_indices, gen_set_of_pixel_partitions, gen_partition_sequence
+from .vcd_utils import gen_full_indices, gen_set_of_pixel_partitions, gen_partition_sequence, morton_sorted_partition
 from .qggmrf import get_b_from_nbr_wts
 
 recon_param_names = ['num_iterations', 'granularity', 'partition_sequence', 'fm_rmse', 'prior_loss',
@@ -304,7 +304,9 @@ class TomographyModel(ParameterHandler):
         fm_hessian, fm_constant, qp, sigma_y = (state['fm_hessian'], state['fm_constant'], state['qp'],
                                                 state['sigma_y'])
         geom = self._geometry()
-        dev_partitions = [torch.as_tensor(part, device=dev, dtype=torch.int32).contiguous() for part in partitions]
+        # subsets in Z-order: same sets, spatially coherent processing order for the projectors
+        dev_partitions = [torch.as_tensor(morton_sorted_partition(part, recon_shape[1]), device=dev,
+                                          dtype=torch.int32).contiguous() for part in partitions]
         workspaces = {}
         max_subsets = max(part.shape[0] for part in partitions)
         stats = torch.zeros((max_subsets, 4), dtype=torch.float64, device=dev)

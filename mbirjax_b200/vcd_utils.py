@@ -58,3 +58,30 @@ def gen_partition_sequence(partition_sequence, max_iterations):
 def gen_full_indices(recon_shape, use_ror_mask=True):
     """All pixels of the region of reconstruction, sorted (vcd_utils.py:310-318)."""
     return gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask)[0]
+
+
+def morton_order(pixel_indices, num_cols):
+    """Positions of pixel_indices sorted by the Z-order (Morton) code of (row, col): neighbouring positions are
+    spatially close, so the channel gathers of a warp of the back projector stay within a few sectors."""
+    idx = np.asarray(pixel_indices, dtype=np.int64)
+    row, col = idx // num_cols, idx % num_cols
+
+    def spread(v):
+        v = v.astype(np.uint64) & np.uint64(0xFFFF)
+        v = (v | (v << np.uint64(8))) & np.uint64(0x00FF00FF)
+        v = (v | (v << np.uint64(4))) & np.uint64(0x0F0F0F0F)
+        v = (v | (v << np.uint64(2))) & np.uint64(0x33333333)
+        v = (v | (v << np.uint64(1))) & np.uint64(0x55555555)
+        return v
+
+    code = spread(row) | (spread(col) << np.uint64(1))
+    return np.argsort(code, kind='stable').astype(np.int32)
+
+
+def morton_sorted_partition(partition, num_cols):
+    """Each subset (row) of a partition reordered by the Z-order code of its pixels.  A subset is a set: the
+    VCD update does not depend on the order of its pixels, but the projectors run faster when consecutive
+    pixels are close in the image (fewer sectors per gather, and whole chunks of the list can be skipped by
+    the channel blocks of the forward projector they cannot reach)."""
+    partition = np.asarray(partition)
+    return np.stack([p[morton_order(p, num_cols)] for p in partition]).astype(np.int32)
