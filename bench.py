@@ -59,7 +59,16 @@ def parse_args():
     ap.add_argument('--workload', default='batched', choices=['batched', 'cone'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
-    return ap.parse_args()
+    ap.add_argument('--scans', type=int, default=None,
+                    help='batched workload: the first N scans only (a small case for profiling; default 24)')
+    ap.add_argument('--iterations', type=int, default=None, help='VCD iterations per scan (default 10 / 20)')
+    args = ap.parse_args()
+    if args.scans is not None:
+        BATCH['num_scans'] = args.scans
+    if args.iterations is not None:
+        BATCH['iterations'] = args.iterations
+        CONE['iterations'] = args.iterations
+    return args
 
 
 # ----------------------------------------------------------------------------------------------- helpers
