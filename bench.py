@@ -22,7 +22,9 @@ sinograms in pinned host memory and the recons copied back each step.  ``rooflin
 (the back- and forward-projection stages of a subset update) live with CUDA events and divides their algorithmic
 bytes, 4 (V N S + V R C) summed over scans, by the measured HBM copy bandwidth.  ``cpu_baseline`` times the
 oracle's restatement of the reference arithmetic on all host cores for one subset update of one scan and scales
-it by the same work model to the whole workload.
+it by the same work model to the whole workload.  ``autograd`` times one gradient of the differentiable
+cone-beam loss (weighted least squares + qGGMRF, backward through the matched back projector in 32-view chunks)
+against one forward projection on the same geometry.
 
 ``--impl reference`` times the reference arithmetic (the oracle port: JAX is not installable offline, so the
 reference's own JAX CPU path cannot run) on the host cores on the same workload and metric.
@@ -315,6 +317,48 @@ def timed_steps(step_fn, steps, warmup, world, flush):
     return start.elapsed_time(end)
 
 
+def autograd_cost():
+    """One gradient of 0.5 ||W^(1/2) (A x - y)||^2 + qGGMRF(x) through torch.autograd (forward projection, loss,
+    backward through the matched back projector in 32-view chunks and the qGGMRF gradient kernel) against one
+    forward projection of the same recon, on the cone geometry of the cone workload (256 views x 128 rows x 256
+    channels, recon 256x256x128, W = exp(-y / max y)).  CUDA events, 10 repetitions each after 3 warm-ups."""
+    import torch
+    import mbirjax_b200 as mb
+    from mbirjax_b200 import autograd as AG
+    model = mb.ConeBeamModel((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(), CONE['sdd'],
+                             CONE['sid'])
+    shape = tuple(model.get_params('recon_shape'))
+    gen = torch.Generator(device='cuda').manual_seed(2)
+    x = (torch.rand(shape, device='cuda', generator=gen) * 0.1).requires_grad_(True)
+    y = torch.rand((CONE['views'], CONE['rows'], CONE['channels']), device='cuda', generator=gen)
+    w = torch.exp(-y / y.max())
+    params = (mb.get_b_from_nbr_wts([1, 1, 1]), 0.3, 2.0, 1.2, 1.0)
+
+    def fwd():
+        with torch.no_grad():
+            AG.forward_project(x, model)
+
+    def grad():
+        loss = AG.weighted_ls_qggmrf_loss(x, model, y, w, params, view_chunk=32)
+        torch.autograd.grad(loss, x)
+
+    res = {}
+    for name, fn in (('fp_ms', fwd), ('grad_ms', grad)):
+        for _ in range(3):
+            fn()
+        torch.cuda.synchronize()
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        for _ in range(10):
+            fn()
+        e.record()
+        torch.cuda.synchronize()
+        res[name] = round(s.elapsed_time(e) / 10, 4)
+    res['grad_over_fp'] = round(res['grad_ms'] / res['fp_ms'], 3)
+    res['config'] = 'cone 256x128x256, recon 256x256x128, backward in 32-view chunks'
+    return res
+
+
 def kernel_roofline(model, sino, peak_gbs, peak_kind):
     """Average duration of one VCD subset's back and forward projection (CUDA events, 20 launches each)."""
     import torch
@@ -324,7 +368,10 @@ def kernel_roofline(model, sino, peak_gbs, peak_kind):
     V, R, C = model.get_params('sinogram_shape')
     S = model.get_params('recon_shape')[2]
     np.random.seed(CONE['seed'])
-    subset = mb.gen_pixel_partition(model.get_params('recon_shape'), CONE['subsets'])[0]
+    from mbirjax_b200.vcd_utils import morton_sorted_partition
+    # the subset in the Z-order the VCD path processes it in
+    subset = morton_sorted_partition(mb.gen_pixel_partition(model.get_params('recon_shape'), CONE['subsets']),
+                                     model.get_params('recon_shape')[1])[0]
     pix = torch.as_tensor(subset, device='cuda')
     n = int(pix.shape[0])
     vox = torch.rand((n, S), device='cuda')
@@ -402,15 +449,16 @@ def cpu_recons_per_s(subset_seconds):
 
 # ----------------------------------------------------------------------------------------------- arms
 def batched_config(world):
-    return {'workload': '24 uneven parallel-beam scans (views U{60..720}, rows U{8..64}, channels U{96..512}, '
-                        'seed i), 10 ellipsoids each, 10 VCD iterations x 4 subsets, FBP init; batched path',
+    return {'workload': '%d uneven parallel-beam scans (views U{60..720}, rows U{8..64}, channels U{96..512}, '
+                        'seed i), 10 ellipsoids each, %d VCD iterations x %d subsets, FBP init; batched path'
+                        % (BATCH['num_scans'], BATCH['iterations'], BATCH['subsets']),
             'num_scans': BATCH['num_scans'], 'iterations': BATCH['iterations'], 'subsets': BATCH['subsets'],
             'parallelism': 'replicas x%d' % world, 'l2': 'flushed before every step (inputs ~1 GB > L2)'}
 
 
 def cone_config(world):
-    return {'workload': 'plain cone-beam VCD, sinogram 256x128x256, recon 256x256x128, 20 iterations x 4 subsets, '
-                        'FDK init, sdd=sid=1024', 'views': CONE['views'], 'det_rows': CONE['rows'],
+    return {'workload': 'plain cone-beam VCD, sinogram 256x128x256, recon 256x256x128, %d iterations x %d subsets, '
+                        'FDK init, sdd=sid=1024' % (CONE['iterations'], CONE['subsets']), 'views': CONE['views'], 'det_rows': CONE['rows'],
             'det_channels': CONE['channels'], 'recon_shape': [256, 256, 128], 'iterations': CONE['iterations'],
             'subsets': CONE['subsets'], 'parallelism': 'replicas x%d' % world, 'l2': 'flushed before every step'}
 
@@ -531,6 +579,8 @@ def run_gpu(args):
         line['roofline'] = batched_roofline(models, sinos, peak_gbs, peak_kind)
     else:
         line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind)
+
+    line['autograd'] = autograd_cost()
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if args.workload == 'batched':
