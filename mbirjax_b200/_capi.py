@@ -55,6 +55,7 @@ _SIGNATURES = {
     'mbx_last_cuda_error': (ctypes.c_int, []),
     'mbx_get_device_error': (ctypes.c_int, [ctypes.POINTER(ctypes.c_int)]),
     'mbx_launch_count': (ctypes.c_uint64, []),
+    'mbx_set_autotune': (ctypes.c_int, [ctypes.c_int]),
     'mbx_forward_project_workspace_bytes': (c_size_t, [ctypes.POINTER(MbxGeom), c_int64, c_int32]),
     'mbx_sparse_forward_project': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_int64, c_void_p,
                                                   c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),
@@ -150,6 +151,11 @@ def _workspace(nbytes, device):
 
 def version():
     return load_library().mbx_version().decode()
+
+
+def set_autotune(enable):
+    """Turn the per-call-shape timing of candidate projector plans on (default) or off; returns the old setting."""
+    return bool(load_library().mbx_set_autotune(1 if enable else 0))
 
 
 def get_device_error():

@@ -1,6 +1,9 @@
 // Library identification, error reporting and device queries for the mbirjax_b200 C ABI.
 #include <atomic>
 #include <cstdio>
+#include <map>
+#include <mutex>
+#include <vector>
 
 #include "mbx_common.cuh"
 #include "mbx_host.hpp"
@@ -26,6 +29,40 @@ int *device_error_ptr() {
         cache[dev] = static_cast<int *>(p);
     }
     return cache[dev];
+}
+
+static std::atomic<bool> g_autotune{true};
+static std::mutex g_tune_mutex;
+static std::map<std::vector<long long>, int> g_tune_cache;
+
+bool autotune_enabled() { return g_autotune.load(std::memory_order_relaxed); }
+
+int autotune_lookup(const long long *key, int n) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<long long> k(key, key + n);
+    k.push_back(dev);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    auto it = g_tune_cache.find(k);
+    return it == g_tune_cache.end() ? -1 : it->second;
+}
+
+void autotune_store(const long long *key, int n, int choice) {
+    int dev = 0;
+    cudaGetDevice(&dev);
+    std::vector<long long> k(key, key + n);
+    k.push_back(dev);
+    std::lock_guard<std::mutex> lock(g_tune_mutex);
+    g_tune_cache[k] = choice;
+}
+
+bool stream_is_capturing(cudaStream_t st) {
+    cudaStreamCaptureStatus cs = cudaStreamCaptureStatusNone;
+    if (cudaStreamIsCapturing(st, &cs) != cudaSuccess) {
+        cudaGetLastError();
+        return true;  // unknown: do not synchronise on it
+    }
+    return cs != cudaStreamCaptureStatusNone;
 }
 
 static std::atomic<unsigned long long> g_launches{0};
@@ -102,6 +139,8 @@ extern "C" const char *mbx_error_string(int code) {
 extern "C" int mbx_last_cuda_error(void) { return mbx::t_last_cuda_error; }
 
 extern "C" uint64_t mbx_launch_count(void) { return mbx::g_launches.load(std::memory_order_relaxed); }
+
+extern "C" int mbx_set_autotune(int enable) { return mbx::g_autotune.exchange(enable != 0) ? 1 : 0; }
 
 extern "C" int mbx_get_device_error(int *flags_out) {
     if (!flags_out) return MBX_ERR_INVALID_ARG;

@@ -211,26 +211,36 @@ size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views
     return plan_fp(g, num_pixels, num_views_sel).workspace;
 }
 
-template <int KIND>
-static cudaError_t launch_fp_cb(const FpArgs &A, cudaStream_t st) {
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(fp_cb_kernel<KIND>, cudaFuncAttributeMaxDynamicSharedMemorySize,
+template <int KIND, int MINB>
+static cudaError_t launch_fp_cb_v(const FpArgs &A, cudaStream_t st) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
+        cudaError_t e = cudaFuncSetAttribute(fp_cb_kernel<KIND, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
                                              200 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
     dim3 grid(A.num_views_sel, A.plan.cblocks);
-    fp_cb_kernel<KIND><<<grid, CB_THREADS, A.plan.smem, st>>>(A, device_error_ptr());
+    fp_cb_kernel<KIND, MINB><<<grid, CB_THREADS, A.plan.smem, st>>>(A, device_error_ptr());
     note_launch();
     return cudaGetLastError();
+}
+
+static cudaError_t launch_fp_cb(const FpArgs &A, cudaStream_t st) {
+    const bool par = A.g.kind == MBX_GEOM_PARALLEL;
+    if (A.plan.minb >= 3)
+        return par ? launch_fp_cb_v<MBX_GEOM_PARALLEL, 3>(A, st) : launch_fp_cb_v<MBX_GEOM_CONE, 3>(A, st);
+    return par ? launch_fp_cb_v<MBX_GEOM_PARALLEL, 2>(A, st) : launch_fp_cb_v<MBX_GEOM_CONE, 2>(A, st);
 }
 
 int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, long long num_pixels,
                     const int32_t *views, int num_views_sel, float *out, void *ws, size_t ws_bytes,
                     cudaStream_t st) {
-    const CbPlan cpl = plan_fp_cb(g, num_views_sel, 4LL * num_sms());
-    if (cpl.ok && num_pixels * g.num_recon_slices < (1LL << 31)) {  // 32-bit cylinder offsets
+    CbPlan cand[3];
+    const int ncand = fp_cb_candidates(g, num_views_sel, 4LL * num_sms(), cand);
+    if (ncand > 0 && num_pixels * g.num_recon_slices < (1LL << 31)) {  // 32-bit cylinder offsets
         FpArgs A;
         A.g = g;
         A.vox = vox;
@@ -240,7 +250,7 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
         A.num_views_sel = num_views_sel;
         A.out = out;
         A.vox_by_index = 0;
-        A.plan = cpl;
+        A.plan = cand[0];
         // bounding boxes of the list's chunks, so that each channel block skips the chunks that miss it
         const size_t need = fp_chunk_box_bytes(num_pixels);
         if (need > 0 && (ws == nullptr || ws_bytes < need)) return MBX_ERR_WORKSPACE;
@@ -252,8 +262,34 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
             cudaError_t e0 = cudaGetLastError();
             if (e0 != cudaSuccess) return set_cuda_error(e0);
         }
-        cudaError_t e = (g.kind == MBX_GEOM_PARALLEL) ? launch_fp_cb<MBX_GEOM_PARALLEL>(A, st)
-                                                       : launch_fp_cb<MBX_GEOM_CONE>(A, st);
+        // plan choice: cached per call shape, or timed now (each candidate overwrites the whole output)
+        int choice = 0;
+        if (ncand > 1 && num_pixels > 0 && autotune_enabled()) {
+            long long n2 = 1;
+            while (n2 < num_pixels) n2 <<= 1;
+            const long long key[10] = {1, g.kind, num_views_sel, g.num_det_rows, g.num_det_channels,
+                                       g.num_recon_slices, g.num_recon_rows, g.num_recon_cols, n2, views ? 1 : 0};
+            choice = autotune_lookup(key, 10);
+            if (choice < 0 || choice >= ncand) {
+                choice = 0;
+                if (!stream_is_capturing(st)) {
+                    float best = 3.0e38f;
+                    for (int c = 0; c < ncand; ++c) {
+                        A.plan = cand[c];
+                        float ms = 0.0f;
+                        cudaError_t e = time_on_stream([&]() { return launch_fp_cb(A, st); }, st, ms);
+                        if (e != cudaSuccess) return set_cuda_error(e);
+                        if (ms < best) {
+                            best = ms;
+                            choice = c;
+                        }
+                    }
+                    autotune_store(key, 10, choice);
+                }
+            }
+        }
+        A.plan = cand[choice];
+        cudaError_t e = launch_fp_cb(A, st);
         return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
     }
     const FpPlan pl = plan_fp(g, num_pixels, num_views_sel);

@@ -52,6 +52,7 @@ struct CbPlan {
     int fill;        // the scan stops adding pixels once a pass holds more than this many
     int nbins;       // nb + 2
     int cblocks;     // channel blocks per view
+    int minb;        // resident CTAs per SM the kernel variant is compiled for (2 or 3)
     // shared-memory layout (4-byte words)
     int o_rec, o_rec2, o_sbin, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_wstart, o_cone, o_hl, o_misc;
     size_t smem;
@@ -89,9 +90,12 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
 }
 
 // num_views_sel: views per call (0 = all); min_blocks: CTAs wanted per call (a narrower channel block is
-// chosen to reach it); 0 = widest block.
-inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min_blocks = 0) {
+// chosen to reach it); 0 = widest block.  minb: 2 (first shared-memory tier 112 KB) or 3 (74 KB, for the kernel
+// variant compiled for three resident CTAs per SM); nb_max: widest channel block allowed.
+inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min_blocks = 0, int minb = 2,
+                         int nb_max = 128) {
     CbPlan pl = {};
+    pl.minb = minb;
     pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || g.bp_psf_radius == 1);
     const int R = g.num_det_rows, C = g.num_det_channels;
     // lane layout: padded rows weighted by the cost of ppw diverging sub-groups, plus a small cost per pass
@@ -112,10 +116,10 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
     pl.row_passes = ceil_div(R, pl.rl * pl.rpl);
     pl.rpad = pl.row_passes * pl.rl * pl.rpl;
     // widest channel block, then largest pass, that fit the shared-memory tier (2, then 1 CTA per SM)
-    static const size_t tiers[2] = {MBX_FPCB_SMEM_TIER0, 200 * 1024};
+    const size_t tiers[2] = {minb >= 3 ? (size_t)74 * 1024 : (size_t)MBX_FPCB_SMEM_TIER0, (size_t)200 * 1024};
     bool found = false;
     for (int t = 0; t < 2 && !found; ++t) {
-        for (int nb = 128; nb >= 32 && !found; nb >>= 1) {
+        for (int nb = nb_max; nb >= 32 && !found; nb >>= 1) {
             const long long nv = num_views_sel > 0 ? num_views_sel : g.num_views;
             if (nb > 32 && min_blocks > 0 && (long long)ceil_div(C, nb) * nv < min_blocks) continue;
             for (int cap = 2048; cap >= 512 && !found; cap >>= 1) {
@@ -143,6 +147,22 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
         if (1.0 / g.magnification - dinv <= 1e-6) pl.ok = false;  // recon reaches the source
     }
     return pl;
+}
+
+// The plans an autotuner times for one call shape: the default, the variant compiled for three resident CTAs
+// per SM (smaller passes), and narrower channel blocks (more CTAs, shorter bins).  Returns how many are usable.
+inline int fp_cb_candidates(const mbx_geom &g, int num_views_sel, long long min_blocks, CbPlan out[3]) {
+    int n = 0;
+    const CbPlan c0 = plan_fp_cb(g, num_views_sel, min_blocks, 2, 128);
+    if (!c0.ok) return 0;
+    out[n++] = c0;
+    const CbPlan c1 = plan_fp_cb(g, num_views_sel, min_blocks, 3, 128);
+    if (c1.ok) out[n++] = c1;
+    if (c0.nb > 32) {
+        const CbPlan c2 = plan_fp_cb(g, num_views_sel, min_blocks, 2, c0.nb / 2);
+        if (c2.ok) out[n++] = c2;
+    }
+    return n;
 }
 
 // Fractional centre channel n_p of one pixel.
@@ -723,11 +743,9 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     }
 }
 
-template <int KIND>
-#ifndef MBX_FPCB_MIN_BLOCKS
-#define MBX_FPCB_MIN_BLOCKS 2  // resident CTAs per SM the forward projection is compiled for
-#endif
-__global__ void __launch_bounds__(CB_THREADS, MBX_FPCB_MIN_BLOCKS) fp_cb_kernel(const FpArgs A, int *err) {
+// MINB = plan.minb: the variant compiled for 2 resident CTAs per SM (up to 128 registers) or 3 (up to 85).
+template <int KIND, int MINB>
+__global__ void __launch_bounds__(CB_THREADS, MINB) fp_cb_kernel(const FpArgs A, int *err) {
     extern __shared__ __align__(16) float smcb[];
     fp_cb_tile<KIND>(A, blockIdx.x, blockIdx.y, smcb, err);
 }

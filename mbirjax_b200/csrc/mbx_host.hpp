@@ -37,6 +37,40 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
                  const int32_t *views, int num_views_sel, int coeff_power, float scale, float *out, void *ws,
                  size_t ws_bytes, cudaStream_t st);
 
+// Autotuning.  The first call of a projector for a given call shape (geometry sizes, views, pixel count rounded
+// up to a power of two) times its candidate plans on the caller's stream and remembers the fastest; later calls
+// of that shape launch it directly.  Calls made while their stream is being captured into a CUDA graph use the
+// default plan and do not tune.  The cache is host memory only; mbx_set_autotune(0) selects the default plans.
+bool autotune_enabled();
+int autotune_lookup(const long long *key, int n);  // -1 if the shape has not been tuned
+void autotune_store(const long long *key, int n, int choice);
+bool stream_is_capturing(cudaStream_t st);
+// Milliseconds of the launches `launch` enqueues on st (one untimed call first, then the best of two).
+template <class F>
+cudaError_t time_on_stream(F launch, cudaStream_t st, float &ms) {
+    cudaError_t e = launch();
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    if ((e = cudaEventCreate(&a)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return e;
+    }
+    ms = 3.0e38f;
+    for (int r = 0; r < 2 && e == cudaSuccess; ++r) {
+        e = cudaEventRecord(a, st);
+        if (e == cudaSuccess) e = launch();
+        if (e == cudaSuccess) e = cudaEventRecord(b, st);
+        if (e == cudaSuccess) e = cudaEventSynchronize(b);
+        float t = 0.0f;
+        if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+        if (e == cudaSuccess && t < ms) ms = t;
+    }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return e;
+}
+
 // Bytes rounded up to a 256-byte boundary (workspace carving).
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 

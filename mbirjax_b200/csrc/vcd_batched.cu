@@ -71,6 +71,7 @@ struct BatchedPlanHost {
     int bp_total, fp_total, el_total, sn_total, rc_total;
     int bp_grid, fp_grid, el_grid, sn_grid, rc_grid;
     size_t bp_smem, fp_smem;
+    int fp_minb;  // b_fp variant: 2 or 3 resident CTAs per SM
     int magic;
 };
 static_assert(sizeof(BatchedPlanHost) <= sizeof(mbx_batched_plan), "plan record too large");
@@ -133,11 +134,9 @@ __global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(BatchedT
     }
 }
 
-template <int KIND>
-#ifndef MBX_BFP_MIN_BLOCKS
-#define MBX_BFP_MIN_BLOCKS 2  // resident CTAs per SM the batched forward projection is compiled for
-#endif
-__global__ void __launch_bounds__(CB_THREADS, MBX_BFP_MIN_BLOCKS) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
+// MINB: resident CTAs per SM the variant is compiled for (2 or 3, matching the plans' fp_cb minb).
+template <int KIND, int MINB>
+__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
     extern __shared__ __align__(16) float smf2[];
     for (int t = fetch_tile(T.counters + 1); t < total; t = fetch_tile(T.counters + 1)) {
         const int k = find_scan(T.fp_off, num_scans, t);
@@ -432,6 +431,77 @@ extern "C" size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t
     return L.total;
 }
 
+static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStream_t st);
+
+// Autotuning of the forward-projection stage: the plans of every scan with the kernel variant compiled for 2
+// resident CTAs per SM (the tables as built) against the same channel blocks with smaller passes and the variant
+// compiled for 3.  Each is timed on step 0 (the stage only writes the scans' projection scratch, whose input is
+// zeroed first); the faster one's argument table stays on the device, and the choice is remembered for the
+// batch shape, so later plans of the same batch do not time again.
+static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vector<ScanSizes> &zs,
+                           const mbx_scan *scans, int num_scans, const FpArgs *hf2, cudaStream_t st) {
+    int ksum = 0;
+    for (int s = 0; s < num_scans; ++s) ksum += scans[s].num_subsets;
+    std::vector<FpArgs> f3(hf2, hf2 + ksum);
+    size_t smem3 = 0;
+    int ki = 0;
+    for (int s = 0; s < num_scans; ++s) {
+        const CbPlan c3 = plan_fp_cb(scans[s].geom, 0, 0, 3, zs[s].fpp.nb);
+        if (!c3.ok || c3.nb != zs[s].fpp.nb || c3.cblocks != zs[s].fpp.cblocks) return MBX_OK;  // same work list only
+        smem3 = std::max(smem3, c3.smem);
+        for (int k = 0; k < scans[s].num_subsets; ++k, ++ki) f3[ki].plan = c3;
+    }
+    char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
+    // the choice is cached per batch shape (every scan's sizes, subsets and pixels per subset)
+    std::vector<long long> key = {2, P.kind, num_scans};
+    for (int s = 0; s < num_scans; ++s) {
+        const mbx_geom &g = scans[s].geom;
+        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
+                               g.num_recon_slices, scans[s].num_subsets, scans[s].subset_size});
+    }
+    auto use3 = [&]() -> int {
+        cudaError_t e3 = cudaMemcpyAsync(base + L.fpargs, f3.data(), sizeof(FpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        if (e3 == cudaSuccess) e3 = cudaStreamSynchronize(st);
+        if (e3 != cudaSuccess) return set_cuda_error(e3);
+        P.fp_minb = 3;
+        P.fp_smem = smem3;
+        P.fp_grid = (P.kind == MBX_GEOM_PARALLEL) ? occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 3>, smem3, P.fp_total)
+                                                  : occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, smem3, P.fp_total);
+        return MBX_OK;
+    };
+    const int cached = autotune_lookup(key.data(), (int)key.size());
+    if (cached == 2) return MBX_OK;
+    if (cached == 3) return use3();
+    if (stream_is_capturing(st)) return MBX_OK;
+    cudaError_t e = cudaSuccess;
+    for (int s = 0; s < num_scans && e == cudaSuccess; ++s)
+        e = cudaMemsetAsync(base + L.buf_off[3 * s + 1], 0, 4 * (size_t)zs[s].ncyl, st);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    int rc = MBX_OK;
+    auto run = [&]() {
+        rc = launch_stage(&P, 0, 2, st);
+        return rc == MBX_OK ? cudaSuccess : cudaErrorLaunchFailure;
+    };
+    float t2 = 0.0f, t3 = 0.0f;
+    e = time_on_stream(run, st, t2);
+    if (rc != MBX_OK) return rc;
+    if (e != cudaSuccess) return set_cuda_error(e);
+    const BatchedPlanHost keep = P;
+    rc = use3();
+    if (rc != MBX_OK) return rc;
+    e = time_on_stream(run, st, t3);
+    if (rc != MBX_OK) return rc;
+    if (e != cudaSuccess) return set_cuda_error(e);
+    autotune_store(key.data(), (int)key.size(), t2 <= t3 ? 2 : 3);
+    if (t2 <= t3) {  // back to the tables as built
+        P = keep;
+        e = cudaMemcpyAsync(base + L.fpargs, hf2, sizeof(FpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return set_cuda_error(e);
+    }
+    return MBX_OK;
+}
+
 extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans, const int32_t *schedule,
                                        int32_t num_steps, int32_t num_iterations, double *step_stats,
                                        double *iter_stats, void *workspace, size_t workspace_bytes,
@@ -603,17 +673,20 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     P.rc_total = L.rc_total;
     P.bp_smem = smem_bp;
     P.fp_smem = smem_fp;
+    P.fp_minb = 2;
     // kernel attributes and resident-CTA grids
     if (P.kind == MBX_GEOM_PARALLEL) {
         cudaFuncSetAttribute(b_bp<MBX_GEOM_PARALLEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-        cudaFuncSetAttribute(b_fp<MBX_GEOM_PARALLEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(b_fp<MBX_GEOM_PARALLEL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(b_fp<MBX_GEOM_PARALLEL, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, smem_bp, L.bp_total);
-        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_PARALLEL>, smem_fp, L.fp_total);
+        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, smem_fp, L.fp_total);
     } else {
         cudaFuncSetAttribute(b_bp<MBX_GEOM_CONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-        cudaFuncSetAttribute(b_fp<MBX_GEOM_CONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(b_fp<MBX_GEOM_CONE, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        cudaFuncSetAttribute(b_fp<MBX_GEOM_CONE, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
         P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_CONE>, smem_bp, L.bp_total);
-        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_CONE>, smem_fp, L.fp_total);
+        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, smem_fp, L.fp_total);
     }
     {   // load every stage kernel now (lazy module loading must not happen inside a stream capture)
         cudaFuncAttributes fa;
@@ -632,6 +705,10 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     P.rc_grid = occupancy_grid(b_iter_partials, 0, L.sn_total + L.rc_total);
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e);
+    if (autotune_enabled()) {
+        const int rc2 = tune_batched_fp(P, L, zs, scans, num_scans, hf, st);
+        if (rc2 != MBX_OK) return rc2;
+    }
     P.magic = BT_MAGIC;
     std::memset(plan_out, 0, sizeof(*plan_out));
     std::memcpy(plan_out, &P, sizeof(P));
@@ -666,10 +743,17 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
                 const cudaError_t me = cudaMemsetAsync(T.counters + 1, 0, sizeof(int), st);
                 if (me != cudaSuccess) return set_cuda_error(me);
             }
-            if (P->kind == MBX_GEOM_PARALLEL)
-                b_fp<MBX_GEOM_PARALLEL><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
-            else
-                b_fp<MBX_GEOM_CONE><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+            if (P->kind == MBX_GEOM_PARALLEL) {
+                if (P->fp_minb >= 3)
+                    b_fp<MBX_GEOM_PARALLEL, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+                else
+                    b_fp<MBX_GEOM_PARALLEL, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+            } else {
+                if (P->fp_minb >= 3)
+                    b_fp<MBX_GEOM_CONE, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+                else
+                    b_fp<MBX_GEOM_CONE, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+            }
             break;
         case 3: b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;
         case 4: b_alpha<<<warp_blocks, 256, 0, st>>>(T, n, step); break;

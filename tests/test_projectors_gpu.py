@@ -182,3 +182,26 @@ def test_determinism_of_back_projection(cuda):
     a = model.sparse_back_project(y, idx).cpu().numpy()
     b = model.sparse_back_project(y, idx).cpu().numpy()
     np.testing.assert_array_equal(a, b)   # no float atomics on the back-projection side
+
+
+def test_autotuned_plans_agree_with_default(cuda):
+    """The plan the autotuner picks for a call shape computes the same projection as the default plan, up to
+    float summation order; repeated calls of the tuned shape are bitwise reproducible."""
+    from mbirjax_b200 import _capi
+    for kind, (v, r, c) in (('parallel', (40, 12, 96)), ('cone', (32, 24, 64))):
+        model, geom = make_case(kind, views=v, rows=r, channels=c)
+        nr, nc, ns = geom.recon_shape
+        np.random.seed(5)
+        sub = mb.gen_pixel_partition(geom.recon_shape, 3)[0]
+        vox = np.random.default_rng(1).random((sub.shape[0], ns)).astype(np.float32)
+        old = _capi.set_autotune(False)
+        try:
+            ref = model.sparse_forward_project(vox, sub).cpu().numpy()
+            _capi.set_autotune(True)
+            tuned = model.sparse_forward_project(vox, sub).cpu().numpy()   # tunes this shape
+            again = model.sparse_forward_project(vox, sub).cpu().numpy()   # cached choice
+        finally:
+            _capi.set_autotune(old)
+        assert rel_l2(tuned, ref) <= 1e-6
+        np.testing.assert_array_equal(tuned, again)
+        np.testing.assert_allclose(ref, O.sparse_forward_project(geom, vox, sub), rtol=2e-4, atol=2e-5 * np.abs(ref).max())
