@@ -95,13 +95,15 @@ MBX_API int mbx_get_device_error(int *flags_out);
  * streams; launches replayed from a captured CUDA graph are not re-counted). */
 MBX_API uint64_t mbx_launch_count(void);
 /* Autotuning of the projector plans (no counterpart in the reference, whose XLA compiler picks its own
- * schedule): the first mbx_sparse_forward_project of a call shape (geometry sizes, views, pixel count rounded up
- * to a power of two) times its candidate plans (channel-block width, pass size, the kernel variant compiled for
- * 2 or 3 resident CTAs per SM) on the caller's stream, synchronising it, and caches the fastest for the process;
- * a call made while its stream is captured uses the default plan.  mbx_vcd_batched_prepare tunes the batched
- * forward-projection stage the same way.  Results of different plans differ only in float rounding order.
- * enable = 0 selects the default plans everywhere; returns the previous setting (default 1). */
-MBX_API int mbx_set_autotune(int enable);
+ * schedule).  The first mbx_sparse_forward_project / mbx_sparse_back_project of a call shape (geometry sizes,
+ * views, pixel count rounded up to a power of two) times its candidate plans on the caller's stream,
+ * synchronising it, and caches the fastest for the process; a call made while its stream is captured uses the
+ * default plan.  Forward candidates: channel-block width, pass size, and the kernel variant compiled for 2 or 3
+ * resident CTAs per SM; back-projection candidates: footprints staged in shared memory or computed per thread.
+ * mbx_vcd_batched_prepare tunes its two projection stages the same way, cached per batch shape.  Plans differ
+ * only in float summation order.  mode: 0 = default plans, 1 = tune (default), k >= 2 = use candidate k-1 (or the
+ * last one) everywhere without timing (to check every plan against the default).  Returns the previous mode. */
+MBX_API int mbx_set_autotune(int mode);
 
 /* ---- projectors ------------------------------------------------------------------------------- */
 

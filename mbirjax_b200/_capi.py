@@ -153,9 +153,13 @@ def version():
     return load_library().mbx_version().decode()
 
 
-def set_autotune(enable):
-    """Turn the per-call-shape timing of candidate projector plans on (default) or off; returns the old setting."""
-    return bool(load_library().mbx_set_autotune(1 if enable else 0))
+def set_autotune(mode):
+    """0: default projector plans; 1 (default): time the candidate plans once per call shape and keep the
+    fastest; k >= 2: always candidate k-1 (a test hook).  Returns the previous mode."""
+    old = load_library().mbx_set_autotune(int(mode))
+    if old < 0:
+        raise ValueError('mode must be >= 0')
+    return old
 
 
 def get_device_error():

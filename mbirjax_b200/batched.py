@@ -104,7 +104,15 @@ class BatchedVCD:
             self.graph.replay()
         else:
             run_all()
-        return self._results(max_iterations)
+        out = self._results(max_iterations)  # reads the statistics back (synchronises)
+        # release the graph and the scratch now rather than whenever the object is collected, so that the
+        # next reconstruction finds its memory in the caching allocator instead of allocating afresh
+        if self.graph is not None:
+            self.graph.reset()
+            self.graph = None
+        self.workspace = None
+        self.plan = None  # its tables lived in the workspace
+        return out
 
     def _results(self, max_iterations):
         step = self.step_stats.cpu().numpy()

@@ -31,11 +31,13 @@ static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const fl
                                   const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
                                   float *dst, long long ss, cudaStream_t st) {
     auto kern = bp_fast_kernel<KIND>;
-    static bool attr_set = false;
-    if (!attr_set) {
+    static bool attr_set[64] = {false};
+    int dev = 0;
+    cudaGetDevice(&dev);
+    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
         cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
         if (e != cudaSuccess) return e;
-        attr_set = true;
+        if (dev >= 0 && dev < 64) attr_set[dev] = true;
     }
     BpArgs A;
     A.g = g;
@@ -69,18 +71,46 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
         float *dst = fpl.splits > 1 ? static_cast<float *>(ws) : out;
         const long long stride = num_pixels * (long long)g.num_recon_slices;
         const long long ss = fpl.splits > 1 ? stride : 0;
-        cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
-                            ? launch_bp_fast<MBX_GEOM_PARALLEL>(g, fpl, sino, w, pix, num_pixels, views, num_views_sel,
-                                                                coeff_power, scale, dst, ss, st)
-                            : launch_bp_fast<MBX_GEOM_CONE>(g, fpl, sino, w, pix, num_pixels, views, num_views_sel,
-                                                            coeff_power, scale, dst, ss, st);
-        if (e != cudaSuccess) return set_cuda_error(e);
-        if (fpl.splits > 1) {
-            launch_split_sum(dst, stride, fpl.splits, scale, out, stride, st);
-            e = cudaGetLastError();
-            if (e != cudaSuccess) return set_cuda_error(e);
+        auto run = [&](const BpfPlan &pl) -> cudaError_t {
+            cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
+                                ? launch_bp_fast<MBX_GEOM_PARALLEL>(g, pl, sino, w, pix, num_pixels, views, num_views_sel,
+                                                                    coeff_power, scale, dst, ss, st)
+                                : launch_bp_fast<MBX_GEOM_CONE>(g, pl, sino, w, pix, num_pixels, views, num_views_sel,
+                                                                coeff_power, scale, dst, ss, st);
+            if (e != cudaSuccess) return e;
+            if (pl.splits > 1) {
+                launch_split_sum(dst, stride, pl.splits, scale, out, stride, st);
+                e = cudaGetLastError();
+            }
+            return e;
+        };
+        // staged (shared-memory) or per-thread (inline) footprints: cached per call shape, or timed now (each
+        // candidate overwrites the whole output); both have the same grid, splits and workspace
+        BpfPlan cand[2] = {fpl, plan_bp_fast(g, num_pixels, num_views_sel, 1)};
+        int choice = 0;
+        if (autotune_forced() >= 0) {
+            choice = autotune_forced() >= 1 ? 1 : 0;
+        } else if (autotune_enabled()) {
+            long long n2 = 1;
+            while (n2 < num_pixels) n2 <<= 1;
+            const long long key[11] = {3, g.kind, num_views_sel, g.num_det_rows, g.num_det_channels, g.num_recon_slices,
+                                       g.num_recon_rows, g.num_recon_cols, n2, views ? 1 : 0, w ? 1 : 0};
+            choice = autotune_lookup(key, 11);
+            if (choice < 0 || choice > 1) {
+                choice = 0;
+                if (!stream_is_capturing(st)) {
+                    float t[2] = {0.0f, 0.0f};
+                    for (int c = 0; c < 2; ++c) {
+                        const cudaError_t e = time_on_stream([&]() { return run(cand[c]); }, st, t[c]);
+                        if (e != cudaSuccess) return set_cuda_error(e);
+                    }
+                    choice = t[1] < t[0] ? 1 : 0;
+                    autotune_store(key, 11, choice);
+                }
+            }
         }
-        return MBX_OK;
+        const cudaError_t e = run(cand[choice]);
+        return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
     }
     const BpPlan pl = plan_bp(g, num_pixels, num_views_sel);
     if (pl.workspace > 0 && (ws == nullptr || ws_bytes < pl.workspace)) return MBX_ERR_WORKSPACE;

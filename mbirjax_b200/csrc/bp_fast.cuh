@@ -37,8 +37,10 @@ struct BpfPlan {
     int nsl;      // slice tiles per CTA (warps per pixel group)
     int npg;      // pixel groups of 32 per CTA
     int lg_pcta;  // log2(32 * npg)
-    int chunk;    // footprints staged per view chunk (a multiple of BPF_THREADS)
-    int vc;       // views per chunk = chunk / (32 * npg)
+    int chunk;    // footprints staged per view chunk (a multiple of BPF_THREADS); 0 with inline footprints
+    int vc;       // views per chunk = chunk / (32 * npg); with inline footprints, views per table refill
+    int inline_fp;  // 1: each thread computes its own pixel's footprints in registers (no staging, no barriers
+                    // inside a view table); pays off when few warps share a pixel (short cylinders)
     int ts;       // slices per tile (<= BPF_ST)
     int tiles;    // ceil(S / ts)
     int gx, gy, splits, views_per_split;
@@ -179,9 +181,11 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
         }
     }
     bool active = p < num_pixels && ns > 0;
+    float oxt = 0.0f, oyt = 0.0f;  // this thread's own pixel (inline footprints)
     if (active) {
         const int idx = pix[p];
         active = idx >= 0 && idx < npix_grid;
+        if (active) pixel_tilde(g, idx, oxt, oyt);
     }
 
     float acc[BPF_ST];
@@ -191,116 +195,141 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
     const float z0 = g.recon_slice_offset - g.delta_voxel * 0.5f * (float)(num_slices - 1);
     float *mycache = cache + tid;
 
-    for (int vb = v_begin; vb < v_end; vb += vc) {
-        const int nv = min(vc, v_end - vb);
-        __syncthreads();
-        if (tid < nv) {
-            const int vi = views ? views[vb + tid] : vb + tid;
-            const bool ok = vi >= 0 && vi < g.num_views;
-            if (!ok && bx == 0 && by == 0) flag_error(err, MBX_ERRFLAG_VIEW);
-            const float ang = ok ? g.angles[vi] : 0.0f;
-            s_voff[tid] = ok ? vi * view_stride : -1;
-            s_cs[tid] = cosf(ang);
-            s_sn[tid] = sinf(ang);
-        }
-        __syncthreads();
-        for (int f = tid; f < chunk; f += BPF_THREADS) {
-            const int t = f >> lg_pcta;
-            if (t < nv) {
-                float4 fa = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f), fb = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (fvalid && s_voff[t] >= 0) bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb);
-                s_fa[f] = fa;
-                if (KIND == MBX_GEOM_CONE) s_fb[f] = fb;
-            }
-        }
-        __syncthreads();
-        if (!active) continue;
-        for (int t = 0; t < nv; ++t) {
-            const int f = (t << lg_pcta) + pl;
-            const float4 fa = s_fa[f];
-            const int first = __float_as_int(fa.x);
-            if (first < 0) continue;
-            const int voff = s_voff[t];
-            if (KIND == MBX_GEOM_PARALLEL) {
-                // three taps at constant offsets from one 32-bit element offset, one detector row per slice
-                int o = voff + s0c + first;
-                if (wts) {
-#pragma unroll
-                    for (int s = 0; s < BPF_ST; ++s) {
-                        if (s < ns) {
-                            const float *q = sino + o, *qw = wts + o;
-                            acc[s] = fmaf(fa.y, __ldg(q) * __ldg(qw),
-                                          fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fmaf(fa.w, __ldg(q + 2) * __ldg(qw + 2), acc[s])));
-                        }
-                        o += num_channels;
-                    }
-                } else if (ns == BPF_ST) {  // full tile: no guards
-#pragma unroll
-                    for (int s = 0; s < BPF_ST; ++s) {
-                        const float *q = sino + o;
-                        acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
-                        o += num_channels;
-                    }
-                } else {
-#pragma unroll
-                    for (int s = 0; s < BPF_ST; ++s) {
-                        if (s < ns) {
-                            const float *q = sino + o;
-                            acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
-                        }
-                        o += num_channels;
-                    }
-                }
-            } else {
-                const float4 fb = s_fb[f];
-                const float A0 = fb.x, A1 = fb.y, c2 = fb.z;
-                const float half_w = (A1 + 1.0f) * 0.5f;
-                const float l_max = fminf(1.0f, A1);
-                const int mc_first = (int)rintf(fmaf((float)s0, A1, A0));
-                const int mc_last = (int)rintf(fmaf((float)(s0 + ns - 1), A1, A0));
-                const int m_lo = min(mc_first, mc_last) - 1;
-                const int m_hi = max(mc_first, mc_last) + 1;
-                if (m_hi - m_lo + 1 > BPF_CACHE_ROWS) {  // excluded by plan_bp_fast; never read past the cache
-                    flag_error(err, MBX_ERRFLAG_CACHE);
-                    continue;
-                }
-                for (int m = m_lo; m <= m_hi; ++m) {
-                    float c = 0.0f;
-                    if (m >= 0 && m < num_rows) {
-                        const int o = voff + m * num_channels + first;
-                        const float *q = sino + o;
-                        if (wts) {
-                            const float *qw = wts + o;
-                            c = fmaf(fa.y, __ldg(q) * __ldg(qw), fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fa.w * (__ldg(q + 2) * __ldg(qw + 2))));
-                        } else {
-                            c = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fa.w * __ldg(q + 2)));
-                        }
-                    }
-                    mycache[(m - m_lo) * BPF_THREADS] = c;
-                }
+    // gather of one view into the accumulators, from the footprint fa (+ fb for cone) at view offset voff
+    auto gather = [&](const float4 &fa, const float4 &fb, int voff) {
+        const int first = __float_as_int(fa.x);
+        if (KIND == MBX_GEOM_PARALLEL) {
+            // three taps at constant offsets from one 32-bit element offset, one detector row per slice
+            int o = voff + s0c + first;
+            if (wts) {
 #pragma unroll
                 for (int s = 0; s < BPF_ST; ++s) {
                     if (s < ns) {
-                        const float k = (float)(s0 + s);
-                        const float m_p = fmaf(k, A1, A0);
-                        const int m_c = (int)rintf(m_p);
-                        const float d = m_p - (float)m_c;
-                        const float z = fmaf(k, g.delta_voxel, z0);
-                        const float q = fmaf(c2, z * z, 1.0f);
-                        float sec = q * rsqrtf(q);                       // 1 / cos(phi_k)
-                        const float l_m = fminf(fmaxf(half_w - fabsf(d + 1.0f), 0.0f), l_max);
-                        const float l_0 = fminf(fmaxf(half_w - fabsf(d), 0.0f), l_max);
-                        const float l_p = fminf(fmaxf(half_w - fabsf(d - 1.0f), 0.0f), l_max);
-                        const float *cc = mycache + (m_c - m_lo) * BPF_THREADS;
-                        const float cm = cc[-BPF_THREADS], c0 = cc[0], cp = cc[BPF_THREADS];
-                        if (coeff_power == 2) {
-                            sec *= sec;
-                            acc[s] = fmaf(sec, fmaf(l_m * l_m, cm, fmaf(l_0 * l_0, c0, (l_p * l_p) * cp)), acc[s]);
-                        } else {
-                            acc[s] = fmaf(sec, fmaf(l_m, cm, fmaf(l_0, c0, l_p * cp)), acc[s]);
-                        }
+                        const float *q = sino + o, *qw = wts + o;
+                        acc[s] = fmaf(fa.y, __ldg(q) * __ldg(qw),
+                                      fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fmaf(fa.w, __ldg(q + 2) * __ldg(qw + 2), acc[s])));
+                    }
+                    o += num_channels;
+                }
+            } else if (ns == BPF_ST) {  // full tile: no guards
+#pragma unroll
+                for (int s = 0; s < BPF_ST; ++s) {
+                    const float *q = sino + o;
+                    acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
+                    o += num_channels;
+                }
+            } else {
+#pragma unroll
+                for (int s = 0; s < BPF_ST; ++s) {
+                    if (s < ns) {
+                        const float *q = sino + o;
+                        acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
+                    }
+                    o += num_channels;
+                }
+            }
+        } else {
+            const float A0 = fb.x, A1 = fb.y, c2 = fb.z;
+            const float half_w = (A1 + 1.0f) * 0.5f;
+            const float l_max = fminf(1.0f, A1);
+            const int mc_first = (int)rintf(fmaf((float)s0, A1, A0));
+            const int mc_last = (int)rintf(fmaf((float)(s0 + ns - 1), A1, A0));
+            const int m_lo = min(mc_first, mc_last) - 1;
+            const int m_hi = max(mc_first, mc_last) + 1;
+            if (m_hi - m_lo + 1 > BPF_CACHE_ROWS) {  // excluded by plan_bp_fast; never read past the cache
+                flag_error(err, MBX_ERRFLAG_CACHE);
+                return;
+            }
+            for (int m = m_lo; m <= m_hi; ++m) {
+                float c = 0.0f;
+                if (m >= 0 && m < num_rows) {
+                    const int o = voff + m * num_channels + first;
+                    const float *q = sino + o;
+                    if (wts) {
+                        const float *qw = wts + o;
+                        c = fmaf(fa.y, __ldg(q) * __ldg(qw), fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fa.w * (__ldg(q + 2) * __ldg(qw + 2))));
+                    } else {
+                        c = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fa.w * __ldg(q + 2)));
                     }
                 }
+                mycache[(m - m_lo) * BPF_THREADS] = c;
+            }
+#pragma unroll
+            for (int s = 0; s < BPF_ST; ++s) {
+                if (s < ns) {
+                    const float k = (float)(s0 + s);
+                    const float m_p = fmaf(k, A1, A0);
+                    const int m_c = (int)rintf(m_p);
+                    const float d = m_p - (float)m_c;
+                    const float z = fmaf(k, g.delta_voxel, z0);
+                    const float q = fmaf(c2, z * z, 1.0f);
+                    float sec = q * rsqrtf(q);                       // 1 / cos(phi_k)
+                    const float l_m = fminf(fmaxf(half_w - fabsf(d + 1.0f), 0.0f), l_max);
+                    const float l_0 = fminf(fmaxf(half_w - fabsf(d), 0.0f), l_max);
+                    const float l_p = fminf(fmaxf(half_w - fabsf(d - 1.0f), 0.0f), l_max);
+                    const float *cc = mycache + (m_c - m_lo) * BPF_THREADS;
+                    const float cm = cc[-BPF_THREADS], c0 = cc[0], cp = cc[BPF_THREADS];
+                    if (coeff_power == 2) {
+                        sec *= sec;
+                        acc[s] = fmaf(sec, fmaf(l_m * l_m, cm, fmaf(l_0 * l_0, c0, (l_p * l_p) * cp)), acc[s]);
+                    } else {
+                        acc[s] = fmaf(sec, fmaf(l_m, cm, fmaf(l_0, c0, l_p * cp)), acc[s]);
+                    }
+                }
+            }
+        }
+    };
+
+    // per-view table of a chunk of views: angle cos/sin and element offset (-1: invalid view)
+    auto fill_views = [&](int vb, int nv) {
+        for (int t = tid; t < nv; t += BPF_THREADS) {
+            const int vi = views ? views[vb + t] : vb + t;
+            const bool ok = vi >= 0 && vi < g.num_views;
+            if (!ok && bx == 0 && by == 0) flag_error(err, MBX_ERRFLAG_VIEW);
+            const float ang = ok ? g.angles[vi] : 0.0f;
+            s_voff[t] = ok ? vi * view_stride : -1;
+            s_cs[t] = cosf(ang);
+            s_sn[t] = sinf(ang);
+        }
+    };
+
+    if (P.inline_fp) {
+        for (int vb = v_begin; vb < v_end; vb += vc) {
+            const int nv = min(vc, v_end - vb);
+            __syncthreads();
+            fill_views(vb, nv);
+            __syncthreads();
+            if (!active) continue;
+            for (int t = 0; t < nv; ++t) {
+                const int voff = s_voff[t];
+                if (voff < 0) continue;
+                float4 fa, fb;
+                bpf_footprint<KIND>(g, s_cs[t], s_sn[t], oxt, oyt, coeff_power, fa, fb);
+                if (__float_as_int(fa.x) >= 0) gather(fa, fb, voff);
+            }
+        }
+    } else {
+        for (int vb = v_begin; vb < v_end; vb += vc) {
+            const int nv = min(vc, v_end - vb);
+            __syncthreads();
+            fill_views(vb, nv);
+            __syncthreads();
+            for (int f = tid; f < chunk; f += BPF_THREADS) {
+                const int t = f >> lg_pcta;
+                if (t < nv) {
+                    float4 fa = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f), fb = make_float4(0.f, 0.f, 0.f, 0.f);
+                    if (fvalid && s_voff[t] >= 0) bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb);
+                    s_fa[f] = fa;
+                    if (KIND == MBX_GEOM_CONE) s_fb[f] = fb;
+                }
+            }
+            __syncthreads();
+            if (!active) continue;
+            for (int t = 0; t < nv; ++t) {
+                const int f = (t << lg_pcta) + pl;
+                const float4 fa = s_fa[f];
+                if (__float_as_int(fa.x) < 0) continue;
+                gather(fa, KIND == MBX_GEOM_CONE ? s_fb[f] : make_float4(0.f, 0.f, 0.f, 0.f), s_voff[t]);
             }
         }
     }
@@ -323,8 +352,10 @@ __global__ void __launch_bounds__(BPF_THREADS, 3) bp_fast_kernel(const BpArgs A,
     bp_fast_tile<KIND>(A, blockIdx.x, blockIdx.y, blockIdx.z, smf, err);
 }
 
-inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_views_sel) {
+// inline_fp: 1 for the variant that computes footprints per thread in registers (see BpfPlan::inline_fp).
+inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_views_sel, int inline_fp = 0) {
     BpfPlan pl;
+    pl.inline_fp = inline_fp;
     // 32-bit element offsets address the sinogram
     pl.ok = (g.psf_radius == 1) && g.num_det_channels >= 3 &&
             (long long)g.num_views * g.num_det_rows * g.num_det_channels < (1LL << 31);
@@ -349,6 +380,10 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
     pl.chunk = (g.kind == MBX_GEOM_CONE) ? MBX_BPF_CHUNK_CONE : MBX_BPF_CHUNK_PARALLEL;
     if (pl.chunk < pcta) pl.chunk = pcta;
     pl.vc = pl.chunk / pcta;
+    if (inline_fp) {  // no staged footprints; a view table of up to 1024 views per refill
+        pl.chunk = 0;
+        pl.vc = 1024;
+    }
     pl.gx = ceil_div(num_pixels > 0 ? num_pixels : 1, pcta);
     pl.gy = ceil_div(pl.tiles, pl.nsl);
     if (g.kind == MBX_GEOM_CONE) {

@@ -31,11 +31,16 @@ int *device_error_ptr() {
     return cache[dev];
 }
 
-static std::atomic<bool> g_autotune{true};
+static std::atomic<int> g_autotune{1};
 static std::mutex g_tune_mutex;
 static std::map<std::vector<long long>, int> g_tune_cache;
 
-bool autotune_enabled() { return g_autotune.load(std::memory_order_relaxed); }
+bool autotune_enabled() { return g_autotune.load(std::memory_order_relaxed) != 0; }
+
+int autotune_forced() {
+    const int m = g_autotune.load(std::memory_order_relaxed);
+    return m >= 2 ? m - 1 : -1;
+}
 
 int autotune_lookup(const long long *key, int n) {
     int dev = 0;
@@ -140,7 +145,10 @@ extern "C" int mbx_last_cuda_error(void) { return mbx::t_last_cuda_error; }
 
 extern "C" uint64_t mbx_launch_count(void) { return mbx::g_launches.load(std::memory_order_relaxed); }
 
-extern "C" int mbx_set_autotune(int enable) { return mbx::g_autotune.exchange(enable != 0) ? 1 : 0; }
+extern "C" int mbx_set_autotune(int mode) {
+    if (mode < 0) return MBX_ERR_INVALID_ARG;
+    return mbx::g_autotune.exchange(mode);
+}
 
 extern "C" int mbx_get_device_error(int *flags_out) {
     if (!flags_out) return MBX_ERR_INVALID_ARG;

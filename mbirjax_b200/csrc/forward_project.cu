@@ -13,6 +13,7 @@
 // vertical fan (detector-row-centric, 2*bp_psf_radius+1 slices) for its row.  The finished tile is written
 // once, coalesced.  When there are too few (view, row-band) tiles to fill the GPU, the pixel range is split
 // over CTAs whose partial tiles are summed by split_sum_kernel in a fixed order (caller workspace).
+#include <algorithm>
 #include <climits>
 
 #include "mbx_common.cuh"
@@ -264,7 +265,9 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
         }
         // plan choice: cached per call shape, or timed now (each candidate overwrites the whole output)
         int choice = 0;
-        if (ncand > 1 && num_pixels > 0 && autotune_enabled()) {
+        if (autotune_forced() >= 0) {
+            choice = std::min(autotune_forced(), ncand - 1);
+        } else if (ncand > 1 && num_pixels > 0 && autotune_enabled()) {
             long long n2 = 1;
             while (n2 < num_pixels) n2 <<= 1;
             const long long key[10] = {1, g.kind, num_views_sel, g.num_det_rows, g.num_det_channels,

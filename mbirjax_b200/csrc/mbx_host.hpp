@@ -42,6 +42,7 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
 // of that shape launch it directly.  Calls made while their stream is being captured into a CUDA graph use the
 // default plan and do not tune.  The cache is host memory only; mbx_set_autotune(0) selects the default plans.
 bool autotune_enabled();
+int autotune_forced();  // mbx_set_autotune(k >= 2): candidate k-1 is used everywhere without timing; else -1
 int autotune_lookup(const long long *key, int n);  // -1 if the shape has not been tuned
 void autotune_store(const long long *key, int n, int choice);
 bool stream_is_capturing(cudaStream_t st);

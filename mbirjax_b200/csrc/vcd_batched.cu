@@ -469,7 +469,8 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
                                                   : occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, smem3, P.fp_total);
         return MBX_OK;
     };
-    const int cached = autotune_lookup(key.data(), (int)key.size());
+    const int cached = autotune_forced() >= 0 ? (autotune_forced() >= 1 ? 3 : 2)
+                                              : autotune_lookup(key.data(), (int)key.size());
     if (cached == 2) return MBX_OK;
     if (cached == 3) return use3();
     if (stream_is_capturing(st)) return MBX_OK;
@@ -496,6 +497,68 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
     if (t2 <= t3) {  // back to the tables as built
         P = keep;
         e = cudaMemcpyAsync(base + L.fpargs, hf2, sizeof(FpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return set_cuda_error(e);
+    }
+    return MBX_OK;
+}
+
+// Autotuning of the back-projection stage: staged (shared-memory) footprints, the tables as built, against
+// per-thread footprints computed in registers (same tiles and work list).  Timed on step 0 (the stage only
+// writes the scans' back-projection scratch) and cached per batch shape like the forward stage.
+static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, int num_scans,
+                           const BpArgs *hb1, cudaStream_t st) {
+    int ksum = 0;
+    for (int s = 0; s < num_scans; ++s) ksum += scans[s].num_subsets;
+    std::vector<BpArgs> b2(hb1, hb1 + ksum);
+    size_t smem2 = 0;
+    for (int k = 0; k < ksum; ++k) {
+        const BpfPlan q = plan_bp_fast(b2[k].g, b2[k].num_pixels, b2[k].g.num_views, 1);
+        if (!q.ok || q.gx != b2[k].plan.gx || q.gy != b2[k].plan.gy || q.splits != 1) return MBX_OK;
+        b2[k].plan = q;
+        smem2 = std::max(smem2, q.smem);
+    }
+    char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
+    std::vector<long long> key = {4, P.kind, num_scans};
+    for (int s = 0; s < num_scans; ++s) {
+        const mbx_geom &g = scans[s].geom;
+        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
+                               g.num_recon_slices, scans[s].num_subsets, scans[s].subset_size,
+                               scans[s].weights ? 1 : 0});
+    }
+    auto use_inline = [&]() -> int {
+        cudaError_t e = cudaMemcpyAsync(base + L.bpargs, b2.data(), sizeof(BpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        P.bp_smem = smem2;
+        P.bp_grid = (P.kind == MBX_GEOM_PARALLEL) ? occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, smem2, P.bp_total)
+                                                  : occupancy_grid(b_bp<MBX_GEOM_CONE>, smem2, P.bp_total);
+        return MBX_OK;
+    };
+    const int cached = autotune_forced() >= 0 ? (autotune_forced() >= 1 ? 1 : 0)
+                                              : autotune_lookup(key.data(), (int)key.size());
+    if (cached == 0) return MBX_OK;
+    if (cached == 1) return use_inline();
+    if (stream_is_capturing(st)) return MBX_OK;
+    int rc = MBX_OK;
+    auto run = [&]() {
+        rc = launch_stage(&P, 0, 0, st);
+        return rc == MBX_OK ? cudaSuccess : cudaErrorLaunchFailure;
+    };
+    float t0 = 0.0f, t1 = 0.0f;
+    cudaError_t e = time_on_stream(run, st, t0);
+    if (rc != MBX_OK) return rc;
+    if (e != cudaSuccess) return set_cuda_error(e);
+    const BatchedPlanHost keep = P;
+    rc = use_inline();
+    if (rc != MBX_OK) return rc;
+    e = time_on_stream(run, st, t1);
+    if (rc != MBX_OK) return rc;
+    if (e != cudaSuccess) return set_cuda_error(e);
+    autotune_store(key.data(), (int)key.size(), t0 <= t1 ? 0 : 1);
+    if (t0 <= t1) {
+        P = keep;
+        e = cudaMemcpyAsync(base + L.bpargs, hb1, sizeof(BpArgs) * ksum, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return set_cuda_error(e);
     }
@@ -705,8 +768,9 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     P.rc_grid = occupancy_grid(b_iter_partials, 0, L.sn_total + L.rc_total);
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e);
-    if (autotune_enabled()) {
-        const int rc2 = tune_batched_fp(P, L, zs, scans, num_scans, hf, st);
+    if (autotune_enabled()) {  // (also in forced mode: the tune functions then apply the forced choice)
+        int rc2 = tune_batched_fp(P, L, zs, scans, num_scans, hf, st);
+        if (rc2 == MBX_OK) rc2 = tune_batched_bp(P, L, scans, num_scans, hb, st);
         if (rc2 != MBX_OK) return rc2;
     }
     P.magic = BT_MAGIC;

@@ -72,3 +72,21 @@ def test_morton_order_is_a_permutation():
     idx = np.sort(np.random.default_rng(0).choice(64 * 64, 500, replace=False)).astype(np.int32)
     o = morton_order(idx, 64)
     assert sorted(o.tolist()) == list(range(500))
+
+
+def test_batched_alternative_plans_match_default(cuda):
+    """The batched stages with the alternative projector plans the autotuner can choose (forced) give the same
+    reconstruction as with the default plans."""
+    from mbirjax_b200 import _capi
+    shapes, seeds = [(30, 6, 40), (26, 20, 48)], [7, 8]
+    out = {}
+    for mode in (0, 2):
+        old = _capi.set_autotune(mode)
+        try:
+            items = [_scan('parallel', v, r, c, sd) for (v, r, c), sd in zip(shapes, seeds)]
+            recons, _ = BatchedVCD([it[0] for it in items], [it[2] for it in items], seeds=seeds).recon(max_iterations=3)
+            out[mode] = [x.cpu().numpy() for x in recons]
+        finally:
+            _capi.set_autotune(old)
+    for a, b in zip(out[0], out[2]):
+        assert rel_l2(b, a) <= 1e-5
