@@ -100,10 +100,8 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
                 choice = 0;
                 if (!stream_is_capturing(st)) {
                     float t[2] = {0.0f, 0.0f};
-                    for (int c = 0; c < 2; ++c) {
-                        const cudaError_t e = time_on_stream([&]() { return run(cand[c]); }, st, t[c]);
-                        if (e != cudaSuccess) return set_cuda_error(e);
-                    }
+                    const cudaError_t e = time_candidates(2, [&](int c) { return run(cand[c]); }, st, t);
+                    if (e != cudaSuccess) return set_cuda_error(e);
                     choice = t[1] < t[0] ? 1 : 0;
                     autotune_store(key, 11, choice);
                 }

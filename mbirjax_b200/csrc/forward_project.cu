@@ -239,7 +239,7 @@ static cudaError_t launch_fp_cb(const FpArgs &A, cudaStream_t st) {
 int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, long long num_pixels,
                     const int32_t *views, int num_views_sel, float *out, void *ws, size_t ws_bytes,
                     cudaStream_t st) {
-    CbPlan cand[3];
+    CbPlan cand[CB_MAX_CANDIDATES];
     const int ncand = fp_cb_candidates(g, num_views_sel, 4LL * num_sms(), cand);
     if (ncand > 0 && num_pixels * g.num_recon_slices < (1LL << 31)) {  // 32-bit cylinder offsets
         FpArgs A;
@@ -276,17 +276,12 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
             if (choice < 0 || choice >= ncand) {
                 choice = 0;
                 if (!stream_is_capturing(st)) {
-                    float best = 3.0e38f;
-                    for (int c = 0; c < ncand; ++c) {
-                        A.plan = cand[c];
-                        float ms = 0.0f;
-                        cudaError_t e = time_on_stream([&]() { return launch_fp_cb(A, st); }, st, ms);
-                        if (e != cudaSuccess) return set_cuda_error(e);
-                        if (ms < best) {
-                            best = ms;
-                            choice = c;
-                        }
-                    }
+                    float t[CB_MAX_CANDIDATES];
+                    const cudaError_t e = time_candidates(
+                        ncand, [&](int c) { A.plan = cand[c]; return launch_fp_cb(A, st); }, st, t);
+                    if (e != cudaSuccess) return set_cuda_error(e);
+                    for (int c = 1; c < ncand; ++c)
+                        if (t[c] < t[choice]) choice = c;
                     autotune_store(key, 10, choice);
                 }
             }

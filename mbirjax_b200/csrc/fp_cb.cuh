@@ -11,9 +11,9 @@
 //     __match_any_sync), during which the kept pixels' footprints are computed and stored as sorted records
 //     {cylinder offset, three channel coefficients} plus the bin.
 //  3. Accumulate: the bins are split into 8 contiguous ranges of about equal record counts, one per warp (at
-//     least two bins each).  A warp's lanes form ppw sub-groups of 32/ppw lanes; each sub-group walks an
-//     equal contiguous share of the warp's records, and each lane carries rpl detector rows (contiguous
-//     voxel-cylinder reads, rows rl apart).  The walk is flat and software-pipelined (8 loads in flight per
+//     least two bins each).  A warp's lanes form ppw sub-groups of 32/ppw lanes; sub-group k walks records
+//     k, k + ppw, ... of the warp's range (so the sub-groups stay in step), and each lane carries rpl detector
+//     rows (contiguous voxel-cylinder reads, rows rl apart).  The walk is flat and software-pipelined (8 loads in flight per
 //     lane); because the records are sorted by centre channel, a lane keeps three running channel sums per
 //     row in registers and, when the bin changes, channel bin-2 is done and is added once to the sub-group's
 //     private tile copy.  Channels at the ends of a warp's range also receive taps from the neighbouring
@@ -92,17 +92,20 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
 // num_views_sel: views per call (0 = all); min_blocks: CTAs wanted per call (a narrower channel block is
 // chosen to reach it); 0 = widest block.  minb: 2 (first shared-memory tier 112 KB) or 3 (74 KB, for the kernel
 // variant compiled for three resident CTAs per SM); nb_max: widest channel block allowed.
+// avoid_ppw: when nonzero, the best lane layout with a different number of sub-groups (an autotuner candidate).
 inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min_blocks = 0, int minb = 2,
-                         int nb_max = 128) {
+                         int nb_max = 128, int avoid_ppw = 0) {
     CbPlan pl = {};
     pl.minb = minb;
     pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || g.bp_psf_radius == 1);
     const int R = g.num_det_rows, C = g.num_det_channels;
     // lane layout: padded rows weighted by the cost of ppw diverging sub-groups, plus a small cost per pass
-    static const int combos[10][2] = {{1, 1}, {1, 2}, {1, 3}, {1, 4}, {2, 1}, {2, 2}, {2, 3}, {2, 4}, {4, 1}, {4, 2}};
+    static const int combos[12][2] = {{1, 1}, {1, 2}, {1, 3}, {1, 4}, {2, 1}, {2, 2},
+                                      {2, 3}, {2, 4}, {4, 1}, {4, 2}, {4, 3}, {4, 4}};
     double best = 1e300;
     for (const auto &cb : combos) {
         const int ppw = cb[0], rpl = cb[1], rows = (32 / ppw) * rpl;
+        if (ppw == avoid_ppw) continue;
         const int passes = ceil_div(R, rows);
         const double f = ppw == 1 ? 1.0 : (ppw == 2 ? 1.15 : 1.35);
         const double cost = (double)passes * rows * f + 2.0 * passes;
@@ -150,8 +153,11 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
 }
 
 // The plans an autotuner times for one call shape: the default, the variant compiled for three resident CTAs
-// per SM (smaller passes), and narrower channel blocks (more CTAs, shorter bins).  Returns how many are usable.
-inline int fp_cb_candidates(const mbx_geom &g, int num_views_sel, long long min_blocks, CbPlan out[3]) {
+// per SM (smaller passes), narrower channel blocks (more CTAs, shorter bins), and the best lane layout with a
+// different number of sub-groups per warp.  Returns how many are usable.
+constexpr int CB_MAX_CANDIDATES = 4;
+inline int fp_cb_candidates(const mbx_geom &g, int num_views_sel, long long min_blocks,
+                            CbPlan out[CB_MAX_CANDIDATES]) {
     int n = 0;
     const CbPlan c0 = plan_fp_cb(g, num_views_sel, min_blocks, 2, 128);
     if (!c0.ok) return 0;
@@ -162,6 +168,8 @@ inline int fp_cb_candidates(const mbx_geom &g, int num_views_sel, long long min_
         const CbPlan c2 = plan_fp_cb(g, num_views_sel, min_blocks, 2, c0.nb / 2);
         if (c2.ok) out[n++] = c2;
     }
+    const CbPlan c3 = plan_fp_cb(g, num_views_sel, min_blocks, 2, 128, c0.ppw);
+    if (c3.ok) out[n++] = c3;
     return n;
 }
 
@@ -368,10 +376,9 @@ __device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, 
     constexpr int U = (CB_LOADS / RPL) > 0 ? (CB_LOADS / RPL) : 1;  // records prefetched per lane
     const int sub = lane / RL, lr = lane % RL;
     const int num_rows = g.num_det_rows, num_slices = g.num_recon_slices, nb = pl.nb;
-    // this sub-group's share of the warp's records
+    // this sub-group's records: every PPW-th of the warp's range, so the sub-groups walk the same bins in step
     const int w_lo = P.bstart[P.b_lo], w_hi = P.bstart[P.b_hi];
-    const int r_a = w_lo + (int)(((long long)(w_hi - w_lo) * sub) / PPW);
-    const int r_b = w_lo + (int)(((long long)(w_hi - w_lo) * (sub + 1)) / PPW);
+    const int r_a = w_lo + sub, r_b = w_hi;
     // edge channels of the warp's range: E0, E1 (shared with the warp below), E2, E3 (with the warp above)
     const int E0 = P.b_lo - 2, E1 = P.b_lo - 1, E2 = P.b_hi - 2, E3 = P.b_hi - 1;
     for (int rp = 0; rp < pl.row_passes; ++rp) {
@@ -420,13 +427,13 @@ __device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, 
             }
             ++bc;
         };
-        for (int i = r_a; i < r_b; i += U) {
+        for (int i = r_a; i < r_b; i += U * PPW) {
             float4 rq[U];
             int bq[U];
             float vq[U][RPL];
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                const int ii = min(i + u, r_b - 1);  // past the end: reread the last record, contribute nothing
+                const int ii = min(i + u * PPW, r_b - 1);  // past the end: reread the last record, contribute nothing
                 rq[u] = P.rec[ii];
                 bq[u] = P.sbin[ii];
                 float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
@@ -438,7 +445,7 @@ __device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, 
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (i + u < r_b) {
+                if (i + u * PPW < r_b) {
                     while (bc < bq[u]) finish();
 #pragma unroll
                     for (int j = 0; j < RPL; ++j) {
@@ -726,7 +733,9 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             case 19: cb_accumulate<KIND, 2, 3>(A, P, warp, lane, kconst); break;
             case 20: cb_accumulate<KIND, 2, 4>(A, P, warp, lane, kconst); break;
             case 33: cb_accumulate<KIND, 4, 1>(A, P, warp, lane, kconst); break;
-            default: cb_accumulate<KIND, 4, 2>(A, P, warp, lane, kconst); break;
+            case 34: cb_accumulate<KIND, 4, 2>(A, P, warp, lane, kconst); break;
+            case 35: cb_accumulate<KIND, 4, 3>(A, P, warp, lane, kconst); break;
+            default: cb_accumulate<KIND, 4, 4>(A, P, warp, lane, kconst); break;
         }
     }
     __syncthreads();

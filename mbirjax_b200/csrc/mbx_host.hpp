@@ -72,6 +72,35 @@ cudaError_t time_on_stream(F launch, cudaStream_t st, float &ms) {
     return e;
 }
 
+// Best-of-three milliseconds of each of n candidates on st: every candidate runs once untimed first, then the
+// timed runs go round-robin, so clock ramp-up and cache state do not favour one candidate.
+template <class F>
+cudaError_t time_candidates(int n, F launch, cudaStream_t st, float *ms) {
+    cudaError_t e = cudaSuccess;
+    for (int c = 0; c < n && e == cudaSuccess; ++c) e = launch(c);
+    if (e != cudaSuccess) return e;
+    cudaEvent_t a, b;
+    if ((e = cudaEventCreate(&a)) != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return e;
+    }
+    for (int c = 0; c < n; ++c) ms[c] = 3.0e38f;
+    for (int r = 0; r < 3 && e == cudaSuccess; ++r)
+        for (int c = 0; c < n && e == cudaSuccess; ++c) {
+            e = cudaEventRecord(a, st);
+            if (e == cudaSuccess) e = launch(c);
+            if (e == cudaSuccess) e = cudaEventRecord(b, st);
+            if (e == cudaSuccess) e = cudaEventSynchronize(b);
+            float t = 0.0f;
+            if (e == cudaSuccess) e = cudaEventElapsedTime(&t, a, b);
+            if (e == cudaSuccess && t < ms[c]) ms[c] = t;
+        }
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return e;
+}
+
 // Bytes rounded up to a 256-byte boundary (workspace carving).
 inline size_t align256(size_t b) { return (b + 255) & ~(size_t)255; }
 
