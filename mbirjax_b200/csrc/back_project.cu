@@ -99,8 +99,15 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
             if (choice < 0 || choice > 1) {
                 choice = 0;
                 if (!stream_is_capturing(st)) {
+                    float t0 = 0.0f;  // the default first: a long call is not tuned (its output is complete)
+                    cudaError_t e = time_once([&]() { return run(cand[0]); }, st, t0);
+                    if (e != cudaSuccess) return set_cuda_error(e);
+                    if (t0 > MBX_TUNE_BUDGET_MS) {
+                        autotune_store(key, 11, 0);
+                        return MBX_OK;
+                    }
                     float t[2] = {0.0f, 0.0f};
-                    const cudaError_t e = time_candidates(2, [&](int c) { return run(cand[c]); }, st, t);
+                    e = time_candidates(2, [&](int c) { return run(cand[c]); }, st, t);
                     if (e != cudaSuccess) return set_cuda_error(e);
                     choice = t[1] < t[0] ? 1 : 0;
                     autotune_store(key, 11, choice);

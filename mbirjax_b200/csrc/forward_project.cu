@@ -276,8 +276,17 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
             if (choice < 0 || choice >= ncand) {
                 choice = 0;
                 if (!stream_is_capturing(st)) {
+                    // the default first, timed once: a long call is not tuned, and its output is already complete
+                    A.plan = cand[0];
+                    float t0 = 0.0f;
+                    cudaError_t e = time_once([&]() { return launch_fp_cb(A, st); }, st, t0);
+                    if (e != cudaSuccess) return set_cuda_error(e);
+                    if (t0 > MBX_TUNE_BUDGET_MS) {
+                        autotune_store(key, 10, 0);
+                        return MBX_OK;
+                    }
                     float t[CB_MAX_CANDIDATES];
-                    const cudaError_t e = time_candidates(
+                    e = time_candidates(
                         ncand, [&](int c) { A.plan = cand[c]; return launch_fp_cb(A, st); }, st, t);
                     if (e != cudaSuccess) return set_cuda_error(e);
                     for (int c = 1; c < ncand; ++c)

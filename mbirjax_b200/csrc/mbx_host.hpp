@@ -72,6 +72,30 @@ cudaError_t time_on_stream(F launch, cudaStream_t st, float &ms) {
     return e;
 }
 
+// A call whose default plan alone takes longer than this is not tuned: timing its other candidates would cost
+// more than a handful of calls could win back.
+constexpr float MBX_TUNE_BUDGET_MS = 100.0f;
+
+// Milliseconds of one run of `launch` on st (synchronises st).
+template <class F>
+cudaError_t time_once(F launch, cudaStream_t st, float &ms) {
+    cudaEvent_t a, b;
+    cudaError_t e = cudaEventCreate(&a);
+    if (e != cudaSuccess) return e;
+    if ((e = cudaEventCreate(&b)) != cudaSuccess) {
+        cudaEventDestroy(a);
+        return e;
+    }
+    e = cudaEventRecord(a, st);
+    if (e == cudaSuccess) e = launch();
+    if (e == cudaSuccess) e = cudaEventRecord(b, st);
+    if (e == cudaSuccess) e = cudaEventSynchronize(b);
+    if (e == cudaSuccess) e = cudaEventElapsedTime(&ms, a, b);
+    cudaEventDestroy(a);
+    cudaEventDestroy(b);
+    return e;
+}
+
 // Best-of-three milliseconds of each of n candidates on st: every candidate runs once untimed first, then the
 // timed runs go round-robin, so clock ramp-up and cache state do not favour one candidate.
 template <class F>
