@@ -192,6 +192,19 @@ MBX_API int mbx_vcd_subset_step(const mbx_geom *g, float *flat_recon, float *err
                         float fm_constant, const mbx_qggmrf_params *qp, double *stats_out, void *workspace,
                         size_t workspace_bytes, void *stream);
 
+/* mbx_vcd_subset_step with the two options of the reference's subset updater:
+ *   prox_input (flat like flat_recon, or NULL): proximal-map prior instead of qGGMRF, g_prior = (x - v) /
+ *     sigma_prox^2 and h_prior = sigma_prox^2 as the reference writes it (tomography_model.py:1388-1391,
+ *     prox_gradient_at_indices qggmrf.py:8-28); qp is then unused;
+ *   positivity != 0: after alpha is found, delta = max(-x / (alpha + eps), delta) at the subset and the clipped
+ *     delta is forward-projected again before the updates (tomography_model.py:1497-1507).
+ * Workspace as mbx_vcd_subset_step_workspace_bytes. */
+MBX_API int mbx_vcd_subset_step_ex(const mbx_geom *g, float *flat_recon, float *error_sinogram, const float *weights,
+                           const float *fm_hessian, const int32_t *pixel_indices, int64_t num_pixels,
+                           float fm_constant, const mbx_qggmrf_params *qp, const float *prox_input,
+                           float sigma_prox, int32_t positivity, double *stats_out, void *workspace,
+                           size_t workspace_bytes, void *stream);
+
 /* ---- batched VCD over many scans ------------------------------------------------------------- */
 
 /* One scan of a batch: its geometry, device buffers and VCD parameters (the state the reference keeps per

@@ -75,6 +75,9 @@ _SIGNATURES = {
     'mbx_vcd_subset_step': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p, c_void_p, c_void_p,
                                            c_int64, c_float, ctypes.POINTER(MbxQggmrfParams), c_void_p, c_void_p,
                                            c_size_t, c_void_p]),
+    'mbx_vcd_subset_step_ex': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p, c_void_p,
+                                              c_void_p, c_int64, c_float, ctypes.POINTER(MbxQggmrfParams), c_void_p,
+                                              c_float, c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),
     'mbx_vcd_batched_workspace_bytes': (c_size_t, [ctypes.POINTER(MbxScan), c_int32, c_int32]),
     'mbx_vcd_batched_prepare': (ctypes.c_int, [ctypes.POINTER(MbxScan), c_int32, c_void_p, c_int32, c_int32,
                                                c_void_p, c_void_p, c_void_p, c_size_t,
@@ -262,18 +265,26 @@ def vcd_subset_step_workspace(geom, num_pixels, device):
 
 
 def vcd_subset_step(geom, flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, fm_constant, qp, stats,
-                    workspace=None):
-    """One device-resident VCD subset update; stats is a device float64 tensor with >= 4 entries."""
+                    workspace=None, prox_input=None, sigma_prox=0.0, positivity=False):
+    """One device-resident VCD subset update; stats is a device float64 tensor with >= 4 entries.  prox_input
+    (flat like flat_recon) selects the proximal-map prior, positivity the clip of the reference's updater."""
     lib = load_library()
-    _require_cuda(flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, stats)
+    _require_cuda(flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, stats, prox_input)
     n = int(pixel_indices.shape[0])
     if workspace is None:
         workspace = vcd_subset_step_workspace(geom, n, flat_recon.device)
     ws, nbytes = workspace
-    rc = lib.mbx_vcd_subset_step(ctypes.byref(geom), _ptr(flat_recon), _ptr(error_sinogram), _ptr(weights),
-                                 _ptr(fm_hessian), _ptr(pixel_indices), n, float(fm_constant), ctypes.byref(qp),
-                                 _ptr(stats), _ptr(ws), nbytes, _stream())
-    _check(rc, 'mbx_vcd_subset_step')
+    if prox_input is None and not positivity:
+        rc = lib.mbx_vcd_subset_step(ctypes.byref(geom), _ptr(flat_recon), _ptr(error_sinogram), _ptr(weights),
+                                     _ptr(fm_hessian), _ptr(pixel_indices), n, float(fm_constant), ctypes.byref(qp),
+                                     _ptr(stats), _ptr(ws), nbytes, _stream())
+        _check(rc, 'mbx_vcd_subset_step')
+        return
+    rc = lib.mbx_vcd_subset_step_ex(ctypes.byref(geom), _ptr(flat_recon), _ptr(error_sinogram), _ptr(weights),
+                                    _ptr(fm_hessian), _ptr(pixel_indices), n, float(fm_constant), ctypes.byref(qp),
+                                    _ptr(prox_input), float(sigma_prox), 1 if positivity else 0, _ptr(stats),
+                                    _ptr(ws), nbytes, _stream())
+    _check(rc, 'mbx_vcd_subset_step_ex')
 
 
 def direct_filter(geom, sinogram, out=None):

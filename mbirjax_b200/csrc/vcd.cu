@@ -48,9 +48,12 @@ __device__ __forceinline__ double fixed_order_sum(const double *__restrict__ par
     return __shfl_sync(0xffffffffu, s, 0);
 }
 
+// prox (optional, flat like recon): proximal-map prior instead of qGGMRF (tomography_model.py:1388-1391):
+// g_p = (x - v) / sigma_prox^2 (qggmrf.py:8-28), h_p = sigma_prox^2 as the reference writes it.
 __global__ void vcd_delta_kernel(const float *__restrict__ recon, int nr, int nc, int ns,
                                  const int32_t *__restrict__ pix, long long num_pixels, const float *__restrict__ bp,
                                  const float *__restrict__ fm_hessian, float fm_constant, const QParams q,
+                                 const float *__restrict__ prox, float sigma_prox,
                                  float *__restrict__ delta, double *__restrict__ partials, int *err) {
     const long long total = num_pixels * ns;
     double pl = 0.0, pq = 0.0;
@@ -64,7 +67,13 @@ __global__ void vcd_delta_kernel(const float *__restrict__ recon, int nr, int nc
             flag_error(err, MBX_ERRFLAG_PIXEL);
         } else {
             float gp, hp;
-            qggmrf_voxel(recon, nr, nc, ns, idx, k, q, gp, hp);
+            if (prox) {
+                const long long v = (long long)idx * ns + k;
+                gp = (1.0f / (sigma_prox * sigma_prox)) * (recon[v] - __ldg(prox + v));
+                hp = sigma_prox * sigma_prox;
+            } else {
+                qggmrf_voxel(recon, nr, nc, ns, idx, k, q, gp, hp);
+            }
             const float gf = -fm_constant * bp[i];
             const float hf = fm_constant * __ldg(fm_hessian + (long long)idx * ns + k);
             d = -((gf + gp) / (hf + hp));
@@ -75,6 +84,23 @@ __global__ void vcd_delta_kernel(const float *__restrict__ recon, int nr, int nc
     }
     const double v[2] = {pl, pq};
     block_reduce_store_n<2>(v, partials);
+}
+
+// Positivity (tomography_model.py:1497-1507): delta = max(-x / (alpha + eps), delta) at the subset, with the
+// alpha already found; the caller then forward-projects the clipped delta again.
+__global__ void vcd_clip_kernel(const float *__restrict__ recon, int ns, const int32_t *__restrict__ pix,
+                                long long num_pixels, int npix_grid, const float *__restrict__ alpha,
+                                float *__restrict__ delta) {
+    const long long total = num_pixels * ns;
+    const float pc = 1.0f / (*alpha + EPS_F32);
+    for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
+         i += (long long)gridDim.x * blockDim.x) {
+        const long long p = i / ns;
+        const int k = (int)(i - p * ns);
+        const int idx = pix[p];
+        if (idx < 0 || idx >= npix_grid) continue;  // flagged by vcd_delta_kernel; its delta is 0
+        delta[i] = fmaxf(-pc * recon[(long long)idx * ns + k], delta[i]);
+    }
 }
 
 __global__ void vcd_linquad_kernel(const float *__restrict__ dsino, const float *__restrict__ err_sino,
@@ -211,7 +237,8 @@ static unsigned red_blocks(long long n, int max_blocks) {
 
 int vcd_subset_step(const mbx_geom &g, float *recon, float *err_sino, const float *wts, const float *fm_hessian,
                     const int32_t *pix, long long num_pixels, float fm_constant, const mbx_qggmrf_params &qp,
-                    double *stats, void *ws, size_t ws_bytes, cudaStream_t st) {
+                    const float *prox, float sigma_prox, int positivity, double *stats, void *ws, size_t ws_bytes,
+                    cudaStream_t st) {
     const VcdLayout L = vcd_layout(g, num_pixels);
     if (!ws || ws_bytes < L.total) return MBX_ERR_WORKSPACE;
     char *base = static_cast<char *>(ws);
@@ -233,7 +260,8 @@ int vcd_subset_step(const mbx_geom &g, float *recon, float *err_sino, const floa
     if (rc != MBX_OK) return rc;
     const unsigned nb1 = red_blocks(ncyl, L.max_blocks);
     vcd_delta_kernel<<<nb1, 256, 0, st>>>(recon, g.num_recon_rows, g.num_recon_cols, ns, pix, num_pixels, bp,
-                                          fm_hessian, fm_constant, make_qparams(qp), delta, prior_partials, err);
+                                          fm_hessian, fm_constant, make_qparams(qp), prox, sigma_prox, delta,
+                                          prior_partials, err);
     mbx::note_launch();
     cudaError_t e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e);
@@ -245,6 +273,16 @@ int vcd_subset_step(const mbx_geom &g, float *recon, float *err_sino, const floa
     vcd_alpha_kernel<<<1, 32, 0, st>>>(prior_partials, (int)nb1, fwd_partials, (int)nb2, (double)fm_constant, alpha,
                                        stats);
     mbx::note_launch();
+    if (positivity) {
+        vcd_clip_kernel<<<red_blocks(ncyl, L.max_blocks), 256, 0, st>>>(recon, ns, pix, num_pixels,
+                                                                       g.num_recon_rows * g.num_recon_cols, alpha,
+                                                                       delta);
+        mbx::note_launch();
+        e = cudaGetLastError();
+        if (e != cudaSuccess) return set_cuda_error(e);
+        rc = forward_project(g, delta, pix, num_pixels, nullptr, g.num_views, dsino, base + L.fpws, L.fp_bytes, st);
+        if (rc != MBX_OK) return rc;
+    }
     const unsigned nb3 = red_blocks(ncyl, L.max_blocks);
     vcd_apply_kernel<<<nb3, 256, 0, st>>>(recon, ns, pix, num_pixels, g.num_recon_rows * g.num_recon_cols, delta,
                                           alpha, l1_partials);
@@ -277,6 +315,27 @@ extern "C" int mbx_vcd_subset_step(const mbx_geom *g, float *flat_recon, float *
     if ((reinterpret_cast<uintptr_t>(error_sinogram) & 15) || (weights && (reinterpret_cast<uintptr_t>(weights) & 15)))
         return MBX_ERR_INVALID_ARG;  // float4 passes over the sinogram need 16-byte alignment
     return mbx::vcd_subset_step(*g, flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, num_pixels,
-                                fm_constant, *qp, stats_out, workspace, workspace_bytes,
+                                fm_constant, *qp, nullptr, 0.0f, 0, stats_out, workspace, workspace_bytes,
                                 static_cast<cudaStream_t>(stream));
+}
+
+extern "C" int mbx_vcd_subset_step_ex(const mbx_geom *g, float *flat_recon, float *error_sinogram,
+                                      const float *weights, const float *fm_hessian, const int32_t *pixel_indices,
+                                      int64_t num_pixels, float fm_constant, const mbx_qggmrf_params *qp,
+                                      const float *prox_input, float sigma_prox, int32_t positivity,
+                                      double *stats_out, void *workspace, size_t workspace_bytes, void *stream) {
+    int rc = mbx::validate_geom(g);
+    if (rc != MBX_OK) return rc;
+    if (!flat_recon || !error_sinogram || !fm_hessian || !pixel_indices || !qp || num_pixels <= 0)
+        return MBX_ERR_INVALID_ARG;
+    if (prox_input) {
+        if (!(sigma_prox > 0.0f)) return MBX_ERR_INVALID_ARG;
+    } else if (!(qp->sigma_x > 0.0f) || !(qp->T > 0.0f) || !(qp->p > 0.0f)) {
+        return MBX_ERR_INVALID_ARG;
+    }
+    if ((reinterpret_cast<uintptr_t>(error_sinogram) & 15) || (weights && (reinterpret_cast<uintptr_t>(weights) & 15)))
+        return MBX_ERR_INVALID_ARG;  // float4 passes over the sinogram need 16-byte alignment
+    return mbx::vcd_subset_step(*g, flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, num_pixels,
+                                fm_constant, *qp, prox_input, sigma_prox, positivity ? 1 : 0, stats_out, workspace,
+                                workspace_bytes, static_cast<cudaStream_t>(stream));
 }

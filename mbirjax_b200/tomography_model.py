@@ -285,6 +285,20 @@ class TomographyModel(ParameterHandler):
         notes = 'Reconstruction completed: {}\n\n'.format(datetime.datetime.now())
         return recon, self.get_recon_dict(recon_params, notes=notes)
 
+    def prox_map(self, prox_input, sinogram, weights=None, init_recon=None, stop_threshold_change_pct=0.2,
+                 max_iterations=3, first_iteration=0, logfile_path='./logs/recon.log', print_logs=True):
+        """Proximal map for Plug-and-Play (tomography_model.py:1660-1697): VCD with the quadratic proximal prior
+        centred on prox_input, using the model's current sigma_y and sigma_prox (no auto-regularisation).
+        Returns (recon, loss_vectors) as the reference does."""
+        recon_shape, granularity = self.get_params(['recon_shape', 'granularity'])
+        partitions = gen_set_of_pixel_partitions(recon_shape, granularity)
+        partition_sequence = gen_partition_sequence(self.get_params('partition_sequence'), max_iterations)
+        partition_sequence = partition_sequence[first_iteration:]
+        if first_iteration == 0 or self.logger is None:
+            self.setup_logger(logfile_path=logfile_path, print_logs=print_logs)
+        return self.vcd_recon(sinogram, partitions, partition_sequence, stop_threshold_change_pct, weights=weights,
+                              init_recon=init_recon, prox_input=prox_input, first_iteration=first_iteration)
+
     def get_recon_dict(self, recon_params, notes=''):
         logs = self.log_buffer.getvalue() if self.log_buffer is not None else ''
         model_params = {k: v.val for k, v in self.params.items()}
@@ -293,11 +307,17 @@ class TomographyModel(ParameterHandler):
     def vcd_recon(self, sinogram, partitions, partition_sequence, stop_threshold_change_pct, weights=None,
                   init_recon=None, prox_input=None, compute_prior_loss=False, first_iteration=0):
         """tomography_model.py:1086-1308; each subset update is one mbx_vcd_subset_step on the device."""
-        if prox_input is not None:
-            raise NotImplementedError('prox_map is not on the mbirjax_b200 hot path')
-        if self.get_params('positivity_flag'):
-            raise NotImplementedError('positivity_flag=True is not on the mbirjax_b200 hot path')
+        positivity = bool(self.get_params('positivity_flag'))
         state = self._vcd_setup(sinogram, weights, init_recon)
+        prox_flat, sigma_prox = None, 0.0
+        if prox_input is not None:  # tomography_model.py:1158-1170
+            recon_shape = self.get_params('recon_shape')
+            prox = self._dev(prox_input)
+            if tuple(prox.shape) != tuple(recon_shape):
+                raise ValueError('prox_input does not have the correct size. \nExpected {}, but got shape {} for '
+                                 'prox_input shape.'.format(recon_shape, tuple(prox.shape)))
+            prox_flat = prox.reshape((-1, recon_shape[2])).contiguous()
+            sigma_prox = float(self.get_params('sigma_prox'))
         recon_shape = self.get_params('recon_shape')
         dev = state['device']
         w, flat_recon, error_sinogram = state['weights'], state['flat_recon'], state['error_sinogram']
@@ -322,7 +342,8 @@ class TomographyModel(ParameterHandler):
                 workspaces[subset_size] = _capi.vcd_subset_step_workspace(geom, subset_size, dev)
             for j, index in enumerate(np.random.permutation(num_subsets)):
                 _capi.vcd_subset_step(geom, flat_recon, error_sinogram, w, fm_hessian, part[int(index)], fm_constant,
-                                      qp, stats[j], workspaces[subset_size])
+                                      qp, stats[j], workspaces[subset_size], prox_input=prox_flat,
+                                      sigma_prox=sigma_prox, positivity=positivity)
             st = stats[:num_subsets].cpu().numpy()
             ell1 = float(np.sum(st[:, 1]))
             alpha_values[i] = float(np.mean(st[:, 0]))

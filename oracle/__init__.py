@@ -30,4 +30,4 @@ from .partitions import (  # noqa: F401
     gen_full_indices,
 )
 from .filters import generate_direct_recon_filter, fbp_filter, fdk_filter  # noqa: F401
-from .vcd import vcd_recon, vcd_subset_update, auto_regularization  # noqa: F401
+from .vcd import vcd_recon, vcd_subset_update, auto_regularization, prox_map  # noqa: F401

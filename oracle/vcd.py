@@ -57,11 +57,21 @@ def forward_model_loss(error_sinogram, sigma_y, weights=None):
 
 
 def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, fm_constant,
-                      qggmrf_params):
-    """One subset step; returns (flat_recon, error_sinogram, ell1, alpha)."""
+                      qggmrf_params, prox_input=None, sigma_prox=None, positivity=False):
+    """One subset step; returns (flat_recon, error_sinogram, ell1, alpha).
+
+    prox_input (flat, like flat_recon): the proximal-map prior of tomography_model.py:1388-1391 instead of qGGMRF,
+    gradient (x - v) / sigma_prox^2 (qggmrf.py:8-28) and Hessian sigma_prox^2, as the reference writes it.
+    positivity: the clip of tomography_model.py:1497-1507, delta >= -x / (alpha + eps) after alpha is found, then
+    the forward projection of the clipped delta; alpha is not recomputed."""
     f32 = np.float32
-    prior_grad, prior_hess = qggmrf_gradient_and_hessian_at_indices(flat_recon, geom.recon_shape, pixel_indices,
-                                                                    qggmrf_params)
+    if prox_input is None:
+        prior_grad, prior_hess = qggmrf_gradient_and_hessian_at_indices(flat_recon, geom.recon_shape, pixel_indices,
+                                                                        qggmrf_params)
+    else:
+        prior_grad = ((1.0 / (f32(sigma_prox) ** 2.0)) *
+                      (flat_recon[pixel_indices] - prox_input[pixel_indices])).astype(f32)
+        prior_hess = f32(sigma_prox) ** 2
     wes = error_sinogram if weights is None else (weights * error_sinogram).astype(f32)
     forward_grad = (-fm_constant * P.sparse_back_project(geom, wes, pixel_indices)).astype(f32)
     forward_hess = (fm_constant * fm_hessian[pixel_indices]).astype(f32)
@@ -74,6 +84,10 @@ def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pix
     forward_quad = f32(fm_constant) * np.sum(delta_sino * delta_sino * w, dtype=f32)
     alpha = (forward_linear - prior_linear) / (forward_quad + prior_quad + EPS_F32)
     alpha = f32(np.clip(alpha, EPS_F32, 1.5))
+    if positivity:
+        pos_constant = f32(1.0) / (alpha + EPS_F32)
+        delta = np.maximum(-pos_constant * flat_recon[pixel_indices], delta).astype(f32)
+        delta_sino = P.sparse_forward_project(geom, delta, pixel_indices)
     delta = (alpha * delta).astype(f32)
     flat_recon = flat_recon.copy()
     np.add.at(flat_recon, pixel_indices, delta)
@@ -83,7 +97,8 @@ def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pix
 
 
 def vcd_recon(geom, sinogram, partitions, partition_sequence, *, sigma_y, sigma_x, p=2.0, q=1.2, T=1.0,
-              qggmrf_nbr_wts=(1.0, 1.0, 1.0), weights=None, init_recon=None, stop_threshold_change_pct=0.0):
+              qggmrf_nbr_wts=(1.0, 1.0, 1.0), weights=None, init_recon=None, stop_threshold_change_pct=0.0,
+              prox_input=None, sigma_prox=None, positivity=False):
     """Returns (recon, dict(fm_rmse, nmae_update, alpha_values))."""
     f32 = np.float32
     sinogram = np.asarray(sinogram, dtype=f32)
@@ -103,13 +118,15 @@ def vcd_recon(geom, sinogram, partitions, partition_sequence, *, sigma_y, sigma_
     b = get_b_from_nbr_wts(list(qggmrf_nbr_wts))
     qparams = (b, sigma_x, p, q, T)
     flat_recon = recon.reshape((-1, geom.recon_shape[2]))
+    prox_flat = None if prox_input is None else np.asarray(prox_input, dtype=f32).reshape((-1, geom.recon_shape[2]))
     fm_rmse, nmae, alphas = [], [], []
     for i in range(len(partition_sequence)):
         partition = partitions[partition_sequence[i]]
         ell1_sum, alpha_sum = 0.0, 0.0
         for index in np.random.permutation(partition.shape[0]):
             flat_recon, error_sinogram, ell1, a = vcd_subset_update(
-                geom, flat_recon, error_sinogram, weights, fm_hessian, partition[index], fm_constant, qparams)
+                geom, flat_recon, error_sinogram, weights, fm_hessian, partition[index], fm_constant, qparams,
+                prox_flat, sigma_prox, positivity)
             ell1_sum += ell1
             alpha_sum += a
         fm_rmse.append(forward_model_loss(error_sinogram, sigma_y, weights))
@@ -123,13 +140,24 @@ def vcd_recon(geom, sinogram, partitions, partition_sequence, *, sigma_y, sigma_
 
 def recon(geom, sinogram, *, granularity, partition_sequence, max_iterations, weights=None, init_recon=None,
           snr_db=30.0, sharpness=1.0, p=2.0, q=1.2, T=1.0, qggmrf_nbr_wts=(1.0, 1.0, 1.0),
-          stop_threshold_change_pct=0.2):
+          stop_threshold_change_pct=0.2, positivity=False):
     """tomography_model.py:966-1084 with the reference's np.random call order."""
     sigma_y, sigma_x, _ = auto_regularization(geom, sinogram, weights, snr_db, sharpness)
     partitions = gen_set_of_pixel_partitions(geom.recon_shape, granularity)
     seq = gen_partition_sequence(partition_sequence, max_iterations)
     out, stats = vcd_recon(geom, sinogram, partitions, seq, sigma_y=sigma_y, sigma_x=sigma_x, p=p, q=q, T=T,
                            qggmrf_nbr_wts=qggmrf_nbr_wts, weights=weights, init_recon=init_recon,
-                           stop_threshold_change_pct=stop_threshold_change_pct)
+                           stop_threshold_change_pct=stop_threshold_change_pct, positivity=positivity)
     stats['sigma_y'], stats['sigma_x'] = sigma_y, sigma_x
     return out, stats
+
+
+def prox_map(geom, prox_input, sinogram, *, sigma_y, sigma_x, sigma_prox, granularity, partition_sequence,
+             max_iterations, weights=None, init_recon=None, stop_threshold_change_pct=0.2, positivity=False):
+    """tomography_model.py:1660-1697: partitions for every granularity entry, the partition sequence, then
+    vcd_recon with the proximal prior (the regularisation parameters are the model's current ones)."""
+    partitions = gen_set_of_pixel_partitions(geom.recon_shape, granularity)
+    seq = gen_partition_sequence(partition_sequence, max_iterations)
+    return vcd_recon(geom, sinogram, partitions, seq, sigma_y=sigma_y, sigma_x=sigma_x, weights=weights,
+                     init_recon=init_recon, stop_threshold_change_pct=stop_threshold_change_pct,
+                     prox_input=prox_input, sigma_prox=sigma_prox, positivity=positivity)

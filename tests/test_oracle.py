@@ -128,3 +128,16 @@ def test_oracle_fbp_recovers_phantom():
     rec = O.back_project(geom, O.fbp_filter(sino, geom.delta_voxel))
     inner = (slice(18, 30), slice(16, 28))
     assert abs(float(np.mean(rec[inner])) - 1.0) < 0.1
+
+
+def test_oracle_prox_map_fixed_point():
+    """The oracle's proximal map leaves a consistent input in place (the reference's tests/test_prox.py corner
+    case, on a small volume)."""
+    ang = np.linspace(0, np.pi, 8, endpoint=False).astype(np.float32)
+    geom = O.parallel_geometry((8, 3, 16), ang)
+    x = np.random.default_rng(0).random(geom.recon_shape).astype(np.float32) * O.get_2d_ror_mask(geom.recon_shape)[:, :, None]
+    y = O.forward_project(geom, x)
+    np.random.seed(0)
+    rec, _ = O.prox_map(geom, x, y, sigma_y=1.0, sigma_x=1.0, sigma_prox=1.0, granularity=[2],
+                        partition_sequence=[0], max_iterations=2, init_recon=x, stop_threshold_change_pct=0)
+    assert np.max(np.abs(rec - x)) < 1e-5

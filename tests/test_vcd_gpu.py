@@ -96,3 +96,64 @@ def test_recon_small_parallel_config(cuda):
     # sanity floor: the iterative recon is closer to the phantom than its FBP initialisation
     fbp = model.direct_recon(sino).cpu().numpy()
     assert rel_l2(rec.cpu().numpy(), ph) < rel_l2(fbp, ph)
+
+
+def _small_parallel_case(seed=3):
+    from mbirjax_b200.utilities import gen_ellipsoid_phantom
+    ang = np.linspace(0, np.pi, 32, endpoint=False).astype(np.float32)
+    model = mb.ParallelBeamModel((32, 8, 48), ang)
+    geom = O.parallel_geometry((32, 8, 48), ang)
+    ph = gen_ellipsoid_phantom(geom.recon_shape, 4, seed).numpy()
+    sino = O.forward_project(geom, ph)
+    sino = (sino + np.random.default_rng(seed).normal(0, 0.02 * np.abs(sino).max(), sino.shape)).astype(np.float32)
+    model.set_params(sharpness=0.0, granularity=[4], partition_sequence=[0], verbose=0)
+    return model, geom, ph, sino
+
+
+def test_recon_with_positivity_matches_oracle(cuda):
+    """positivity_flag=True: the update of each subset is clipped so no voxel goes below zero, then re-projected
+    (tomography_model.py:1497-1507); same recon as the oracle's restatement."""
+    model, geom, ph, sino = _small_parallel_case()
+    model.set_params(positivity_flag=True)
+    np.random.seed(3)
+    rec, d = model.recon(sino, max_iterations=4, stop_threshold_change_pct=0, logfile_path=None, print_logs=False)
+    rec = rec.cpu().numpy()
+    np.random.seed(3)
+    ref, stats = O.vcd.recon(geom, sino, granularity=[4], partition_sequence=[0], max_iterations=4, sharpness=0.0,
+                             stop_threshold_change_pct=0, positivity=True)
+    assert rel_l2(rec, ref) <= 1e-4
+    np.testing.assert_allclose(d['recon_params']['alpha_values'], stats['alpha_values'], rtol=1e-4)
+    mask = O.get_2d_ror_mask(geom.recon_shape)[:, :, None] > 0
+    assert rec[np.broadcast_to(mask, rec.shape)].min() >= -1e-6 * np.abs(rec).max()
+
+
+def test_prox_map_matches_oracle(cuda):
+    """prox_map: VCD with the proximal prior centred on prox_input (tomography_model.py:1660-1697, prior
+    gradient (x - v) / sigma_prox^2 and Hessian sigma_prox^2) at the model's sigma_y and sigma_prox."""
+    model, geom, ph, sino = _small_parallel_case(seed=4)
+    sigma_y, sigma_x, sigma_prox = O.auto_regularization(geom, sino, None, 30.0, 0.0)
+    model.set_params(sigma_y=float(sigma_y), sigma_x=float(sigma_x), sigma_prox=float(sigma_prox))
+    prox = (ph + np.random.default_rng(9).normal(0, 0.05, ph.shape)).astype(np.float32)
+    np.random.seed(4)
+    rec, loss = model.prox_map(prox, sino, max_iterations=3, stop_threshold_change_pct=0, logfile_path=None,
+                               print_logs=False)
+    np.random.seed(4)
+    ref, stats = O.prox_map(geom, prox, sino, sigma_y=sigma_y, sigma_x=sigma_x, sigma_prox=sigma_prox,
+                            granularity=[4], partition_sequence=[0], max_iterations=3, stop_threshold_change_pct=0)
+    assert rel_l2(rec.cpu().numpy(), ref) <= 1e-4
+    np.testing.assert_allclose(np.asarray(loss[0]), stats['fm_rmse'], rtol=1e-4)
+
+
+def test_prox_map_fixed_point(cuda):
+    """The reference's proximal-map corner case (tests/test_prox.py): input, initial recon and the noiseless data
+    all agree with the phantom, so five iterations leave it in place to 1e-5."""
+    from mbirjax_b200.utilities import gen_ellipsoid_phantom
+    ang = np.linspace(0, np.pi, 32, endpoint=False).astype(np.float32)
+    model = mb.ParallelBeamModel((32, 40, 128), ang)
+    phantom = gen_ellipsoid_phantom(model.get_params('recon_shape'), 6, 0)
+    sino = model.forward_project(phantom)
+    model.set_params(verbose=0)
+    np.random.seed(0)
+    rec, _ = model.prox_map(phantom, sino, max_iterations=5, init_recon=phantom, logfile_path=None,
+                            print_logs=False)
+    assert float(torch.max(torch.abs(rec - phantom.to(rec.device)))) < 1e-5
