@@ -205,6 +205,25 @@ MBX_API int mbx_vcd_subset_step_ex(const mbx_geom *g, float *flat_recon, float *
                            float sigma_prox, int32_t positivity, double *stats_out, void *workspace,
                            size_t workspace_bytes, void *stream);
 
+/* ---- qGGMRF denoiser ---------------------------------------------------------------------------- */
+
+/* Workspace for one mbx_qggmrf_denoise_step over num_pixels cylinders of num_slices voxels. */
+MBX_API size_t mbx_qggmrf_denoise_step_workspace_bytes(int64_t num_pixels, int32_t num_slices);
+/* One subset update of the qGGMRF denoiser (identity forward model), fully on the device:
+ *   delta = -(-fm e + g_prior) / (1 + h_prior) with e = flat_error_image[idx] (noisy - current image)
+ *   alpha = clip((fm <e, delta> - <g_prior, delta>) / (fm <delta, delta> + <h_prior, delta^2>/1.1 + eps), eps, 1.5)
+ *   flat_image[idx] += alpha delta;  flat_error_image[idx] -= alpha delta
+ * Images are flat (num_rows * num_cols, num_slices); inner products in float64; stats_out (device double[4], may
+ * be NULL) receives {alpha, sum|alpha delta|, numerator, denominator}.  Replaces vcd_subset_denoiser
+ * (denoising.py:366-411). */
+MBX_API int mbx_qggmrf_denoise_step(float *flat_image, float *flat_error_image, int32_t num_rows, int32_t num_cols,
+                            int32_t num_slices, const int32_t *pixel_indices, int64_t num_pixels,
+                            float fm_constant, const mbx_qggmrf_params *qp, double *stats_out, void *workspace,
+                            size_t workspace_bytes, void *stream);
+/* 3x3x3 median filter with edge replication of a (d0, d1, d2) float32 volume into out (not in place).
+ * Replaces median_filter3d (denoising.py:414-490). */
+MBX_API int mbx_median_filter3d(const float *x, int32_t d0, int32_t d1, int32_t d2, float *out, void *stream);
+
 /* ---- batched VCD over many scans ------------------------------------------------------------- */
 
 /* One scan of a batch: its geometry, device buffers and VCD parameters (the state the reference keeps per

@@ -4,7 +4,8 @@ Public API mirrors the reference: ``ParallelBeamModel``, ``ConeBeamModel`` (both
 ``set_params``, ``forward_project``, ``back_project``, ``sparse_forward_project``, ``sparse_back_project``,
 ``compute_hessian_diagonal``, ``recon``, ``direct_recon``), the pixel-partition utilities and the qGGMRF
 prior.  ``mbirjax_b200.autograd`` wraps the projector pair as torch autograd functions and
-``mbirjax_b200.batched`` reconstructs many scans of uneven geometry together.
+``mbirjax_b200.batched`` reconstructs many scans of uneven geometry together.  ``QGGMRFDenoiser`` and
+``median_filter3d`` are the reference's denoising tools.
 
 All compute runs in the CUDA library ``mbirjax_b200/_lib/libmbirjax_b200.so`` (C ABI:
 ``include/mbirjax_b200.h``), built by ``mbirjax_b200.build()``.
@@ -16,6 +17,7 @@ from .parameter_handler import ParameterHandler, Param
 from .tomography_model import TomographyModel
 from .parallel_beam import ParallelBeamModel
 from .cone_beam import ConeBeamModel
+from .denoising import QGGMRFDenoiser, median_filter3d
 from .vcd_utils import (get_2d_ror_mask, gen_pixel_partition, gen_set_of_pixel_partitions, gen_partition_sequence,
                         gen_full_indices)
 from .qggmrf import get_b_from_nbr_wts, qggmrf_gradient_and_hessian_at_indices, qggmrf_loss, qggmrf_loss_and_grad

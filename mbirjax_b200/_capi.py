@@ -78,6 +78,11 @@ _SIGNATURES = {
     'mbx_vcd_subset_step_ex': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p, c_void_p,
                                               c_void_p, c_int64, c_float, ctypes.POINTER(MbxQggmrfParams), c_void_p,
                                               c_float, c_int32, c_void_p, c_void_p, c_size_t, c_void_p]),
+    'mbx_qggmrf_denoise_step_workspace_bytes': (c_size_t, [c_int64, c_int32]),
+    'mbx_qggmrf_denoise_step': (ctypes.c_int, [c_void_p, c_void_p, c_int32, c_int32, c_int32, c_void_p, c_int64,
+                                               c_float, ctypes.POINTER(MbxQggmrfParams), c_void_p, c_void_p,
+                                               c_size_t, c_void_p]),
+    'mbx_median_filter3d': (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
     'mbx_vcd_batched_workspace_bytes': (c_size_t, [ctypes.POINTER(MbxScan), c_int32, c_int32]),
     'mbx_vcd_batched_prepare': (ctypes.c_int, [ctypes.POINTER(MbxScan), c_int32, c_void_p, c_int32, c_int32,
                                                c_void_p, c_void_p, c_void_p, c_size_t,
@@ -285,6 +290,34 @@ def vcd_subset_step(geom, flat_recon, error_sinogram, weights, fm_hessian, pixel
                                     _ptr(prox_input), float(sigma_prox), 1 if positivity else 0, _ptr(stats),
                                     _ptr(ws), nbytes, _stream())
     _check(rc, 'mbx_vcd_subset_step_ex')
+
+
+def qggmrf_denoise_step(flat_image, flat_error_image, image_shape, pixel_indices, fm_constant, qp, stats,
+                        workspace=None):
+    """One subset update of the qGGMRF denoiser on flat (Nr*Nc, S) device images."""
+    lib = load_library()
+    _require_cuda(flat_image, flat_error_image, pixel_indices, stats)
+    nr, nc, ns = (int(v) for v in image_shape)
+    n = int(pixel_indices.shape[0])
+    if workspace is None:
+        workspace = _workspace(lib.mbx_qggmrf_denoise_step_workspace_bytes(n, ns), flat_image.device)
+    ws, nbytes = workspace
+    rc = lib.mbx_qggmrf_denoise_step(_ptr(flat_image), _ptr(flat_error_image), nr, nc, ns, _ptr(pixel_indices), n,
+                                     float(fm_constant), ctypes.byref(qp), _ptr(stats), _ptr(ws), nbytes, _stream())
+    _check(rc, 'mbx_qggmrf_denoise_step')
+
+
+def median_filter3d(x, out=None):
+    """3x3x3 median with edge replication of a float32 (d0, d1, d2) device volume."""
+    lib = load_library()
+    _require_cuda(x)
+    if x.dim() != 3:
+        raise ValueError('median_filter3d needs a 3-D array')
+    if out is None:
+        out = torch.empty_like(x)
+    rc = lib.mbx_median_filter3d(_ptr(x), *(int(v) for v in x.shape), _ptr(out), _stream())
+    _check(rc, 'mbx_median_filter3d')
+    return out
 
 
 def direct_filter(geom, sinogram, out=None):

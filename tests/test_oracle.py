@@ -141,3 +141,22 @@ def test_oracle_prox_map_fixed_point():
     rec, _ = O.prox_map(geom, x, y, sigma_y=1.0, sigma_x=1.0, sigma_prox=1.0, granularity=[2],
                         partition_sequence=[0], max_iterations=2, init_recon=x, stop_threshold_change_pct=0)
     assert np.max(np.abs(rec - x)) < 1e-5
+
+
+def test_median_filter_golden():
+    """The oracle's 27-point median with edge replication reproduces the reference's known answer."""
+    from oracle.denoise import median_filter3d
+    g = json.load(open(os.path.join(os.path.dirname(GOLDEN), 'median_golden.json')))
+    np.testing.assert_array_equal(median_filter3d(np.arange(27).reshape(3, 3, 3)), np.array(g['expected']))
+
+
+def test_denoiser_noise_estimate_matches_oracle():
+    """QGGMRFDenoiser's host-side noise estimate (denoising.py:80-136) agrees with the oracle's restatement."""
+    import mbirjax_b200 as mb
+    from oracle.denoise import estimate_image_noise_std
+    rng = np.random.default_rng(0)
+    img = np.zeros((24, 20, 6), np.float32)
+    img[4:18, 5:15, 1:5] = 1.0
+    img += 0.1 * rng.standard_normal(img.shape).astype(np.float32)
+    d = mb.QGGMRFDenoiser(img.shape)
+    assert d.estimate_image_noise_std(img) == pytest.approx(estimate_image_noise_std(img), rel=1e-6)
