@@ -13,6 +13,11 @@ path (``ParallelBeamModel.recon`` scan after scan) measured the same way, and th
 ``--workload cone``: plain cone-beam VCD on one scan (256 views x 128 rows x 256 channels, sdd = sid = 1024,
 recon 256x256x128 from 20 ellipsoids, 20 iterations x 4 subsets, FDK init).
 
+``--workload translation``: plain translation-geometry VCD on the setup of the reference's translation experiment
+(experiments/translation/exp_translation.py: a 7 x 7 raster of translations 22 ALU apart = 49 views, 128 x 128
+detector, sdd = sid = 64, recon 21x196x196 from the model's own sizing, sharpness 1, zero init, 15 iterations),
+with 10 seeded ellipsoids in place of the rendered-text phantom and 4 subsets per iteration.
+
 Synthetic data stands in for measured scans (the reference publishes no benchmark dataset).
 Timing: W untimed warm-up steps, then exactly K steps between barriers + device synchronisations, timed with
 CUDA events on the launching stream; max over ranks.  L2 is flushed (a 256 MB write) before every step, inside
@@ -50,6 +55,8 @@ METRIC = 'batched vs plain recons/s at 1e-4 NRMSE; proj HBM GB/s; autograd/fwd t
 CONE = dict(views=256, rows=128, channels=256, sdd=1024.0, sid=1024.0, ellipsoids=20, seed=1, subsets=4,
             iterations=20)
 BATCH = dict(num_scans=24, ellipsoids=10, subsets=4, iterations=10, cpu_sample_scan=0)
+TRANS = dict(nx=7, nz=7, spacing=22.0, rows=128, channels=128, sdd=64.0, sid=64.0, ellipsoids=10, seed=2, subsets=4,
+             iterations=15, sharpness=1.0)
 
 
 def parse_args():
@@ -58,18 +65,19 @@ def parse_args():
     ap.add_argument('--steps', type=int, default=5)
     ap.add_argument('--warmup', type=int, default=3)
     ap.add_argument('--impl', default='mbirjax_b200', choices=['mbirjax_b200', 'reference'])
-    ap.add_argument('--workload', default='batched', choices=['batched', 'cone'])
+    ap.add_argument('--workload', default='batched', choices=['batched', 'cone', 'translation'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--scans', type=int, default=None,
                     help='batched workload: the first N scans only (a small case for profiling; default 24)')
-    ap.add_argument('--iterations', type=int, default=None, help='VCD iterations per scan (default 10 / 20)')
+    ap.add_argument('--iterations', type=int, default=None, help='VCD iterations per scan (default 10 / 20 / 15)')
     args = ap.parse_args()
     if args.scans is not None:
         BATCH['num_scans'] = args.scans
     if args.iterations is not None:
         BATCH['iterations'] = args.iterations
         CONE['iterations'] = args.iterations
+        TRANS['iterations'] = args.iterations
     return args
 
 
@@ -187,6 +195,32 @@ def recon_once(model, sino):
     np.random.seed(CONE['seed'])
     rec, _ = model.recon(sino, max_iterations=CONE['iterations'], stop_threshold_change_pct=0, logfile_path=None,
                          print_logs=False)
+    return rec
+
+
+def translation_vectors():
+    from mbirjax_b200.utilities import gen_translation_vectors
+    return gen_translation_vectors(TRANS['nx'], TRANS['nz'], TRANS['spacing'], TRANS['spacing'])
+
+
+def build_translation_workload(device):
+    import mbirjax_b200 as mb
+    from mbirjax_b200.utilities import gen_ellipsoid_phantom, add_noise
+    tv = translation_vectors()
+    model = mb.TranslationModel((tv.shape[0], TRANS['rows'], TRANS['channels']), tv,
+                                source_detector_dist=TRANS['sdd'], source_iso_dist=TRANS['sid'])
+    model.set_params(sharpness=TRANS['sharpness'], snr_db=30.0, granularity=[TRANS['subsets']],
+                     partition_sequence=[0], verbose=0)
+    phantom = gen_ellipsoid_phantom(model.get_params('recon_shape'), TRANS['ellipsoids'], TRANS['seed'], device=device)
+    np.random.seed(TRANS['seed'])
+    sino = add_noise(model.forward_project(phantom), 0.01, TRANS['seed']).contiguous()
+    return model, sino, phantom
+
+
+def translation_recon_once(model, sino):
+    np.random.seed(TRANS['seed'])
+    rec, _ = model.recon(sino, init_recon=0, max_iterations=TRANS['iterations'], stop_threshold_change_pct=0,
+                         logfile_path=None, print_logs=False)
     return rec
 
 
@@ -360,7 +394,7 @@ def autograd_cost():
     return res
 
 
-def kernel_roofline(model, sino, peak_gbs, peak_kind):
+def kernel_roofline(model, sino, peak_gbs, peak_kind, prefix='cone', spec=CONE):
     """Average duration of one VCD subset's back and forward projection (CUDA events, 20 launches each)."""
     import torch
     from mbirjax_b200 import _capi
@@ -368,10 +402,10 @@ def kernel_roofline(model, sino, peak_gbs, peak_kind):
     g = model._geometry()
     V, R, C = model.get_params('sinogram_shape')
     S = model.get_params('recon_shape')[2]
-    np.random.seed(CONE['seed'])
+    np.random.seed(spec['seed'])
     from mbirjax_b200.vcd_utils import morton_sorted_partition
     # the subset in the Z-order the VCD path processes it in
-    subset = morton_sorted_partition(mb.gen_pixel_partition(model.get_params('recon_shape'), CONE['subsets']),
+    subset = morton_sorted_partition(mb.gen_pixel_partition(model.get_params('recon_shape'), spec['subsets']),
                                      model.get_params('recon_shape')[1])[0]
     pix = torch.as_tensor(subset, device='cuda')
     n = int(pix.shape[0])
@@ -379,8 +413,8 @@ def kernel_roofline(model, sino, peak_gbs, peak_kind):
     out_fp = torch.empty((V, R, C), device='cuda')
     out_bp = torch.empty((n, S), device='cuda')
     res = {}
-    for name, fn in (('bp_cone', lambda: _capi.back_project(g, sino, pix, out=out_bp)),
-                     ('fp_cone', lambda: _capi.forward_project(g, vox, pix, out=out_fp))):
+    for name, fn in (('bp_' + prefix, lambda: _capi.back_project(g, sino, pix, out=out_bp)),
+                     ('fp_' + prefix, lambda: _capi.forward_project(g, vox, pix, out=out_fp))):
         for _ in range(3):
             fn()
         torch.cuda.synchronize()
@@ -419,18 +453,25 @@ def profile_traffic(kernel):
     return None
 
 
-def cpu_reference_sample(workers=None):
-    """One VCD subset update of the workload with the oracle on all host cores; returns (seconds, cores, note)."""
+def cpu_reference_sample(workers=None, workload='cone'):
+    """One VCD subset update of the workload with the oracle on all host cores; returns (seconds, cores)."""
     import oracle as O
     from oracle.pool import OraclePool, vcd_subset_update_pooled
-    geom = O.cone_geometry((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(), CONE['sdd'], CONE['sid'])
+    if workload == 'translation':
+        tv = translation_vectors()
+        geom = O.translation_geometry((tv.shape[0], TRANS['rows'], TRANS['channels']), tv, TRANS['sdd'], TRANS['sid'])
+        spec = TRANS
+    else:
+        geom = O.cone_geometry((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(), CONE['sdd'],
+                               CONE['sid'])
+        spec = CONE
     nr, nc, ns = geom.recon_shape
     rng = np.random.default_rng(0)
     flat = rng.random((nr * nc, ns)).astype(np.float32) * 0.1
     err = rng.standard_normal(geom.sinogram_shape).astype(np.float32)
     hess = np.full((nr * nc, ns), 1000.0, dtype=np.float32)
-    np.random.seed(CONE['seed'])
-    subset = O.gen_pixel_partition(geom.recon_shape, CONE['subsets'])[0]
+    np.random.seed(spec['seed'])
+    subset = O.gen_pixel_partition(geom.recon_shape, spec['subsets'])[0]
     params = (O.get_b_from_nbr_wts([1, 1, 1]), 0.05, 2.0, 1.2, 1.0)
     pool = OraclePool(geom, workers)
     try:
@@ -457,6 +498,24 @@ def batched_config(world):
             'parallelism': 'replicas x%d' % world, 'l2': 'flushed before every step (inputs ~1 GB > L2)'}
 
 
+def translation_config(world):
+    tv = translation_vectors()
+    return {'workload': 'plain translation VCD, %d x %d translations %g ALU apart (%d views), detector %dx%d, '
+                        'sdd=sid=%g, %d iterations x %d subsets, zero init, sharpness %g'
+                        % (TRANS['nx'], TRANS['nz'], TRANS['spacing'], tv.shape[0], TRANS['rows'], TRANS['channels'],
+                           TRANS['sdd'], TRANS['iterations'], TRANS['subsets'], TRANS['sharpness']),
+            'views': int(tv.shape[0]), 'det_rows': TRANS['rows'], 'det_channels': TRANS['channels'],
+            'iterations': TRANS['iterations'], 'subsets': TRANS['subsets'], 'parallelism': 'replicas x%d' % world,
+            'l2': 'flushed before every step'}
+
+
+def single_scan_spec(workload):
+    """(spec, config function, cpu sample label) of a single-scan workload."""
+    if workload == 'translation':
+        return TRANS, translation_config, 'the translation scan'
+    return CONE, cone_config, 'the cone scan'
+
+
 def cone_config(world):
     return {'workload': 'plain cone-beam VCD, sinogram 256x128x256, recon 256x256x128, %d iterations x %d subsets, '
                         'FDK init, sdd=sid=1024' % (CONE['iterations'], CONE['subsets']), 'views': CONE['views'], 'det_rows': CONE['rows'],
@@ -474,8 +533,9 @@ def run_reference(args):
         if args.workload == 'batched':
             dt, cores, scale = cpu_batched_sample()
         else:
-            dt, cores = cpu_reference_sample()
-            scale = CONE['subsets'] * CONE['iterations']
+            spec = single_scan_spec(args.workload)[0]
+            dt, cores = cpu_reference_sample(workload=args.workload)
+            scale = spec['subsets'] * spec['iterations']
         if i >= args.warmup:
             samples.append(dt)
     mean = float(np.mean(samples))
@@ -483,11 +543,12 @@ def run_reference(args):
     value = units / (mean * scale)
     sample = ('one VCD subset update of %s per step, oracle NumPy port on %d processes, scaled x%.1f to the whole '
               'workload' % ('scan %d of the batch' % BATCH['cpu_sample_scan'] if args.workload == 'batched'
-                            else 'the cone scan', cores, scale))
+                            else single_scan_spec(args.workload)[2], cores, scale))
     line = {'impl': 'reference', 'metric': METRIC, 'value': value, 'unit': 'recons/s', 'n_gpus': args.gpus,
             'steps': args.steps, 'warmup': args.warmup, 'ms_per_step': mean * 1e3, 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic',
-            'config': batched_config(world) if args.workload == 'batched' else cone_config(world),
+            'config': (batched_config(world) if args.workload == 'batched'
+                       else single_scan_spec(args.workload)[1](world)),
             'cpu_baseline': {'value': value, 'unit': 'recons/s', 'cores': cores, 'kind': 'port', 'sample': sample},
             'e2e': {'value': value, 'unit': 'recons/s', 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0},
             'note': 'reference JAX CPU path unavailable (jax not installable offline); oracle NumPy port timed'}
@@ -513,13 +574,22 @@ def run_gpu(args):
 
         def step():
             batched_recon(models, sinos)
+    elif args.workload == 'translation':
+        model, sino, phantom = build_translation_workload(device)
+        units = 1
+        config = translation_config(world)
+        recon_fn = translation_recon_once
+
+        def step():
+            recon_fn(model, sino)
     else:
         model, sino, phantom = build_cone_workload(device)
         units = 1
         config = cone_config(world)
+        recon_fn = recon_once
 
         def step():
-            recon_once(model, sino)
+            recon_fn(model, sino)
 
     for _ in range(args.warmup):
         step()
@@ -568,7 +638,7 @@ def run_gpu(args):
             out_host = torch.empty(tuple(model.get_params('recon_shape')), dtype=torch.float32).pin_memory()
 
             def e2e_step():
-                r = recon_once(model, host_sino)
+                r = recon_fn(model, host_sino)
                 out_host.copy_(r, non_blocking=True)
             h2d, d2h = int(host_sino.numel()) * 4, int(out_host.numel()) * 4
         e_ms = timed_steps(e2e_step, args.steps, 1, world, flush)
@@ -579,22 +649,25 @@ def run_gpu(args):
     if args.workload == 'batched':
         line['roofline'] = batched_roofline(models, sinos, peak_gbs, peak_kind)
     else:
-        line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind)
+        line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind, args.workload,
+                                           single_scan_spec(args.workload)[0])
 
-    line['autograd'] = autograd_cost()
+    if args.workload != 'translation':
+        line['autograd'] = autograd_cost()
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if args.workload == 'batched':
             dt, cores, scale = cpu_batched_sample()
         else:
-            dt, cores = cpu_reference_sample()
-            scale = CONE['subsets'] * CONE['iterations']
+            spec = single_scan_spec(args.workload)[0]
+            dt, cores = cpu_reference_sample(workload=args.workload)
+            scale = spec['subsets'] * spec['iterations']
         line['cpu_baseline'] = {'value': round(units / (dt * scale), 6), 'unit': 'recons/s', 'cores': cores,
                                 'kind': 'port',
                                 'sample': 'one VCD subset update of %s (oracle NumPy port, %d processes), %.2f s, '
                                           'scaled x%.1f to the workload' % (
                                               'scan %d' % BATCH['cpu_sample_scan'] if args.workload == 'batched'
-                                              else 'the cone scan', cores, dt, scale)}
+                                              else single_scan_spec(args.workload)[2], cores, dt, scale)}
     if rank == 0:
         print(json.dumps(line), flush=True)
     if world > 1:

@@ -41,14 +41,18 @@ extern "C" {
 
 #define MBX_GEOM_PARALLEL 0
 #define MBX_GEOM_CONE 1
+#define MBX_GEOM_TRANSLATION 2
 
 /* Largest psf_radius / bp_psf_radius the kernels accept. */
 #define MBX_MAX_PSF_RADIUS 4
 
 /* Projector geometry.  Replaces the (sinogram_shape, recon_shape, geometry_params) namedtuple that
  * Projectors.create_projectors closes over (projectors.py:47-54), built from
- * ParallelBeamModel.get_geometry_parameters (parallel_beam.py:94-113) or
- * ConeBeamModel.get_geometry_parameters (cone_beam.py:110-136). */
+ * ParallelBeamModel.get_geometry_parameters (parallel_beam.py:94-113),
+ * ConeBeamModel.get_geometry_parameters (cone_beam.py:110-136) or
+ * TranslationModel.get_geometry_parameters (translation_model.py:83-107).  For MBX_GEOM_TRANSLATION the
+ * object moves by a translation vector per view in front of a fixed cone-beam source (no rotation): angles is
+ * unused (may be NULL), psf_radius serves both fans, and bp_psf_radius / recon_slice_offset are unused. */
 typedef struct mbx_geom {
     int32_t kind;                        /* MBX_GEOM_PARALLEL or MBX_GEOM_CONE */
     int32_t num_views;                   /* sinogram_shape[0]; length of angles */
@@ -68,7 +72,9 @@ typedef struct mbx_geom {
     float recon_slice_offset;            /* cone only */
     float source_detector_dist;          /* cone only; +inf allowed */
     float magnification;                 /* cone only; source_detector_dist / source_iso_dist */
-    const float *angles;                 /* device pointer, num_views angles in radians */
+    const float *angles;                 /* parallel / cone: device pointer, num_views angles in radians */
+    float delta_recon_row;               /* translation only: recon row pitch along the source axis (ALU) */
+    const float *translations;           /* translation only: device pointer, num_views x 3 (tx, ty, tz) in ALU */
 } mbx_geom;
 
 /* qGGMRF prior parameters (b, sigma_x, p, q, T) as TomographyModel.create_vcd_subset_updater builds them

@@ -1,6 +1,7 @@
 """mbirjax_b200: the MBIR hot path of mbirjax (v0.6.7) re-built for NVIDIA B200 (sm_100a).
 
-Public API mirrors the reference: ``ParallelBeamModel``, ``ConeBeamModel`` (both ``TomographyModel``s with
+Public API mirrors the reference: ``ParallelBeamModel``, ``ConeBeamModel``, ``TranslationModel`` (all
+``TomographyModel``s with
 ``set_params``, ``forward_project``, ``back_project``, ``sparse_forward_project``, ``sparse_back_project``,
 ``compute_hessian_diagonal``, ``recon``, ``direct_recon``), the pixel-partition utilities and the qGGMRF
 prior.  ``mbirjax_b200.autograd`` wraps the projector pair as torch autograd functions and
@@ -17,6 +18,7 @@ from .parameter_handler import ParameterHandler, Param
 from .tomography_model import TomographyModel
 from .parallel_beam import ParallelBeamModel
 from .cone_beam import ConeBeamModel
+from .translation_model import TranslationModel
 from .denoising import QGGMRFDenoiser, median_filter3d
 from .vcd_utils import (get_2d_ror_mask, gen_pixel_partition, gen_set_of_pixel_partitions, gen_partition_sequence,
                         gen_full_indices)

@@ -14,6 +14,7 @@ _LIB_PATH = os.path.join(os.path.dirname(os.path.abspath(__file__)), '_lib', 'li
 
 MBX_GEOM_PARALLEL = 0
 MBX_GEOM_CONE = 1
+MBX_GEOM_TRANSLATION = 2
 MBX_MAX_PSF_RADIUS = 4
 
 c_int32, c_int64, c_float, c_size_t, c_void_p = (ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_size_t,
@@ -27,7 +28,8 @@ class MbxGeom(ctypes.Structure):
                 ('psf_radius', c_int32), ('bp_psf_radius', c_int32), ('entries_per_cylinder_batch', c_int32),
                 ('delta_det_channel', c_float), ('delta_det_row', c_float), ('det_channel_offset', c_float),
                 ('det_row_offset', c_float), ('delta_voxel', c_float), ('recon_slice_offset', c_float),
-                ('source_detector_dist', c_float), ('magnification', c_float), ('angles', c_void_p)]
+                ('source_detector_dist', c_float), ('magnification', c_float), ('angles', c_void_p),
+                ('delta_recon_row', c_float), ('translations', c_void_p)]
 
 
 class MbxQggmrfParams(ctypes.Structure):

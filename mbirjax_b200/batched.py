@@ -7,8 +7,9 @@ updates run: instead of one chain of launches per scan, every stage of a subset 
 over a packed work list of all scans (``mbx_vcd_batched_step``), and all iterations of all scans are captured
 in a single CUDA graph and replayed, so the host issues no launches and reads nothing back until the end.
 
-Restrictions of the batched path: all scans share one geometry kind, have psf radius 1, and use a single
-partition with the same number of subsets (``granularity=[K]``, ``partition_sequence=[0]``).
+Restrictions of the batched path: all scans share one geometry kind (parallel or cone beam; translation
+geometry runs through ``TomographyModel.recon`` only), have psf radius 1, and use a single partition with the
+same number of subsets (``granularity=[K]``, ``partition_sequence=[0]``).
 """
 import numpy as np
 import torch

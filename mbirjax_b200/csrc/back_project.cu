@@ -1,9 +1,12 @@
-// Sparse back projector for parallel- and cone-beam geometry (sm_100a).
+// Sparse back projector for parallel-beam, cone-beam and translation geometry (sm_100a).
 //
 // Replaces Projectors.sparse_back_project (projectors.py:131-209) over the geometry plugins
-// ParallelBeamModel.back_project_one_view_to_pixel_batch (parallel_beam.py:180-221) and
-// ConeBeamModel.back_project_one_view_to_pixel_batch (cone_beam.py:379-541); coeff_power = 2 gives the
-// Hessian diagonal of TomographyModel.compute_hessian_diagonal (tomography_model.py:679-708).
+// ParallelBeamModel.back_project_one_view_to_pixel_batch (parallel_beam.py:180-221),
+// ConeBeamModel.back_project_one_view_to_pixel_batch (cone_beam.py:379-541) and
+// TranslationModel.back_project_one_view_to_pixel_batch (translation_model.py:382-542); coeff_power = 2 gives
+// the Hessian diagonal of TomographyModel.compute_hessian_diagonal (tomography_model.py:679-708).  Parallel
+// and cone beam run bp_fast.cuh when its plan fits; translation geometry and the other cases run the general
+// kernel of back_project.cuh, described here.
 //
 // One thread owns one pixel and a tile of ST slices.  Its ST accumulators stay in registers across all
 // views, so there are no global atomics and no per-view partial cylinders.  Lanes run along pixels, so the
@@ -122,11 +125,14 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
     float *dst = pl.splits > 1 ? static_cast<float *>(ws) : out;
     const long long stride = num_pixels * (long long)g.num_recon_slices;
     const long long ss = pl.splits > 1 ? stride : 0;
-    cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
-                        ? launch_bp_parallel(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power,
-                                             scale, dst, ss, st)
-                        : launch_bp_cone(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power, scale,
-                                         dst, ss, st);
+    cudaError_t e;
+    if (g.kind == MBX_GEOM_PARALLEL)
+        e = launch_bp_parallel(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power, scale, dst, ss, st);
+    else if (g.kind == MBX_GEOM_CONE)
+        e = launch_bp_cone(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power, scale, dst, ss, st);
+    else
+        e = launch_bp_translation(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power, scale, dst, ss,
+                                  st);
     if (e != cudaSuccess) return set_cuda_error(e);
     if (pl.splits > 1) {
         launch_split_sum(dst, stride, pl.splits, scale, out, stride, st);

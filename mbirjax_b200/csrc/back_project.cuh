@@ -1,5 +1,5 @@
 // Back-projection kernel template and launch plan, shared by the per-geometry translation units
-// bp_parallel.cu and bp_cone.cu (see back_project.cu for the design notes).
+// bp_parallel.cu, bp_cone.cu and bp_translation.cu (see back_project.cu for the design notes).
 #pragma once
 #include <climits>
 #include <cmath>
@@ -76,7 +76,7 @@ bp_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restr
         }
     }
     float xt = 0.0f, yt = 0.0f;
-    if (active) pixel_tilde(g, idx, xt, yt);
+    if (active && KIND != MBX_GEOM_TRANSLATION) pixel_tilde(g, idx, xt, yt);
 
     float acc[ST];
 #pragma unroll
@@ -93,24 +93,32 @@ bp_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restr
             const int vi = views ? views[vb + t] : vb + t;
             const bool ok = vi >= 0 && vi < g.num_views;
             if (!ok && blockIdx.x == 0 && blockIdx.y == 0) flag_error(err, MBX_ERRFLAG_VIEW);
-            const float ang = ok ? g.angles[vi] : 0.0f;
             s_vi[t] = ok ? vi : -1;
-            s_ang[t] = ang;
-            s_cs[t] = cosf(ang);
-            s_sn[t] = sinf(ang);
+            if (KIND == MBX_GEOM_TRANSLATION) {  // (zoff = -tz, tx, ty) in the (angle, cos, sin) slots
+                s_ang[t] = ok ? -g.translations[3 * vi + 2] : 0.0f;
+                s_cs[t] = ok ? g.translations[3 * vi] : 0.0f;
+                s_sn[t] = ok ? g.translations[3 * vi + 1] : 0.0f;
+            } else {
+                const float ang = ok ? g.angles[vi] : 0.0f;
+                s_ang[t] = ang;
+                s_cs[t] = cosf(ang);
+                s_sn[t] = sinf(ang);
+            }
         }
         __syncthreads();
         if (!active) continue;
         for (int t = 0; t < nv; ++t) {
             const int vi = s_vi[t];
             if (vi < 0) continue;
-            const ChannelFootprint f = (KIND == MBX_GEOM_PARALLEL)
-                                           ? parallel_footprint(g, s_cs[t], s_sn[t], xt, yt)
-                                           : cone_footprint(g, s_ang[t], s_cs[t], s_sn[t], xt, yt);
+            const ChannelFootprint f = (KIND == MBX_GEOM_PARALLEL) ? parallel_footprint(g, s_cs[t], s_sn[t], xt, yt)
+                                       : (KIND == MBX_GEOM_CONE) ? cone_footprint(g, s_ang[t], s_cs[t], s_sn[t], xt, yt)
+                                                                 : translation_footprint(g, idx, s_cs[t], s_sn[t]);
             float a[NT];
 #pragma unroll
             for (int k = -MAXR; k <= MAXR; ++k) {
-                const float c = (k < -r || k > r) ? 0.0f : channel_coeff(g, f, k);
+                const float c = (k < -r || k > r) ? 0.0f
+                                : (KIND == MBX_GEOM_TRANSLATION) ? translation_channel_coeff(g, f, k)
+                                                                 : channel_coeff(g, f, k);
                 a[k + MAXR] = (coeff_power == 2) ? c * c : c;
             }
             const float *view = sino + (long long)vi * num_rows * num_channels;
@@ -120,13 +128,16 @@ bp_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restr
                 for (int s = 0; s < ST; ++s)
                     if (s < ns) acc[s] += horizontal_row_sum<MAXR>(view, wview, s0 + s, num_channels, f.n_c, a);
             } else {
+                // slice k sits at height delta_voxel (k - (S-1)/2) + zoff: recon_slice_offset for the cone,
+                // -tz for a translation view (translation_model.py:654)
+                const float zoff = (KIND == MBX_GEOM_TRANSLATION) ? s_ang[t] : g.recon_slice_offset;
                 const float mag = f.mag;
                 const float w_r = mag * (g.delta_voxel / g.delta_det_row);
                 const float l_max = fminf(1.0f, w_r);
                 const float half_w = (w_r + 1.0f) * 0.5f;
                 // Detector rows touched by this slice tile: between the centre rows of its end slices +- r.
-                const float z_first = g.delta_voxel * ((float)s0 - center_slice) + g.recon_slice_offset;
-                const float z_last = g.delta_voxel * ((float)(s0 + ns - 1) - center_slice) + g.recon_slice_offset;
+                const float z_first = g.delta_voxel * ((float)s0 - center_slice) + zoff;
+                const float z_last = g.delta_voxel * ((float)(s0 + ns - 1) - center_slice) + zoff;
                 const int mc_first = (int)rintf((mag * z_first + g.det_row_offset) / g.delta_det_row + det_center_row);
                 const int mc_last = (int)rintf((mag * z_last + g.det_row_offset) / g.delta_det_row + det_center_row);
                 const int m_lo = max(min(mc_first, mc_last) - r, 0);
@@ -138,7 +149,7 @@ bp_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restr
 #pragma unroll
                 for (int s = 0; s < ST; ++s) {
                     if (s < ns) {
-                        const float z = g.delta_voxel * ((float)(s0 + s) - center_slice) + g.recon_slice_offset;
+                        const float z = g.delta_voxel * ((float)(s0 + s) - center_slice) + zoff;
                         const float v = mag * z;
                         const float m_p = (v + g.det_row_offset) / g.delta_det_row + det_center_row;
                         const int m_c = (int)rintf(m_p);
@@ -187,6 +198,15 @@ inline int cone_cache_rows(const mbx_geom &g, int st) {
     return (int)rows;
 }
 
+// Translation geometry: the host does not see the translations, so the cache is sized from psf_radius, which the
+// model derives from the largest magnification (translation_model.py:134-172): a slice spans at most
+// ceil(W) <= 2 psf_radius rows.  A view whose rows do not fit takes the uncached path.
+inline int translation_cache_rows(const mbx_geom &g, int st) {
+    const int r = g.psf_radius > 0 ? g.psf_radius : 1;
+    const int rows = st * 2 * r + 2 * g.psf_radius + 2;
+    return rows > BP_MAX_CACHE_ROWS ? BP_MAX_CACHE_ROWS : rows;
+}
+
 inline BpPlan plan_bp(const mbx_geom &g, long long num_pixels, int num_views_sel) {
     BpPlan pl;
     const int S = g.num_recon_slices;
@@ -194,7 +214,9 @@ inline BpPlan plan_bp(const mbx_geom &g, long long num_pixels, int num_views_sel
     pl.st = (S >= 16 && psf_bucket(g.psf_radius) <= 2) ? 16 : 8;
     pl.gx = ceil_div(num_pixels > 0 ? num_pixels : 1, BP_THREADS);
     pl.gy = ceil_div(S, pl.st);
-    pl.cache_rows = (g.kind == MBX_GEOM_CONE) ? cone_cache_rows(g, pl.st) : 0;
+    pl.cache_rows = (g.kind == MBX_GEOM_CONE)          ? cone_cache_rows(g, pl.st)
+                    : (g.kind == MBX_GEOM_TRANSLATION) ? translation_cache_rows(g, pl.st)
+                                                       : 0;
     pl.smem = (size_t)pl.cache_rows * BP_THREADS * 4;
     const long long base = (long long)pl.gx * pl.gy;
     const int sms = num_sms();
@@ -252,12 +274,15 @@ cudaError_t launch_bp_kind(const mbx_geom &g, const BpPlan &pl, const float *sin
 }
 
 
-// Defined in bp_parallel.cu / bp_cone.cu.
+// Defined in bp_parallel.cu / bp_cone.cu / bp_translation.cu.
 cudaError_t launch_bp_parallel(const mbx_geom &g, const BpPlan &pl, const float *sino, const float *w,
                                const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
                                float *dst, long long ss, cudaStream_t st);
 cudaError_t launch_bp_cone(const mbx_geom &g, const BpPlan &pl, const float *sino, const float *w,
                            const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
                            float *dst, long long ss, cudaStream_t st);
+cudaError_t launch_bp_translation(const mbx_geom &g, const BpPlan &pl, const float *sino, const float *w,
+                                  const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
+                                  float *dst, long long ss, cudaStream_t st);
 
 }  // namespace mbx

@@ -357,7 +357,7 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
     BpfPlan pl;
     pl.inline_fp = inline_fp;
     // 32-bit element offsets address the sinogram
-    pl.ok = (g.psf_radius == 1) && g.num_det_channels >= 3 &&
+    pl.ok = (g.kind == MBX_GEOM_PARALLEL || g.kind == MBX_GEOM_CONE) && (g.psf_radius == 1) && g.num_det_channels >= 3 &&
             (long long)g.num_views * g.num_det_rows * g.num_det_channels < (1LL << 31);
     const int S = g.num_recon_slices;
     // tile height: the fewest tiles of <= BPF_ST slices, rounded up to a power of two (<= 8) or a multiple of 8,

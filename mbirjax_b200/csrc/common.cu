@@ -1,5 +1,6 @@
 // Library identification, error reporting and device queries for the mbirjax_b200 C ABI.
 #include <atomic>
+#include <cmath>
 #include <cstdio>
 #include <map>
 #include <mutex>
@@ -101,7 +102,8 @@ int num_sms() {
 
 int validate_geom(const mbx_geom *g) {
     if (!g) return MBX_ERR_INVALID_ARG;
-    if (g->kind != MBX_GEOM_PARALLEL && g->kind != MBX_GEOM_CONE) return MBX_ERR_INVALID_ARG;
+    if (g->kind != MBX_GEOM_PARALLEL && g->kind != MBX_GEOM_CONE && g->kind != MBX_GEOM_TRANSLATION)
+        return MBX_ERR_INVALID_ARG;
     if (g->num_views <= 0 || g->num_det_rows <= 0 || g->num_det_channels <= 0) return MBX_ERR_INVALID_ARG;
     if (g->num_recon_rows <= 0 || g->num_recon_cols <= 0 || g->num_recon_slices <= 0) return MBX_ERR_INVALID_ARG;
     if ((long long)g->num_recon_rows * g->num_recon_cols > 2147483647LL) return MBX_ERR_UNSUPPORTED;
@@ -114,6 +116,15 @@ int validate_geom(const mbx_geom *g) {
         return MBX_ERR_INVALID_ARG;
     if (g->kind == MBX_GEOM_CONE && (!(g->magnification > 0.0f) || !(g->source_detector_dist > 0.0f)))
         return MBX_ERR_INVALID_ARG;
+    if (g->kind == MBX_GEOM_TRANSLATION) {
+        // a finite source distance: with the source at infinity every translated view carries the same
+        // information (translation_model.py:69-81)
+        if (!g->translations || !(g->delta_recon_row > 0.0f) || !(g->magnification > 0.0f) ||
+            !(g->source_detector_dist > 0.0f) || !std::isfinite(g->source_detector_dist) ||
+            g->entries_per_cylinder_batch <= 0)
+            return MBX_ERR_INVALID_ARG;
+        return MBX_OK;
+    }
     if (!g->angles) return MBX_ERR_INVALID_ARG;
     return MBX_OK;
 }

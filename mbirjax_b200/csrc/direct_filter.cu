@@ -92,6 +92,9 @@ extern "C" int mbx_direct_filter(const mbx_geom *g, const float *sinogram, float
     int rc = mbx::validate_geom(g);
     if (rc != MBX_OK) return rc;
     if (!sinogram || !out || sinogram == out) return MBX_ERR_INVALID_ARG;
+    // translation geometry has no direct reconstruction (the base TomographyModel's zeros,
+    // tomography_model.py:934-964)
+    if (g->kind == MBX_GEOM_TRANSLATION) return MBX_ERR_UNSUPPORTED;
     const int C = g->num_det_channels, R = g->num_det_rows;
     const size_t smem = ((size_t)C * mbx::FILT_ROWS + 2 * (size_t)C - 1) * sizeof(float);
     if (smem > 200 * 1024) return MBX_ERR_UNSUPPORTED;

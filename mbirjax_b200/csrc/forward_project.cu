@@ -1,8 +1,11 @@
-// Sparse forward projector for parallel- and cone-beam geometry (sm_100a).
+// Sparse forward projector for parallel-beam, cone-beam and translation geometry (sm_100a).
 //
 // Replaces Projectors.sparse_forward_project (projectors.py:61-129) over the geometry plugins
-// ParallelBeamModel.forward_project_pixel_batch_to_one_view (parallel_beam.py:138-178) and
-// ConeBeamModel.forward_project_pixel_batch_to_one_view (cone_beam.py:189-377).
+// ParallelBeamModel.forward_project_pixel_batch_to_one_view (parallel_beam.py:138-178),
+// ConeBeamModel.forward_project_pixel_batch_to_one_view (cone_beam.py:189-377) and
+// TranslationModel.forward_project_pixel_batch_to_one_view (translation_model.py:190-378).
+// Parallel and cone beam run the channel-block kernel of fp_cb.cuh when its plan fits; translation geometry and
+// the other cases run the general kernel below.
 //
 // One CTA owns an output tile (one view x a band of detector rows x all channels) held in shared memory,
 // walks every pixel of its pixel range in chunks of FP_PB, and scatters into the tile with shared-memory
@@ -51,7 +54,16 @@ fp_kernel(const mbx_geom g, const float *__restrict__ vox, const int32_t *__rest
     const int vi = views ? views[j] : j;
     const bool view_ok = vi >= 0 && vi < g.num_views;
     if (!view_ok && tid == 0) flag_error(err, MBX_ERRFLAG_VIEW);
-    const float angle = view_ok ? g.angles[vi] : 0.0f;
+    float angle = 0.0f, tx = 0.0f, ty = 0.0f, zoff = 0.0f;
+    if (view_ok) {
+        if (KIND == MBX_GEOM_TRANSLATION) {
+            tx = g.translations[3 * vi];
+            ty = g.translations[3 * vi + 1];
+            zoff = -g.translations[3 * vi + 2];
+        } else {
+            angle = g.angles[vi];
+        }
+    }
     const float cs = cosf(angle);
     const float sn = sinf(angle);
 
@@ -72,16 +84,23 @@ fp_kernel(const mbx_geom g, const float *__restrict__ vox, const int32_t *__rest
                 if (idx < 0 || idx >= npix_grid) {
                     flag_error(err, MBX_ERRFLAG_PIXEL);
                 } else {
-                    float xt, yt;
-                    pixel_tilde(g, idx, xt, yt);
-                    const ChannelFootprint f = (KIND == MBX_GEOM_PARALLEL)
-                                                   ? parallel_footprint(g, cs, sn, xt, yt)
-                                                   : cone_footprint(g, angle, cs, sn, xt, yt);
+                    ChannelFootprint f;
+                    if (KIND == MBX_GEOM_TRANSLATION) {
+                        f = translation_footprint(g, idx, tx, ty);
+                    } else {
+                        float xt, yt;
+                        pixel_tilde(g, idx, xt, yt);
+                        f = (KIND == MBX_GEOM_PARALLEL) ? parallel_footprint(g, cs, sn, xt, yt)
+                                                        : cone_footprint(g, angle, cs, sn, xt, yt);
+                    }
                     nc = f.n_c;
 #pragma unroll
                     for (int k = -MAXR; k <= MAXR; ++k)
                         h_a[tid * NT + k + MAXR] =
-                            (k < -g.psf_radius || k > g.psf_radius) ? 0.0f : channel_coeff(g, f, k);
+                            (k < -g.psf_radius || k > g.psf_radius)
+                                ? 0.0f
+                                : (KIND == MBX_GEOM_TRANSLATION ? translation_channel_coeff(g, f, k)
+                                                                : channel_coeff(g, f, k));
                     h_mag[tid] = f.mag;
                 }
             }
@@ -101,8 +120,10 @@ fp_kernel(const mbx_geom g, const float *__restrict__ vox, const int32_t *__rest
                 float val;
                 if (KIND == MBX_GEOM_PARALLEL)
                     val = __ldg(cyl + m0 + ml);
-                else
+                else if (KIND == MBX_GEOM_CONE)
                     val = cone_fp_vertical<MAXRBP>(g, cyl, mag, m0 + ml);
+                else
+                    val = fan_fp_vertical<MAXRBP>(g, cyl, mag, m0 + ml, zoff, g.psf_radius);
                 float *trow = tile + ml * c_pad;
 #pragma unroll
                 for (int k = -MAXR; k <= MAXR; ++k) {
@@ -200,7 +221,10 @@ static cudaError_t launch_fp_kind(const mbx_geom &g, const FpPlan &pl, const flo
                                   long long n, const int32_t *views, int nv, float *dst, long long ss,
                                   cudaStream_t st) {
     const int r = psf_bucket(g.psf_radius);
-    const int rb = (KIND == MBX_GEOM_CONE) ? psf_bucket(g.bp_psf_radius) : 1;
+    // vertical taps: bp_psf_radius for the cone, psf_radius for translation (translation_model.py:364)
+    const int rb = (KIND == MBX_GEOM_CONE)          ? psf_bucket(g.bp_psf_radius)
+                   : (KIND == MBX_GEOM_TRANSLATION) ? psf_bucket(g.psf_radius)
+                                                    : 1;
     if (r == 1 && rb == 1) return launch_fp_t<KIND, 1, 1>(g, pl, vox, pix, n, views, nv, dst, ss, st);
     if (r == 2 && rb <= 2) return launch_fp_t<KIND, 2, 2>(g, pl, vox, pix, n, views, nv, dst, ss, st);
     if (r == 1 && rb == 2) return launch_fp_t<KIND, 2, 2>(g, pl, vox, pix, n, views, nv, dst, ss, st);
@@ -304,9 +328,13 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
     float *dst = pl.splits > 1 ? static_cast<float *>(ws) : out;
     const long long stride = (long long)num_views_sel * g.num_det_rows * g.num_det_channels;
     const long long ss = pl.splits > 1 ? stride : 0;
-    cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
-                        ? launch_fp_kind<MBX_GEOM_PARALLEL>(g, pl, vox, pix, num_pixels, views, num_views_sel, dst, ss, st)
-                        : launch_fp_kind<MBX_GEOM_CONE>(g, pl, vox, pix, num_pixels, views, num_views_sel, dst, ss, st);
+    cudaError_t e;
+    if (g.kind == MBX_GEOM_PARALLEL)
+        e = launch_fp_kind<MBX_GEOM_PARALLEL>(g, pl, vox, pix, num_pixels, views, num_views_sel, dst, ss, st);
+    else if (g.kind == MBX_GEOM_CONE)
+        e = launch_fp_kind<MBX_GEOM_CONE>(g, pl, vox, pix, num_pixels, views, num_views_sel, dst, ss, st);
+    else
+        e = launch_fp_kind<MBX_GEOM_TRANSLATION>(g, pl, vox, pix, num_pixels, views, num_views_sel, dst, ss, st);
     if (e != cudaSuccess) return set_cuda_error(e);
     if (pl.splits > 1) {
         launch_split_sum(dst, stride, pl.splits, 1.0f, out, stride, st);

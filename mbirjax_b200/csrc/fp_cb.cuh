@@ -97,7 +97,7 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
                          int nb_max = 128, int avoid_ppw = 0) {
     CbPlan pl = {};
     pl.minb = minb;
-    pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || g.bp_psf_radius == 1);
+    pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || (g.kind == MBX_GEOM_CONE && g.bp_psf_radius == 1));
     const int R = g.num_det_rows, C = g.num_det_channels;
     // lane layout: padded rows weighted by the cost of ppw diverging sub-groups, plus a small cost per pass
     static const int combos[12][2] = {{1, 1}, {1, 2}, {1, 3}, {1, 4}, {2, 1}, {2, 2},

@@ -87,13 +87,14 @@ class TomographyModel(ParameterHandler):
         return _cuda_device()
 
     def _geometry(self):
-        """The mbx_geom record for the current parameters.  Its angle pointer refers to a device tensor owned by
-        this model, so the record is valid only while the model is alive and its geometry parameters unchanged."""
+        """The mbx_geom record for the current parameters.  Its angle (or translation) pointer refers to a device
+        tensor owned by this model, so the record is valid only while the model is alive and its geometry
+        parameters unchanged."""
         if self._geom is None:
             dev = self._device()
             sinogram_shape, recon_shape = self.get_params(['sinogram_shape', 'recon_shape'])
-            angles = np.asarray(self.get_params(self.get_params('view_params_name')), dtype=np.float32)
-            self._angles_dev = torch.as_tensor(angles, device=dev).contiguous()
+            view_params = np.asarray(self.get_params(self.get_params('view_params_name')), dtype=np.float32)
+            self._angles_dev = torch.as_tensor(view_params, device=dev).contiguous()
             gp = self.get_geometry_parameters()
             g = _capi.MbxGeom()
             g.kind = self._kind()
@@ -110,7 +111,11 @@ class TomographyModel(ParameterHandler):
             g.recon_slice_offset = float(getattr(gp, 'recon_slice_offset', 0.0))
             g.source_detector_dist = float(getattr(gp, 'source_detector_dist', np.inf))
             g.magnification = float(getattr(gp, 'magnification', 1.0))
-            g.angles = self._angles_dev.data_ptr()
+            if g.kind == _capi.MBX_GEOM_TRANSLATION:  # (num_views, 3) translation vectors
+                g.translations = self._angles_dev.data_ptr()
+                g.delta_recon_row = float(gp.delta_recon_row)
+            else:
+                g.angles = self._angles_dev.data_ptr()
             if g.psf_radius > _capi.MBX_MAX_PSF_RADIUS or g.bp_psf_radius > _capi.MBX_MAX_PSF_RADIUS:
                 raise ValueError('psf radius %d / %d exceeds the supported maximum %d' % (
                     g.psf_radius, g.bp_psf_radius, _capi.MBX_MAX_PSF_RADIUS))

@@ -53,3 +53,14 @@ def batched_scan_shapes(num_scans=24):
         rng = np.random.default_rng(i)
         shapes.append((int(rng.integers(60, 721)), int(rng.integers(8, 65)), int(rng.integers(96, 513))))
     return shapes
+
+
+def gen_translation_vectors(num_x_translations, num_z_translations, x_spacing, z_spacing):
+    """(num_x * num_z, 3) translation vectors [dx, 0, dz] on a raster centred at 0, x fastest
+    (utilities.py:1003-1031 of the reference)."""
+    x = (np.arange(num_x_translations) - (num_x_translations - 1) / 2) * x_spacing
+    z = (np.arange(num_z_translations) - (num_z_translations - 1) / 2) * z_spacing
+    out = np.zeros((num_x_translations * num_z_translations, 3))
+    out[:, 0] = np.tile(x, num_z_translations)
+    out[:, 2] = np.repeat(z, num_x_translations)
+    return out

@@ -1,7 +1,7 @@
 """CPU oracle for the MBIR hot path: TEST INFRASTRUCTURE ONLY.
 
 This package restates, in NumPy, the arithmetic of the mbirjax reference (v0.6.7) for the functions
-on the hot path: parallel- and cone-beam sparse forward/back projection, the qGGMRF surrogate
+on the hot path: parallel-beam, cone-beam and translation sparse forward/back projection, the qGGMRF surrogate
 gradient/Hessian and loss, pixel partitions, the VCD subset update and FBP/FDK filtering.  Every
 function cites the reference file:line it follows.
 
@@ -16,7 +16,7 @@ tests (adjointness, Hessian finite difference, view batching) because the refere
 not installable offline.
 """
 
-from .geometry import OracleGeometry, parallel_geometry, cone_geometry  # noqa: F401
+from .geometry import OracleGeometry, parallel_geometry, cone_geometry, translation_geometry  # noqa: F401
 from .projectors import (  # noqa: F401
     sparse_forward_project, sparse_back_project, forward_project, back_project,
     compute_hessian_diagonal,

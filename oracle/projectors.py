@@ -15,7 +15,15 @@ Reference functions restated here:
 * cone horizontal FP: ``cone_beam.py:244-284``; horizontal BP: ``cone_beam.py:409-451``
 * cone vertical BP one pixel: ``cone_beam.py:480-541`` with ``compute_vertical_data_single_pixel``
   ``cone_beam.py:543-591`` (voxel-centric, 128-slice batches)
+* translation ``compute_horizontal_data``: ``translation_model.py:595-644``; ``recon_ijk_to_xyz``:
+  ``translation_model.py:646-656``; ``compute_y_mag_for_pixel``: ``translation_model.py:694-706``
+* translation horizontal FP / BP: ``translation_model.py:244-284`` / ``:412-453`` (coefficient L / cos(theta_p),
+  no delta_voxel factor); vertical FP: ``translation_model.py:286-378`` and vertical BP:
+  ``translation_model.py:482-593``, the cone's fans with the slice axis shifted by -tz and psf_radius taps
 * batching over views / pixels: ``projectors.py:61-209``; ``tomography_model.py:531-708``
+
+For translation geometry ``geom.angles`` holds the (views, 3) translation vectors and the per-view functions
+take one translation vector where the rotating geometries take an angle.
 """
 import numpy as np
 import scipy.sparse as sp
@@ -71,14 +79,46 @@ def cone_horizontal_data(geom, pixel_indices, angle, dt=np.float32):
     return n_p, n_p_center, w_p_c.astype(dt), cos_alpha
 
 
+def _translation_xy(geom, pixel_indices, tv, dt):
+    """recon_ijk_to_xyz, translation_model.py:646-656: (x_p, y_p) of each pixel for translation vector tv."""
+    nr, nc = geom.recon_shape[:2]
+    row, col = np.unravel_index(np.asarray(pixel_indices, dtype=np.int64), (nr, nc))
+    y_p = dt(geom.delta_recon_row) * (row.astype(dt) - dt((nr - 1) / 2.0)) - dt(tv[1])
+    x_p = dt(geom.delta_voxel) * (col.astype(dt) - dt((nc - 1) / 2.0)) - dt(tv[0])
+    return x_p, y_p
+
+
+def _translation_pixel_mag(geom, pixel_indices, tv, dt):
+    """compute_y_mag_for_pixel, translation_model.py:694-706."""
+    _, y_p = _translation_xy(geom, pixel_indices, tv, dt)
+    return dt(1) / (dt(1 / geom.magnification) - y_p / dt(geom.source_detector_dist))
+
+
+def translation_horizontal_data(geom, pixel_indices, tv, dt=np.float32):
+    """translation_model.py:595-644: returns n_p, n_p_center, W_p_c, cos_theta_p."""
+    x_p, y_p = _translation_xy(geom, pixel_indices, tv, dt)
+    D = dt(geom.source_detector_dist)
+    pixel_mag = dt(1) / (dt(1 / geom.magnification) - y_p / D)
+    u_p = pixel_mag * x_p
+    det_center_channel = dt((geom.sinogram_shape[2] - 1) / 2.0)
+    n_p = (u_p + dt(geom.det_channel_offset)) / dt(geom.delta_det_channel) + det_center_channel
+    n_p_center = np.round(n_p).astype(np.int64)
+    cos_theta = np.cos(np.arctan2(u_p, D).astype(dt)).astype(dt)
+    w_p_c = pixel_mag * (dt(geom.delta_voxel) / dt(geom.delta_det_channel))
+    return n_p, n_p_center, w_p_c.astype(dt), cos_theta
+
+
 def _channel_matrix(geom, pixel_indices, angle, dt, coeff_power):
     """Sparse (C x N) matrix of channel coefficients A_chan_n for one view (raised to coeff_power).
 
-    The coefficient is the reference's (parallel_beam.py:170-175 / cone_beam.py:276-281)."""
+    The coefficient is the reference's (parallel_beam.py:170-175 / cone_beam.py:276-281 / translation_model.py:
+    275-281, where it has no delta_voxel factor); ``angle`` is the translation vector for translation geometry."""
     if geom.kind == 'parallel':
         n_p, n_c, w, cos_a = parallel_proj_data(geom, pixel_indices, angle, dt)
-    else:
+    elif geom.kind == 'cone':
         n_p, n_c, w, cos_a = cone_horizontal_data(geom, pixel_indices, angle, dt)
+    else:
+        n_p, n_c, w, cos_a = translation_horizontal_data(geom, pixel_indices, angle, dt)
     num_det_channels = geom.sinogram_shape[2]
     l_max = np.minimum(dt(1), w)
     num_pixels = n_p.shape[0]
@@ -87,7 +127,7 @@ def _channel_matrix(geom, pixel_indices, angle, dt, coeff_power):
         n = n_c + n_offset
         abs_delta = np.abs(n_p - n.astype(dt))
         l_pcn = np.clip((w + dt(1)) / dt(2) - abs_delta, dt(0), l_max)
-        a = dt(geom.delta_voxel) * l_pcn / cos_a
+        a = l_pcn / cos_a if geom.kind == 'translation' else dt(geom.delta_voxel) * l_pcn / cos_a
         valid = (n >= 0) & (n < num_det_channels)
         a = a * valid.astype(dt)
         if coeff_power != 1:
@@ -111,12 +151,24 @@ def _cone_pixel_mag(geom, pixel_indices, angle, dt):
 
 def cone_forward_vertical(geom, voxel_values, pixel_indices, angle, dt=np.float32):
     """cone_beam.py:286-377, vectorised over pixels: (N, S) voxel cylinders -> (N, R) detector columns."""
+    pixel_mag = _cone_pixel_mag(geom, pixel_indices, angle, dt)
+    return _fan_forward_vertical(geom, voxel_values, pixel_mag, geom.recon_slice_offset, geom.bp_psf_radius, dt)
+
+
+def translation_forward_vertical(geom, voxel_values, pixel_indices, tv, dt=np.float32):
+    """translation_model.py:286-378: the cone's detector-row-centric fan with slice heights
+    delta_voxel (k - (S-1)/2) - tz and psf_radius taps."""
+    pixel_mag = _translation_pixel_mag(geom, pixel_indices, tv, dt)
+    return _fan_forward_vertical(geom, voxel_values, pixel_mag, -dt(tv[2]), geom.psf_radius, dt)
+
+
+def _fan_forward_vertical(geom, voxel_values, pixel_mag, zoff, radius, dt):
     num_views, num_det_rows, _ = geom.sinogram_shape
     num_slices = voxel_values.shape[1]
     dv = dt(geom.delta_voxel)
-    pixel_mag = _cone_pixel_mag(geom, pixel_indices, angle, dt)[:, None]       # (N, 1)
+    pixel_mag = pixel_mag[:, None]                                             # (N, 1)
     k = np.arange(num_slices)
-    z = dv * (k.astype(dt) - dt((num_slices - 1) / 2.0)) + dt(geom.recon_slice_offset)
+    z = dv * (k.astype(dt) - dt((num_slices - 1) / 2.0)) + dt(zoff)
     v = pixel_mag * z[None, :]
     D = dt(geom.source_detector_dist)
     cos_phi = np.cos(np.arctan2(v, D).astype(dt)).astype(dt)
@@ -134,11 +186,11 @@ def cone_forward_vertical(geom, voxel_values, pixel_indices, angle, dt=np.float3
         m_center = start + row_batch
         v_m = (m_center.astype(dt) - det_center_row) * dt(geom.delta_det_row) - dt(geom.det_row_offset)
         z_m = v_m[None, :] / pixel_mag                                          # (N, rpb)
-        k_m = (z_m - dt(geom.recon_slice_offset)) / dv + dt((num_slices - 1) / 2.0)
+        k_m = (z_m - dt(zoff)) / dv + dt((num_slices - 1) / 2.0)
         k_m_center = np.round(k_m).astype(np.int64)
         m_p = slope * (k_m_center.astype(dt) - k_m[:, :1]) + dt(m_center[0])
         new_col = np.zeros(k_m.shape, dtype=dt)
-        for k_offset in range(-geom.bp_psf_radius, geom.bp_psf_radius + 1):
+        for k_offset in range(-radius, radius + 1):
             k_ind = k_m_center + k_offset
             abs_delta = np.abs(m_p + slope * dt(k_offset) - m_center[None, :].astype(dt))
             a = np.clip((w_p_r + dt(1)) / dt(2) - abs_delta, dt(0), l_max)
@@ -151,22 +203,34 @@ def cone_forward_vertical(geom, voxel_values, pixel_indices, angle, dt=np.float3
 
 def cone_back_vertical(geom, det_columns, pixel_indices, angle, coeff_power=1, dt=np.float32):
     """cone_beam.py:480-591, vectorised over pixels: (N, R) detector columns -> (N, S) voxel cylinders."""
-    num_views, num_det_rows, _ = geom.sinogram_shape
-    num_slices = geom.recon_shape[2]
-    dv = dt(geom.delta_voxel)
     x_tilde, y_tilde = _pixel_xy_tilde(geom, pixel_indices, dt)
     angle = dt(angle)
     cosine, sine = dt(np.cos(angle)), dt(np.sin(angle))
-    y_p = (sine * x_tilde + cosine * y_tilde)[:, None]
+    y_p = sine * x_tilde + cosine * y_tilde
+    pixel_mag = dt(1) / (dt(1 / geom.magnification) - y_p / dt(geom.source_detector_dist))
+    return _fan_back_vertical(geom, det_columns, pixel_mag, geom.recon_slice_offset, coeff_power, dt)
+
+
+def translation_back_vertical(geom, det_columns, pixel_indices, tv, coeff_power=1, dt=np.float32):
+    """translation_model.py:482-593: the cone's voxel-centric fan with slice heights
+    delta_voxel (k - (S-1)/2) - tz."""
+    pixel_mag = _translation_pixel_mag(geom, pixel_indices, tv, dt)
+    return _fan_back_vertical(geom, det_columns, pixel_mag, -dt(tv[2]), coeff_power, dt)
+
+
+def _fan_back_vertical(geom, det_columns, pixel_mag, zoff, coeff_power, dt):
+    num_views, num_det_rows, _ = geom.sinogram_shape
+    num_slices = geom.recon_shape[2]
+    dv = dt(geom.delta_voxel)
     D = dt(geom.source_detector_dist)
-    pixel_mag = dt(1) / (dt(1 / geom.magnification) - y_p / D)              # (N, 1)
+    pixel_mag = pixel_mag[:, None]                                             # (N, 1)
     slices_per_batch = min(geom.entries_per_cylinder_batch, num_slices)
     num_batches = (num_slices + slices_per_batch - 1) // slices_per_batch
     det_center_row = dt((num_det_rows - 1) / 2.0)
     out = []
     for b in range(num_batches):
         cur = slices_per_batch * b + np.arange(slices_per_batch)
-        z_p = dv * (cur.astype(dt) - dt((num_slices - 1) / 2.0)) + dt(geom.recon_slice_offset)
+        z_p = dv * (cur.astype(dt) - dt((num_slices - 1) / 2.0)) + dt(zoff)
         v_p = pixel_mag * z_p[None, :]
         m_p = (v_p + dt(geom.det_row_offset)) / dt(geom.delta_det_row) + det_center_row
         m_c = np.round(m_p).astype(np.int64)
@@ -189,24 +253,30 @@ def cone_back_vertical(geom, det_columns, pixel_indices, angle, coeff_power=1, d
 
 
 def forward_project_one_view(geom, voxel_values, pixel_indices, angle, dt=np.float32):
-    """(N, S) -> (R, C) for one view; parallel_beam.py:138-178 / cone_beam.py:189-217."""
+    """(N, S) -> (R, C) for one view; parallel_beam.py:138-178 / cone_beam.py:189-217 /
+    translation_model.py:190-217."""
     voxel_values = np.asarray(voxel_values, dtype=dt)
     if geom.kind == 'parallel':
         columns = voxel_values                                                  # slice k <-> row k
-    else:
+    elif geom.kind == 'cone':
         columns = cone_forward_vertical(geom, voxel_values, pixel_indices, angle, dt)
+    else:
+        columns = translation_forward_vertical(geom, voxel_values, pixel_indices, angle, dt)
     chan = _channel_matrix(geom, pixel_indices, angle, dt, 1)
     return np.asarray((chan @ columns).T, dtype=dt)
 
 
 def back_project_one_view(geom, view, pixel_indices, angle, coeff_power=1, dt=np.float32):
-    """(R, C) -> (N, S) for one view; parallel_beam.py:180-221 / cone_beam.py:379-407."""
+    """(R, C) -> (N, S) for one view; parallel_beam.py:180-221 / cone_beam.py:379-407 /
+    translation_model.py:382-410."""
     view = np.asarray(view, dtype=dt)
     chan = _channel_matrix(geom, pixel_indices, angle, dt, coeff_power)
     columns = np.asarray(chan.T @ view.T, dtype=dt)                             # (N, R)
     if geom.kind == 'parallel':
         return columns
-    return cone_back_vertical(geom, columns, pixel_indices, angle, coeff_power, dt)
+    if geom.kind == 'cone':
+        return cone_back_vertical(geom, columns, pixel_indices, angle, coeff_power, dt)
+    return translation_back_vertical(geom, columns, pixel_indices, angle, coeff_power, dt)
 
 
 def _view_list(geom, view_indices):

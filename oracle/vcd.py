@@ -40,6 +40,8 @@ def auto_regularization(geom, sinogram, weights=None, snr_db=30.0, sharpness=1.0
 
 
 def direct_recon(geom, sinogram):
+    if geom.kind == 'translation':  # no direct recon: the base model's zeros (tomography_model.py:934-949)
+        return np.zeros(geom.recon_shape, dtype=np.float32)
     if geom.kind == 'parallel':
         filtered = fbp_filter(sinogram, geom.delta_voxel)
     else:

@@ -13,13 +13,27 @@ def angles_for(kind, num_views, num_det_channels, sdd):
     return np.linspace(start, end, num_views, endpoint=False).astype(np.float32)
 
 
-def make_case(kind, views=16, rows=8, channels=32, sdd_factor=4.0, sid_factor=None, **params):
+def translations_for(num_views, seed=0, y_spread=0.0):
+    """Translation vectors of the reference's projector tests (tests/test_projectors.py:54-62): x and z uniform
+    in [-10, 10], y = 0 (or uniform in [-y_spread, y_spread])."""
+    rng = np.random.default_rng(seed)
+    tv = np.zeros((num_views, 3))
+    tv[:, 0] = rng.uniform(-10, 10, num_views)
+    tv[:, 1] = rng.uniform(-y_spread, y_spread, num_views) if y_spread else 0.0
+    tv[:, 2] = rng.uniform(-10, 10, num_views)
+    return tv
+
+
+def make_case(kind, views=16, rows=8, channels=32, sdd_factor=4.0, sid_factor=None, y_spread=0.0, **params):
     """Returns (model, oracle_geometry).  params are set on the model before the oracle geometry is derived."""
     sdd = sdd_factor * channels
     sid = sdd if sid_factor is None else sid_factor * channels
     ang = angles_for(kind, views, channels, sdd)
     if kind == 'parallel':
         model = mb.ParallelBeamModel((views, rows, channels), ang)
+    elif kind == 'translation':
+        model = mb.TranslationModel((views, rows, channels), translations_for(views, y_spread=y_spread),
+                                    source_detector_dist=sdd, source_iso_dist=sid)
     else:
         model = mb.ConeBeamModel((views, rows, channels), ang, source_detector_dist=sdd, source_iso_dist=sid)
     if params:
@@ -29,11 +43,15 @@ def make_case(kind, views=16, rows=8, channels=32, sdd_factor=4.0, sid_factor=No
 
 def oracle_geometry(model):
     sino_shape, recon_shape = model.get_params(['sinogram_shape', 'recon_shape'])
-    ang = np.asarray(model.get_params('angles'), dtype=np.float32)
     kw = dict(delta_det_channel=model.get_params('delta_det_channel'), delta_det_row=model.get_params('delta_det_row'),
               det_channel_offset=model.get_params('det_channel_offset'),
               det_row_offset=model.get_params('det_row_offset'), delta_voxel=model.get_params('delta_voxel'),
               recon_shape=recon_shape)
+    if isinstance(model, mb.TranslationModel):
+        return O.translation_geometry(sino_shape, model.get_params('translation_vectors'),
+                                      model.get_params('source_detector_dist'), model.get_params('source_iso_dist'),
+                                      delta_recon_row=model.get_params('delta_recon_row'), **kw)
+    ang = np.asarray(model.get_params('angles'), dtype=np.float32)
     if isinstance(model, mb.ConeBeamModel):
         g = O.cone_geometry(sino_shape, ang, model.get_params('source_detector_dist'),
                             model.get_params('source_iso_dist'), recon_slice_offset=model.get_params('recon_slice_offset'),

@@ -68,6 +68,17 @@ def test_batched_cone_with_weights(cuda):
         assert rel_l2(rec.cpu().numpy(), plain) <= 1e-5
 
 
+def test_batched_rejects_translation_geometry(cuda):
+    # the batched kernels cover parallel and cone beam; translation scans are refused before any launch
+    from cases import make_case
+    model, geom = make_case('translation', views=12, rows=6, channels=24)
+    model.set_params(sharpness=0.0, granularity=[4], partition_sequence=[0], verbose=0)
+    sino = np.random.default_rng(0).random(geom.sinogram_shape).astype(np.float32)
+    with pytest.warns(UserWarning):  # no direct recon for translation geometry: the init is zeros
+        with pytest.raises(mb.MbxError):
+            BatchedVCD([model], [sino], seeds=[0]).recon(max_iterations=1)
+
+
 def test_morton_order_is_a_permutation():
     idx = np.sort(np.random.default_rng(0).choice(64 * 64, 500, replace=False)).astype(np.int32)
     o = morton_order(idx, 64)

@@ -57,7 +57,9 @@ def test_compute_without_gpu_fails_loudly(monkeypatch):
 
 
 @pytest.mark.parametrize('kind,kw', [('parallel', {}), ('cone', {}), ('cone', {'sid_factor': 2.0}),
-                                     ('parallel', {'delta_voxel': 2.5}), ('cone', {'delta_voxel': 3.0})])
+                                     ('parallel', {'delta_voxel': 2.5}), ('cone', {'delta_voxel': 3.0}),
+                                     ('translation', {}), ('translation', {'sid_factor': 2.0}),
+                                     ('translation', {'y_spread': 4.0})])
 def test_geometry_matches_oracle(kind, kw):
     model, geom = make_case(kind, views=8, rows=10, channels=40, **kw)
     gp = model.get_geometry_parameters()
@@ -65,9 +67,35 @@ def test_geometry_matches_oracle(kind, kw):
     if kind == 'cone':
         assert gp.bp_psf_radius == geom.bp_psf_radius
         assert model.get_magnification() == pytest.approx(geom.magnification)
-    # default recon sizes (parallel_beam.py:125-136, cone_beam.py:174-187)
+    # default recon sizes (parallel_beam.py:125-136, cone_beam.py:174-187, translation_model.py:142-186)
     m2, g2 = make_case(kind, views=8, rows=10, channels=40)
     assert tuple(m2.get_params('recon_shape')) == tuple(g2.recon_shape)
+    if kind == 'translation':  # the oracle derives recon size, row pitch and psf radius on its own
+        g3 = O.translation_geometry(m2.get_params('sinogram_shape'), m2.get_params('translation_vectors'),
+                                    m2.get_params('source_detector_dist'), m2.get_params('source_iso_dist'))
+        assert tuple(g3.recon_shape) == tuple(m2.get_params('recon_shape'))
+        assert g3.delta_recon_row == m2.get_params('delta_recon_row')
+        assert g3.psf_radius == m2.get_geometry_parameters().psf_radius
+
+
+def test_translation_model_reference_geometry():
+    """The geometry TranslationModel derives for the reference's VCD test setup (tests/test_vcd.py:27-64:
+    40 rows x 128 channels, source at 512 = detector distance, a 7 x 7 raster of translations 22 ALU apart,
+    one view per translation), worked out by hand from translation_model.py:109-186: half cone angle
+    atan(128 / 1024), row pitch sqrt(2) * 8, a box of (132 + 64) x (132 + 20) voxels,
+    ceil(49 * 128 * 40 / (196 * 152)) = 9 rows."""
+    from mbirjax_b200.utilities import gen_translation_vectors
+    tv = gen_translation_vectors(7, 7, 22, 22)
+    model = mb.TranslationModel((49, 40, 128), tv, source_detector_dist=512, source_iso_dist=512)
+    assert model.get_params('delta_recon_row') == pytest.approx(np.sqrt(2) * 8, rel=1e-6)
+    assert tuple(model.get_params('recon_shape')) == (9, 196, 152)
+    assert model.get_geometry_parameters().psf_radius == 1
+    assert list(model.get_params('qggmrf_nbr_wts')) == [0.5, 1, 1]
+    assert model.use_ror_mask  # reset to True by the base constructor, as in the reference
+    with pytest.raises(ValueError):
+        mb.TranslationModel((48, 40, 128), tv, source_detector_dist=512, source_iso_dist=512)
+    with pytest.raises(ValueError):
+        mb.TranslationModel((49, 40, 128), tv, source_detector_dist=np.inf, source_iso_dist=512)
 
 
 def test_set_params_semantics():
@@ -112,7 +140,7 @@ def test_morton_sorted_partition_keeps_each_subset():
     assert np.mean(np.abs(np.diff(r)) + np.abs(np.diff(c))) < 6.0
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_auto_regularization_matches_oracle(kind):
     model, geom = make_case(kind, views=40, rows=6, channels=32)
     rng = np.random.default_rng(5)

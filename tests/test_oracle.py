@@ -57,7 +57,7 @@ def test_qggmrf_loss_gradient_finite_difference():
     assert np.allclose(g_ref, g_surr.reshape(x.shape))
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_oracle_adjoint_exact_in_float64(kind):
     from cases import make_case
     _, geom = make_case(kind, views=12, rows=6, channels=24)
@@ -71,7 +71,7 @@ def test_oracle_adjoint_exact_in_float64(kind):
     assert abs(np.sum(ax * y) - np.sum(aty * x)) <= 1e-12 * abs(np.sum(ax * y))
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_oracle_hessian_finite_difference(kind):
     # tests/test_projectors.py:264-303
     from cases import make_case
@@ -87,7 +87,7 @@ def test_oracle_hessian_finite_difference(kind):
     assert np.isclose(hess[i, j, k], atax[i, j, k] / 0.01)
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_oracle_view_batching(kind):
     # tests/test_projectors.py:152-198; exact here since the oracle rounds consistently
     from cases import make_case

@@ -27,6 +27,11 @@ CASES = [
     ('cone', dict(views=10, rows=7, channels=27, det_row_offset=0.7, det_channel_offset=-1.1,
                   recon_slice_offset=0.4)),
     ('cone', dict(views=12, rows=10, channels=30, delta_voxel=2.2)),        # psf radius 2
+    ('translation', dict(views=16, rows=8, channels=32)),
+    ('translation', dict(views=12, rows=10, channels=30, sid_factor=2.0)),  # magnification 2
+    ('translation', dict(views=10, rows=7, channels=27, det_row_offset=0.7, det_channel_offset=-1.1,
+                         y_spread=3.0)),
+    ('translation', dict(views=12, rows=10, channels=30, delta_voxel=2.2)),  # psf radius 2
 ]
 
 
@@ -76,7 +81,7 @@ def test_forward_back_parity(cuda, kind, kw):
     assert abs(rhs - ref64) <= TOL * abs(ref64)
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_view_subsets_and_weights(cuda, kind):
     model, geom = make_case(kind, views=15, rows=6, channels=28)
     nr, nc, ns = geom.recon_shape
@@ -97,7 +102,7 @@ def test_view_subsets_and_weights(cuda, kind):
     assert rel_l2(bw, O.sparse_back_project(geom, w * y, idx)) <= TOL
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_view_batching_consistency(cuda, kind):
     # tests/test_projectors.py:152-198: interleaved view subsets reassemble the full projection
     model, geom = make_case(kind, views=24, rows=8, channels=32)
@@ -117,7 +122,7 @@ def test_view_batching_consistency(cuda, kind):
     assert np.abs(parts - bp).max() <= 1e-5 * np.abs(bp).max()
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_hessian_diagonal(cuda, kind):
     model, geom = make_case(kind, views=12, rows=6, channels=24)
     h = model.compute_hessian_diagonal().cpu().numpy()
@@ -135,9 +140,10 @@ def test_hessian_diagonal(cuda, kind):
     assert np.isclose(h[i, j, k], atax[i, j, k] / 0.01, rtol=1e-5)
 
 
-@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_full_projection_reference_test_geometry(cuda, kind):
-    # the reference's projector-test geometry: 64 views, 40 rows, 128 channels, cone sdd = sid = 512
+    # the reference's projector-test geometry: 64 views, 40 rows, 128 channels, cone and translation
+    # sdd = sid = 512
     model, geom = make_case(kind, views=64, rows=40, channels=128)
     rng = np.random.default_rng(2)
     recon = rng.random(geom.recon_shape).astype(np.float32)

@@ -22,7 +22,8 @@ def _phantom_and_sino(model, geom, seed, weights=False):
     return ph, sino.astype(np.float32), w
 
 
-@pytest.mark.parametrize('kind,weighted', [('parallel', False), ('parallel', True), ('cone', False), ('cone', True)])
+@pytest.mark.parametrize('kind,weighted', [('parallel', False), ('parallel', True), ('cone', False), ('cone', True),
+                                           ('translation', True)])
 def test_subset_step_matches_oracle(cuda, kind, weighted):
     model, geom = make_case(kind, views=24, rows=6, channels=40)
     ph, sino, w = _phantom_and_sino(model, geom, 3, weighted)
@@ -61,11 +62,13 @@ def _recon_pair(kind, shape_kw, granularity, iterations, weighted, seed):
                              logfile_path=None, print_logs=False)
     np.random.seed(seed)
     ref, stats = O.vcd.recon(geom, sino, granularity=granularity, partition_sequence=[0], max_iterations=iterations,
-                             weights=w, sharpness=0.0, snr_db=30.0, stop_threshold_change_pct=0)
+                             weights=w, sharpness=0.0, snr_db=30.0, stop_threshold_change_pct=0,
+                             qggmrf_nbr_wts=tuple(model.get_params('qggmrf_nbr_wts')))
     return rec.cpu().numpy(), ref, rdict, stats, ph
 
 
-@pytest.mark.parametrize('kind,weighted', [('parallel', False), ('cone', False), ('cone', True)])
+@pytest.mark.parametrize('kind,weighted', [('parallel', False), ('cone', False), ('cone', True),
+                                           ('translation', False)])
 def test_recon_matches_oracle(cuda, kind, weighted):
     rec, ref, rdict, stats, ph = _recon_pair(kind, dict(views=32, rows=6, channels=48), [4], 5, weighted, 0)
     assert rel_l2(rec, ref) <= 1e-4
