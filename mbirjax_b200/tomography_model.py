@@ -13,10 +13,14 @@ the reference keeps on the host: parameters, partitions (NumPy, same ``np.random
 auto-regularisation statistics and the iteration loop.
 """
 import datetime
+import inspect
+import io
+import warnings
 from collections import namedtuple
 
 import numpy as np
 import torch
+import yaml
 
 from . import _capi
 from .parameter_handler import ParameterHandler
@@ -304,10 +308,88 @@ class TomographyModel(ParameterHandler):
         return self.vcd_recon(sinogram, partitions, partition_sequence, stop_threshold_change_pct, weights=weights,
                               init_recon=init_recon, prox_input=prox_input, first_iteration=first_iteration)
 
-    def get_recon_dict(self, recon_params, notes=''):
-        logs = self.log_buffer.getvalue() if self.log_buffer is not None else ''
-        model_params = {k: v.val for k, v in self.params.items()}
-        return {'recon_params': recon_params, 'notes': notes, 'recon_logs': logs, 'model_params': model_params}
+    # ------------------------------------------------------------------ parameter files and recon dicts
+    @classmethod
+    def get_required_param_names(cls):
+        """Names of the constructor's parameters, in signature order (tomography_model.py:94-115)."""
+        params = inspect.signature(cls.__init__).parameters.values()
+        return [p.name for p in params if p.name != 'self' and
+                p.kind not in (inspect.Parameter.VAR_POSITIONAL, inspect.Parameter.VAR_KEYWORD)]
+
+    @classmethod
+    def from_file(cls, source):
+        """A model of this class from parameters saved by :meth:`to_file` (a .yml/.yaml file name, a YAML string
+        or a stream) (tomography_model.py:296-317)."""
+        required_params, params = ParameterHandler.load_param_dict(source, cls.get_required_param_names(),
+                                                                   values_only=True)
+        with warnings.catch_warnings():
+            warnings.simplefilter("ignore")
+            new_model = cls(**required_params)
+            new_model.set_params(**params)
+        return new_model
+
+    def to_file(self, filename):
+        """Every parameter to a .yml/.yaml file, or the YAML text when filename is None
+        (tomography_model.py:319-331)."""
+        return self.save_params(self.params, filename)
+
+    def get_recon_dict(self, recon_params=None, notes=None, save_log=True, save_model=True, str_format=False):
+        """Dict with 'recon_params', 'recon_log', 'notes' and 'model_params' (the Param dict, or its YAML text
+        when str_format) (tomography_model.py:333-386)."""
+        recon_dict = dict()
+        recon_dict['recon_params'] = "# Recon params not saved." if recon_params is None else recon_params
+        if self.log_buffer is None or not save_log:
+            recon_dict['recon_log'] = "# Log info not saved."
+        else:
+            recon_dict['recon_log'] = self.log_buffer.getvalue()
+        recon_dict['notes'] = '# No notes saved' if notes is None else notes
+        recon_dict['model_params'] = self.params.copy() if save_model else '# Model not saved'
+        if str_format:
+            recon_dict = self.convert_subdicts_to_strings(recon_dict)
+        return recon_dict
+
+    @staticmethod
+    def convert_subdicts_to_strings(recon_dict):
+        """Every entry as a string: model_params as a parameter file, other dicts as YAML, the rest by str()
+        (tomography_model.py:387-410)."""
+        if not isinstance(recon_dict, dict):
+            return recon_dict
+        string_dict = recon_dict.copy()
+        for key, value in string_dict.items():
+            if key == 'model_params' and isinstance(value, dict):
+                string_dict[key] = ParameterHandler.save_params(value)
+            elif isinstance(value, dict):
+                buf = io.StringIO()
+                yaml.safe_dump(_yaml_plain(value), buf, default_flow_style=False, sort_keys=False)
+                string_dict[key] = buf.getvalue()
+            else:
+                try:
+                    string_dict[key] = str(value)
+                except Exception:
+                    raise ValueError('Entries in recon_dict must be strings or dicts that can be converted to strings')
+        return string_dict
+
+    def save_recon_hdf5(self, filepath, recon, recon_dict=None):
+        """One dataset 'recon' with the recon_dict entries as string attributes (tomography_model.py:412-440).
+        Needs h5py."""
+        from .utilities import save_data_hdf5
+        save_data_hdf5(filepath, _to_numpy(recon), 'recon', recon_dict)
+        if self.logger:
+            self.logger.info(f"Saved reconstruction and params to '{filepath}'")
+
+    @staticmethod
+    def load_recon_hdf5(filepath, recreate_model=False):
+        """(recon, recon_dict) from :meth:`save_recon_hdf5`, plus the model rebuilt from its parameters when
+        recreate_model (tomography_model.py:442-473).  Needs h5py."""
+        from .utilities import load_data_hdf5
+        recon, recon_dict = load_data_hdf5(filepath)
+        if not recreate_model:
+            return recon, recon_dict
+        model_yaml = recon_dict['model_params']
+        class_name = model_yaml.split("<class '")[1].split("'>")[0].split(".")[-1]
+        import mbirjax_b200
+        ct_model = getattr(mbirjax_b200, class_name).from_file(model_yaml)
+        return recon, recon_dict, ct_model
 
     def vcd_recon(self, sinogram, partitions, partition_sequence, stop_threshold_change_pct, weights=None,
                   init_recon=None, prox_input=None, compute_prior_loss=False, first_iteration=0):
@@ -420,6 +502,19 @@ class TomographyModel(ParameterHandler):
         new = (int(old_rows * row_scale), int(old_cols * col_scale), int(old_slices * slice_scale))
         self.set_params(recon_shape=new)
         return new[0] - old_rows, new[1] - old_cols, new[2] - old_slices
+
+
+def _yaml_plain(value):
+    """Tuples as lists and NumPy scalars as Python scalars, recursively, for a YAML dump."""
+    if isinstance(value, dict):
+        return {k: _yaml_plain(v) for k, v in value.items()}
+    if isinstance(value, (list, tuple)):
+        return [_yaml_plain(v) for v in value]
+    if isinstance(value, np.generic):
+        return value.item()
+    if isinstance(value, np.ndarray):
+        return value.tolist()
+    return value
 
 
 def _to_numpy(x):

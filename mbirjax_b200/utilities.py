@@ -5,7 +5,12 @@ axis-aligned ellipsoids with centres uniform in the inner 70% of the volume, sem
 voxels and densities uniform in [0.1, 1], summed where they overlap (the same construction as the
 reference's ``add_ellipsoid``, ``utilities.py:856-895``, without rotation).  Generation runs with torch on
 whatever device the caller names (the CPU in tests, the GPU for the large configurations).
+
+Also here: the translation-vector raster of the reference's translation experiments and its HDF5 helpers
+``save_data_hdf5`` / ``load_data_hdf5`` (which need h5py).
 """
+import os
+
 import numpy as np
 import torch
 
@@ -64,3 +69,40 @@ def gen_translation_vectors(num_x_translations, num_z_translations, x_spacing, z
     out[:, 0] = np.tile(x, num_z_translations)
     out[:, 2] = np.repeat(z, num_x_translations)
     return out
+
+
+def _h5py():
+    try:
+        import h5py
+    except ImportError as e:
+        raise ImportError('HDF5 files need the h5py package, which is not installed') from e
+    return h5py
+
+
+def save_data_hdf5(file_path, array, array_name='array', attributes_dict=None):
+    """One dataset holding the array, with the entries of attributes_dict (converted to strings as
+    TomographyModel.convert_subdicts_to_strings does) as its attributes (utilities.py:98-141 of the reference)."""
+    h5py = _h5py()
+    d = os.path.dirname(str(file_path))
+    if d:
+        os.makedirs(d, exist_ok=True)
+    with h5py.File(file_path, 'w') as f:
+        data = f.create_dataset(array_name, data=np.asarray(
+            array.detach().cpu().numpy() if isinstance(array, torch.Tensor) else array))
+        if isinstance(attributes_dict, dict):
+            from .tomography_model import TomographyModel
+            for key, value in TomographyModel.convert_subdicts_to_strings(attributes_dict).items():
+                data.attrs[key] = value
+
+
+def load_data_hdf5(file_path):
+    """(array, attribute dict) from a file written by save_data_hdf5 (utilities.py:27-61 of the reference)."""
+    h5py = _h5py()
+    with h5py.File(file_path, 'r') as f:
+        names = list(f.keys())
+        if len(names) > 1:
+            raise ValueError('More than one array found in {}. Unable to load.'.format(file_path))
+        data = f[names[0]]
+        array = data[()]
+        data_dict = {name: data.attrs[name] for name in data.attrs.keys()}
+    return array, data_dict

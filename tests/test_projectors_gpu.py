@@ -156,6 +156,23 @@ def test_full_projection_reference_test_geometry(cuda, kind):
     assert rel_l2(bp, O.back_project(geom, sino_ref)) <= TOL
 
 
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
+def test_saved_and_loaded_model_projects_the_same(cuda, kind, tmp_path):
+    # tests/test_projectors.py:96-145: A^T A of one pixel cylinder before and after to_file / from_file
+    model, geom = make_case(kind, views=16, rows=8, channels=32)
+    nr, nc, ns = geom.recon_shape
+    idx = np.arange(nr * nc, dtype=np.int32)
+    x = np.zeros((nr * nc, ns), np.float32)
+    x[(nr // 4) * nc + nc // 3, :] = 1
+    aty = model.sparse_back_project(model.sparse_forward_project(x, idx), idx).cpu().numpy()
+    fn = str(tmp_path / 'model.yaml')
+    model.to_file(fn)
+    new = type(model).from_file(fn)
+    assert mb.ParameterHandler.compare_parameter_handlers(model, new)
+    aty_new = new.sparse_back_project(new.sparse_forward_project(x, idx), idx).cpu().numpy()
+    assert np.allclose(aty, aty_new, atol=1e-4)
+
+
 def test_edge_cases(cuda):
     model, geom = make_case('parallel', views=6, rows=4, channels=16)
     ns = geom.recon_shape[2]
