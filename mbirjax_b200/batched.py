@@ -39,10 +39,15 @@ class BatchedVCD:
     def _setup(self, max_iterations):
         scans, schedules, self.states, self.partitions, self.reg = [], [], [], [], []
         num_subsets = None
+        # the auto-regularisation statistics use at most ~20 views of each sinogram on the host: copy those views
+        # of every scan first, so that the per-scan host work below overlaps the GPU setup work queued before it
+        # (subsampling the subsample again selects the same views)
+        small = [_view_subsample(sino) for sino in self.sinograms]
+        small_w = [None if w is None else _view_subsample(w) for w in self.weights]
         for i, model in enumerate(self.models):
             if self.seeds is not None:
                 np.random.seed(int(self.seeds[i]))
-            reg = model.auto_set_regularization_params(self.sinograms[i], weights=self.weights[i])
+            reg = model.auto_set_regularization_params(small[i], weights=small_w[i])
             recon_shape, granularity = model.get_params(['recon_shape', 'granularity'])
             seq = gen_partition_sequence(model.get_params('partition_sequence'), max_iterations)
             if len(set(int(v) for v in seq)) != 1:
@@ -58,7 +63,9 @@ class BatchedVCD:
             schedules.append(np.stack([np.random.permutation(num_subsets) for _ in range(max_iterations)]))
             dev = state['device']
             part = morton_sorted_partition(part, recon_shape[1])  # spatially coherent processing order
-            part_d = torch.as_tensor(part, device=dev, dtype=torch.int32).contiguous()
+            # from pinned memory, so that the copy does not wait for the setup work queued before it
+            part_d = torch.from_numpy(np.ascontiguousarray(part, dtype=np.int32)).pin_memory().to(
+                dev, non_blocking=True)
             rec = _capi.MbxScan()
             rec.geom = model._geometry()
             rec.flat_recon = state['flat_recon'].data_ptr()
@@ -140,3 +147,11 @@ class BatchedVCD:
                           'stop_threshold_change_pct': [100 * float(v) for v in nmae],
                           'alpha_values': [float(v) for v in alphas]})
         return recons, dicts
+
+
+def _view_subsample(x):
+    """The views auto_set_regularization_params reads (tomography_model.py:766-770), on the host."""
+    num_views = x.shape[0]
+    step = num_views // min(20, num_views)
+    sub = x[::step]
+    return sub.cpu().numpy() if isinstance(sub, torch.Tensor) else np.asarray(sub)

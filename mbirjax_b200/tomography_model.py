@@ -47,6 +47,7 @@ class TomographyModel(ParameterHandler):
         super().__init__()
         self._geom = None
         self._angles_dev = None
+        self._full_idx = None
         self.set_params(no_compile=True, no_warning=True, sinogram_shape=tuple(int(v) for v in sinogram_shape),
                         **kwargs)
         if self.get_params('delta_voxel') is None:
@@ -163,19 +164,30 @@ class TomographyModel(ParameterHandler):
         out = _capi.back_project(self._geometry(), sino, pix, views, coeff_power=coeff_power)
         return out.cpu() if output_device == 'cpu' else out
 
+    def _full_indices(self):
+        """gen_full_indices(recon_shape, use_ror_mask) as an int32 device tensor.  The host call runs every time,
+        because it draws from np.random as the reference's does (and so shapes the partitions drawn after it); its
+        result (the sorted region of reconstruction) depends only on the shape and the mask, so the device copy
+        is kept and reused: a host-to-device copy would wait for the GPU work queued before it."""
+        recon_shape = tuple(self.get_params('recon_shape'))
+        idx = gen_full_indices(recon_shape, use_ror_mask=self.use_ror_mask)
+        key = (recon_shape, bool(self.use_ror_mask))
+        if self._full_idx is None or self._full_idx[0] != key:
+            self._full_idx = (key, torch.as_tensor(idx, dtype=torch.int32, device=self._device()))
+        return self._full_idx[1]
+
     def forward_project(self, recon):
-        recon_shape = self.get_params('recon_shape')
-        full_indices = gen_full_indices(recon_shape, use_ror_mask=self.use_ror_mask)
+        full_indices = self._full_indices()
         voxel_values = self.get_voxels_at_indices(recon, full_indices)
         return self.sparse_forward_project(voxel_values, full_indices)
 
     def back_project(self, sinogram):
         recon_shape = self.get_params('recon_shape')
-        full_indices = gen_full_indices(recon_shape, use_ror_mask=self.use_ror_mask)
+        full_indices = self._full_indices()
         cyl = self.sparse_back_project(sinogram, full_indices)
         recon = torch.zeros((recon_shape[0] * recon_shape[1], recon_shape[2]), dtype=torch.float32,
                             device=cyl.device)
-        recon[torch.as_tensor(full_indices, device=cyl.device, dtype=torch.int64)] = cyl
+        recon[full_indices.long()] = cyl
         return recon.reshape(recon_shape)
 
     def compute_hessian_diagonal(self, weights=None, output_device=None):
@@ -468,14 +480,17 @@ class TomographyModel(ParameterHandler):
         if tuple(init.shape) != tuple(recon_shape):
             raise ValueError('init_recon does not have the correct shape. \nExpected {}, but got shape {} for '
                              'init_recon shape.'.format(recon_shape, tuple(init.shape)))
-        # alpha minimising (1/2)||y - alpha A x||_W^2 (tomography_model.py:1137-1152)
+        # alpha minimising (1/2)||y - alpha A x||_W^2 (tomography_model.py:1137-1152), kept on the device (float64
+        # sums, applied in float32) so that setting up queues GPU work without waiting for it
         error_sinogram = self.forward_project(init)
         wes = error_sinogram if w is None else w * error_sinogram
-        norm = float(torch.sum(wes.double() * error_sinogram.double()))
-        alpha = float(torch.sum(wes.double() * sino.double())) / norm if norm > 0 else 1.0
-        error_sinogram = (sino - np.float32(alpha) * error_sinogram).contiguous()
-        flat_recon = (np.float32(alpha) * init).reshape((-1, num_slices)).contiguous()
-        del wes
+        norm = torch.sum(wes.double() * error_sinogram.double())
+        num = torch.sum(wes.double() * sino.double())
+        alpha = torch.where(norm > 0, num / torch.where(norm > 0, norm, torch.ones_like(norm)),
+                            torch.ones_like(norm)).float()
+        error_sinogram = (sino - alpha * error_sinogram).contiguous()
+        flat_recon = (alpha * init).reshape((-1, num_slices)).contiguous()
+        del wes, norm, num
         sigma_y = float(self.get_params('sigma_y'))
         fm_hessian = self.compute_hessian_diagonal(weights=w).reshape((-1, num_slices)).contiguous()
         b, sigma_x, p, q, T = self._qggmrf_params()
