@@ -106,9 +106,20 @@ class BatchedVCD:
                 _capi.vcd_batched_iteration_stats(self.plan, it)
 
         if use_graph:
+            # captured on a side stream that first waits for the setup work; capture_begin / capture_end directly
+            # rather than torch.cuda.graph(), whose entry synchronises, runs the garbage collector and empties the
+            # caching allocator (so that every later allocation goes back to cudaMalloc)
             self.graph = torch.cuda.CUDAGraph()
-            with torch.cuda.graph(self.graph):
-                run_all()
+            main = torch.cuda.current_stream()
+            side = torch.cuda.Stream()
+            side.wait_stream(main)
+            with torch.cuda.stream(side):
+                self.graph.capture_begin()
+                try:
+                    run_all()
+                finally:
+                    self.graph.capture_end()
+            main.wait_stream(side)
             self.graph.replay()
         else:
             run_all()

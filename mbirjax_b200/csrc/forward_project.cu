@@ -232,7 +232,8 @@ static cudaError_t launch_fp_kind(const mbx_geom &g, const FpPlan &pl, const flo
 }
 
 size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel) {
-    if (plan_fp_cb(g).ok && num_pixels * g.num_recon_slices < (1LL << 31)) return fp_chunk_box_bytes(num_pixels);
+    if (plan_fp_cb(g).ok && num_pixels * g.num_recon_slices < (1LL << 31) && num_pixels <= (1LL << 24))
+        return fp_chunk_box_bytes(num_pixels);
     return plan_fp(g, num_pixels, num_views_sel).workspace;
 }
 
@@ -265,7 +266,8 @@ int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, lon
                     cudaStream_t st) {
     CbPlan cand[CB_MAX_CANDIDATES];
     const int ncand = fp_cb_candidates(g, num_views_sel, 4LL * num_sms(), cand);
-    if (ncand > 0 && num_pixels * g.num_recon_slices < (1LL << 31)) {  // 32-bit cylinder offsets
+    // 32-bit cylinder offsets; list positions share a word with the bin
+    if (ncand > 0 && num_pixels * g.num_recon_slices < (1LL << 31) && num_pixels <= (1LL << 24)) {
         FpArgs A;
         A.g = g;
         A.vox = vox;

@@ -55,7 +55,7 @@ struct CbPlan {
     int cblocks;     // channel blocks per view
     int minb;        // resident CTAs per SM the kernel variant is compiled for (2 or 3)
     // shared-memory layout (4-byte words)
-    int o_rec, o_rec2, o_sbin, o_ulist, o_ubin, o_bstart, o_run, o_wcnt, o_wstart, o_cone, o_hl, o_misc;
+    int o_rec, o_rec2, o_sbin, o_ubin, o_bstart, o_run, o_wcnt, o_wstart, o_cone, o_hl, o_misc;
     size_t smem;
     bool ok;
 };
@@ -69,8 +69,6 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
     if (kind == MBX_GEOM_CONE) o += 4 * (size_t)pl.cap;
     pl.o_sbin = (int)o;
     o += pl.cap + CB_PAD;
-    pl.o_ulist = (int)o;
-    o += pl.cap;
     pl.o_ubin = (int)o;
     o += pl.cap;
     pl.o_bstart = (int)o;
@@ -618,8 +616,9 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     float4 *rec = reinterpret_cast<float4 *>(sm + pl.o_rec);    // sorted {cylinder offset (int bits), a0, a1, a2}
     float4 *rec2 = reinterpret_cast<float4 *>(sm + pl.o_rec2);  // cone: sorted {imd, W_r, mdz, mz0}
     int *sbin = reinterpret_cast<int *>(sm + pl.o_sbin);        // bin of each sorted record
-    int *ulist = reinterpret_cast<int *>(sm + pl.o_ulist);      // kept pixel positions, scan order
-    int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // their bin << 24 | pixel index
+    int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // kept pixels, scan order: bin << 24 | key
+                                                                // (key: pixel index when vox is indexed by pixel,
+                                                                // else list position; both < 2^24)
     int *bstart = reinterpret_cast<int *>(sm + pl.o_bstart);    // [nbins + 1] padded start of each bin
     int *run = reinterpret_cast<int *>(sm + pl.o_run);          // [nbins] histogram, then placement cursor
     int *wcnt = reinterpret_cast<int *>(sm + pl.o_wcnt);        // [warps][nbins] per-warp counts of a chunk
@@ -737,8 +736,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             }
             if (take) {
                 const int pos = base + __popc(ballot & ((1u << lane) - 1u));
-                ulist[pos] = (int)p;
-                ubin[pos] = (int)(((unsigned)bin << 24) | (unsigned)idx);
+                ubin[pos] = (int)(((unsigned)bin << 24) | (unsigned)(A.vox_by_index ? idx : (int)p));
                 atomicAdd(run + bin, 1);  // integer histogram: order-independent
             }
             count += total;
@@ -798,14 +796,14 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             __syncthreads();
             if (valid) {
                 const int pos = wstart[warp * nbins + b] + rank;
-                const int p = ulist[i];
-                const int idx = (int)(ub & 0xFFFFFFu);
+                const int key = (int)(ub & 0xFFFFFFu);
+                const int idx = A.vox_by_index ? key : __ldg(A.pix + key);  // checked in the scan
                 float xt, yt;
                 pixel_tilde_fast(g, idx, inv_cols, xt, yt);
                 float a0, a1, a2, imd, wr, mdz, mz0;
                 cb_footprint<KIND>(g, cs, sn, xt, yt, n0 + b - 1, a0, a1, a2, imd, wr, mdz, mz0);
                 // element offset of the pixel's cylinder (the host admits vox buffers of < 2^31 elements)
-                rec[pos] = make_float4(__int_as_float((A.vox_by_index ? idx : p) * num_slices), a0, a1, a2);
+                rec[pos] = make_float4(__int_as_float(key * num_slices), a0, a1, a2);
                 if (KIND == MBX_GEOM_CONE) rec2[pos] = make_float4(imd, wr, mdz, mz0);
                 sbin[pos] = b;
             }

@@ -342,6 +342,7 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
     z.fpp = plan_fp_cb(g);
     if (!z.bpp.ok || !z.fpp.ok) return MBX_ERR_UNSUPPORTED;  // batched path needs the radius-1 kernels
     if ((long long)sc.subset_size * g.num_recon_slices >= (1LL << 31)) return MBX_ERR_UNSUPPORTED;
+    if (sc.subset_size > (1 << 24)) return MBX_ERR_UNSUPPORTED;  // list positions share a word with the bin
     z.ncyl = (long long)sc.subset_size * g.num_recon_slices;
     z.nsino = (long long)g.num_views * g.num_det_rows * g.num_det_channels;
     z.nrecon = (long long)g.num_recon_rows * g.num_recon_cols * g.num_recon_slices;
