@@ -493,12 +493,15 @@ __device__ __forceinline__ void ldg_if(float &v, const float *p, int ok) {
 // the warp below (E0, E1), and only the last two of the final flush with the warp above (E2, E3).
 // (Measured alternatives that ran no faster: sub-groups walking whole bins of their own, which diverge at every
 // bin end; a walk split into edge, guard-free and tail loops.)
-template <int PPW, int RPL>
+template <int PPW, int RPL, int MINB>
 __device__ __forceinline__ void cb_accumulate_par(const FpArgs &A, const CbPass &P, int warp, int lane) {
     const mbx_geom &g = A.g;
     const CbPlan &pl = A.plan;
     constexpr int RL = 32 / PPW;
-    constexpr int U = (CB_LOADS / RPL) > 0 ? (CB_LOADS / RPL) : 1;  // records prefetched per lane
+    // records prefetched per lane: about 16 row loads in flight (the walk is latency-bound), at most 8 records;
+    // the variant for three CTAs per SM (85 registers) keeps CB_LOADS, which it holds without spilling
+    constexpr int LOADS = MINB >= 3 ? CB_LOADS : 16;
+    constexpr int U = (LOADS / RPL) < 1 ? 1 : ((LOADS / RPL) > 8 ? 8 : (LOADS / RPL));
     const int sub = lane / RL, lr = lane % RL;
     const int num_rows = g.num_det_rows, nb = pl.nb, pitch = pl.pitch;
     const int w_lo = P.bstart[P.b_lo], w_hi = P.bstart[P.b_hi];
@@ -604,7 +607,7 @@ __device__ __forceinline__ void cb_accumulate_par(const FpArgs &A, const CbPass 
     }
 }
 
-template <int KIND>
+template <int KIND, int MINB>
 __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) {
     const mbx_geom &g = A.g;
     const CbPlan &pl = A.plan;
@@ -855,18 +858,18 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
         P.s_b0 = s_b0;
         if (KIND == MBX_GEOM_PARALLEL) {
             switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
-                case 9: cb_accumulate_par<1, 1>(A, P, warp, lane); break;
-                case 10: cb_accumulate_par<1, 2>(A, P, warp, lane); break;
-                case 11: cb_accumulate_par<1, 3>(A, P, warp, lane); break;
-                case 12: cb_accumulate_par<1, 4>(A, P, warp, lane); break;
-                case 17: cb_accumulate_par<2, 1>(A, P, warp, lane); break;
-                case 18: cb_accumulate_par<2, 2>(A, P, warp, lane); break;
-                case 19: cb_accumulate_par<2, 3>(A, P, warp, lane); break;
-                case 20: cb_accumulate_par<2, 4>(A, P, warp, lane); break;
-                case 33: cb_accumulate_par<4, 1>(A, P, warp, lane); break;
-                case 34: cb_accumulate_par<4, 2>(A, P, warp, lane); break;
-                case 35: cb_accumulate_par<4, 3>(A, P, warp, lane); break;
-                default: cb_accumulate_par<4, 4>(A, P, warp, lane); break;
+                case 9: cb_accumulate_par<1, 1, MINB>(A, P, warp, lane); break;
+                case 10: cb_accumulate_par<1, 2, MINB>(A, P, warp, lane); break;
+                case 11: cb_accumulate_par<1, 3, MINB>(A, P, warp, lane); break;
+                case 12: cb_accumulate_par<1, 4, MINB>(A, P, warp, lane); break;
+                case 17: cb_accumulate_par<2, 1, MINB>(A, P, warp, lane); break;
+                case 18: cb_accumulate_par<2, 2, MINB>(A, P, warp, lane); break;
+                case 19: cb_accumulate_par<2, 3, MINB>(A, P, warp, lane); break;
+                case 20: cb_accumulate_par<2, 4, MINB>(A, P, warp, lane); break;
+                case 33: cb_accumulate_par<4, 1, MINB>(A, P, warp, lane); break;
+                case 34: cb_accumulate_par<4, 2, MINB>(A, P, warp, lane); break;
+                case 35: cb_accumulate_par<4, 3, MINB>(A, P, warp, lane); break;
+                default: cb_accumulate_par<4, 4, MINB>(A, P, warp, lane); break;
             }
         } else switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
             case 9: cb_accumulate<KIND, 1, 1>(A, P, warp, lane, kconst); break;
@@ -901,7 +904,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
 template <int KIND, int MINB>
 __global__ void __launch_bounds__(CB_THREADS, MINB) fp_cb_kernel(const FpArgs A, int *err) {
     extern __shared__ __align__(16) float smcb[];
-    fp_cb_tile<KIND>(A, blockIdx.x, blockIdx.y, smcb, err);
+    fp_cb_tile<KIND, MINB>(A, blockIdx.x, blockIdx.y, smcb, err);
 }
 
 }  // namespace mbx

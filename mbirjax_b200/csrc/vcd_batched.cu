@@ -145,7 +145,7 @@ __global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(BatchedTables T, int nu
         const int sub = __ldg(T.schedule + step * num_scans + s);
         const int K = T.scans[s].K;
         const int cbs = __ldg(T.fp_cblocks + s);
-        fp_cb_tile<KIND>(T.fpargs[s * K + sub], local / cbs, local % cbs, smf2, err);
+        fp_cb_tile<KIND, MINB>(T.fpargs[s * K + sub], local / cbs, local % cbs, smf2, err);
     }
 }
 
