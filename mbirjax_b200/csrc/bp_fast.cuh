@@ -131,6 +131,19 @@ struct BpArgs {
     BpfPlan plan;
 };
 
+// Parallel-beam gather of one view into the first TS accumulators: three taps at constant offsets from one
+// 32-bit element offset, one detector row per slice (TS = the tile's slice count, so no slot is predicated off).
+template <int TS>
+__device__ __forceinline__ void bpf_gather_rows(float (&acc)[BPF_ST], const float *__restrict__ sino, int o,
+                                                int num_channels, const float4 &fa) {
+#pragma unroll
+    for (int s = 0; s < TS; ++s) {
+        const float *q = sino + o;
+        acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
+        o += num_channels;
+    }
+}
+
 template <int KIND>
 __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf, int *err) {
     const mbx_geom &g = A.g;
@@ -211,21 +224,24 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                     }
                     o += num_channels;
                 }
-            } else if (ns == BPF_ST) {  // full tile: no guards
-#pragma unroll
-                for (int s = 0; s < BPF_ST; ++s) {
-                    const float *q = sino + o;
-                    acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
-                    o += num_channels;
-                }
             } else {
-#pragma unroll
-                for (int s = 0; s < BPF_ST; ++s) {
-                    if (s < ns) {
-                        const float *q = sino + o;
-                        acc[s] = fmaf(fa.y, __ldg(q), fmaf(fa.z, __ldg(q + 1), fmaf(fa.w, __ldg(q + 2), acc[s])));
-                    }
-                    o += num_channels;
+                switch (ns) {  // the same for every lane of the warp (a warp holds one slice tile)
+                    case 1: bpf_gather_rows<1>(acc, sino, o, num_channels, fa); break;
+                    case 2: bpf_gather_rows<2>(acc, sino, o, num_channels, fa); break;
+                    case 3: bpf_gather_rows<3>(acc, sino, o, num_channels, fa); break;
+                    case 4: bpf_gather_rows<4>(acc, sino, o, num_channels, fa); break;
+                    case 5: bpf_gather_rows<5>(acc, sino, o, num_channels, fa); break;
+                    case 6: bpf_gather_rows<6>(acc, sino, o, num_channels, fa); break;
+                    case 7: bpf_gather_rows<7>(acc, sino, o, num_channels, fa); break;
+                    case 8: bpf_gather_rows<8>(acc, sino, o, num_channels, fa); break;
+                    case 9: bpf_gather_rows<9>(acc, sino, o, num_channels, fa); break;
+                    case 10: bpf_gather_rows<10>(acc, sino, o, num_channels, fa); break;
+                    case 11: bpf_gather_rows<11>(acc, sino, o, num_channels, fa); break;
+                    case 12: bpf_gather_rows<12>(acc, sino, o, num_channels, fa); break;
+                    case 13: bpf_gather_rows<13>(acc, sino, o, num_channels, fa); break;
+                    case 14: bpf_gather_rows<14>(acc, sino, o, num_channels, fa); break;
+                    case 15: bpf_gather_rows<15>(acc, sino, o, num_channels, fa); break;
+                    default: bpf_gather_rows<BPF_ST>(acc, sino, o, num_channels, fa); break;
                 }
             }
         } else {

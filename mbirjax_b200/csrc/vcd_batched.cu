@@ -121,9 +121,9 @@ template <int KIND>
 #ifndef MBX_BBP_MIN_BLOCKS
 #define MBX_BBP_MIN_BLOCKS 3  // resident CTAs per SM the batched back projection is compiled for
 #endif
-__global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(BatchedTables T, int num_scans, int step, int total, int *err) {
+__global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(BatchedTables T, int num_scans, int step, int first, int total, int *err) {
     extern __shared__ __align__(16) float smb[];
-    for (int t = fetch_tile(T.counters); t < total; t = fetch_tile(T.counters)) {
+    for (int t = first + fetch_tile(T.counters); t < total; t = first + fetch_tile(T.counters)) {
         const int k = find_scan(T.bp_off, num_scans, t);
         const int s = __ldg(T.bp_scan + k);
         const int local = t - __ldg(T.bp_off + k);
@@ -136,9 +136,9 @@ __global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(BatchedT
 
 // MINB: resident CTAs per SM the variant is compiled for (2 or 3, matching the plans' fp_cb minb).
 template <int KIND, int MINB>
-__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(BatchedTables T, int num_scans, int step, int total, int *err) {
+__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(BatchedTables T, int num_scans, int step, int first, int total, int *err) {
     extern __shared__ __align__(16) float smf2[];
-    for (int t = fetch_tile(T.counters + 1); t < total; t = fetch_tile(T.counters + 1)) {
+    for (int t = first + fetch_tile(T.counters + 1); t < total; t = first + fetch_tile(T.counters + 1)) {
         const int k = find_scan(T.fp_off, num_scans, t);
         const int s = __ldg(T.fp_scan + k);
         const int local = t - __ldg(T.fp_off + k);
@@ -504,65 +504,211 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
     return MBX_OK;
 }
 
-// Autotuning of the back-projection stage: staged (shared-memory) footprints, the tables as built, against
-// per-thread footprints computed in registers (same tiles and work list).  Timed on step 0 (the stage only
-// writes the scans' back-projection scratch) and cached per batch shape like the forward stage.
+// Per-scan lane layout of the forward-projection stage, after the kernel variant is chosen: each scan is timed
+// alone on step 0 with its plan and with the best layout that has another number of sub-groups per warp (same
+// channel blocks, so the same tiles), and keeps the faster.  Cached per batch shape.
+static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, int num_scans,
+                                   const int *o_fp, const int *scan_of, cudaStream_t st) {
+    const int K = scans[0].num_subsets;  // every scan of a batch has the same number of subsets
+    const int ksum = K * num_scans;
+    char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
+    std::vector<FpArgs> cur(ksum);
+    cudaError_t e = cudaMemcpyAsync(cur.data(), base + L.fpargs, sizeof(FpArgs) * ksum, cudaMemcpyDeviceToHost, st);
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    const std::vector<FpArgs> orig = cur;
+    std::vector<FpArgs> alt = cur;
+    std::vector<char> can(num_scans, 0);
+    size_t smem_alt = 0;
+    for (int sc = 0; sc < num_scans; ++sc) {
+        const CbPlan &c0 = orig[sc * K].plan;
+        const CbPlan q = plan_fp_cb(scans[sc].geom, 0, 0, c0.minb, c0.nb, c0.ppw);
+        if (!q.ok || q.nb != c0.nb || q.cblocks != c0.cblocks || q.minb != c0.minb) continue;
+        can[sc] = 1;
+        for (int j = 0; j < K; ++j) alt[sc * K + j].plan = q;
+        smem_alt = std::max(smem_alt, q.smem);
+    }
+    std::vector<long long> key = {5, P.kind, num_scans, P.fp_minb, -1};
+    for (int sc = 0; sc < num_scans; ++sc) {
+        const mbx_geom &g = scans[sc].geom;
+        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
+                               g.num_recon_slices, scans[sc].num_subsets, scans[sc].subset_size});
+    }
+    auto use = [&](int sc, int c) {
+        for (int j = 0; j < K; ++j) cur[sc * K + j] = c ? alt[sc * K + j] : orig[sc * K + j];
+    };
+    auto upload = [&]() -> cudaError_t {
+        cudaError_t e2 = cudaMemcpyAsync(base + L.fpargs, cur.data(), sizeof(FpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        return e2 == cudaSuccess ? cudaStreamSynchronize(st) : e2;
+    };
+    auto apply_smem = [&]() {
+        size_t sm = 0;
+        for (int k = 0; k < ksum; ++k) sm = std::max(sm, cur[k].plan.smem);
+        P.fp_smem = sm;
+        if (P.kind == MBX_GEOM_PARALLEL)
+            P.fp_grid = P.fp_minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 3>, sm, P.fp_total)
+                                       : occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, sm, P.fp_total);
+        else
+            P.fp_grid = P.fp_minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, sm, P.fp_total)
+                                       : occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, sm, P.fp_total);
+    };
+    bool all_cached = true;
+    std::vector<int> choice(num_scans, 0);
+    for (int sc = 0; sc < num_scans; ++sc) {
+        if (!can[sc]) continue;
+        if (autotune_forced() >= 0) {
+            choice[sc] = autotune_forced() >= 1 ? 1 : 0;
+        } else {
+            key[4] = sc;
+            const int c = autotune_lookup(key.data(), (int)key.size());
+            if (c < 0) all_cached = false;
+            choice[sc] = c == 1 ? 1 : 0;
+        }
+    }
+    if (all_cached || autotune_forced() >= 0 || stream_is_capturing(st)) {
+        for (int sc = 0; sc < num_scans; ++sc) use(sc, choice[sc]);
+        e = upload();
+        if (e != cudaSuccess) return set_cuda_error(e);
+        apply_smem();
+        return MBX_OK;
+    }
+    P.fp_smem = std::max(P.fp_smem, smem_alt);  // tuning launches fit either plan
+    int *err = device_error_ptr();
+    for (int k = 0; k < num_scans; ++k) {
+        const int sc = scan_of[num_scans + k];
+        if (!can[sc]) continue;
+        const int first = o_fp[k], last = o_fp[k + 1];
+        const int grid = std::min(P.fp_grid, last - first);
+        auto run = [&]() -> cudaError_t {
+            cudaError_t e2 = cudaMemsetAsync(P.t.counters + 1, 0, sizeof(int), st);
+            if (e2 != cudaSuccess) return e2;
+            if (P.kind == MBX_GEOM_PARALLEL) {
+                if (P.fp_minb >= 3)
+                    b_fp<MBX_GEOM_PARALLEL, 3><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
+                else
+                    b_fp<MBX_GEOM_PARALLEL, 2><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
+            } else {
+                if (P.fp_minb >= 3)
+                    b_fp<MBX_GEOM_CONE, 3><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
+                else
+                    b_fp<MBX_GEOM_CONE, 2><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
+            }
+            note_launch();
+            return cudaGetLastError();
+        };
+        float t[2] = {0.0f, 0.0f};
+        for (int c = 0; c < 2; ++c) {
+            use(sc, c);
+            e = upload();
+            if (e == cudaSuccess) e = time_on_stream(run, st, t[c]);
+            if (e != cudaSuccess) return set_cuda_error(e);
+        }
+        choice[sc] = t[1] < t[0] ? 1 : 0;
+        use(sc, choice[sc]);
+        key[4] = sc;
+        autotune_store(key.data(), (int)key.size(), choice[sc]);
+    }
+    e = upload();
+    if (e != cudaSuccess) return set_cuda_error(e);
+    apply_smem();
+    return MBX_OK;
+}
+
+// Autotuning of the back-projection stage, per scan: staged (shared-memory) footprints, the tables as built,
+// against per-thread footprints computed in registers (same tiles).  Each scan is timed alone on step 0 (the
+// launch walks only that scan's tiles; the stage only writes the scans' back-projection scratch), so that every
+// scan keeps the plan that suits its shape, as the plain path's per-call tuner would choose.  The choices are
+// cached per batch shape.
 static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, int num_scans,
-                           const BpArgs *hb1, cudaStream_t st) {
-    int ksum = 0;
-    for (int s = 0; s < num_scans; ++s) ksum += scans[s].num_subsets;
-    std::vector<BpArgs> b2(hb1, hb1 + ksum);
-    size_t smem2 = 0;
+                           const BpArgs *hb1, const int *o_bp, const int *scan_of, cudaStream_t st) {
+    const int K = scans[0].num_subsets;  // every scan of a batch has the same number of subsets
+    const int ksum = K * num_scans;
+    std::vector<BpArgs> cur(hb1, hb1 + ksum), alt(hb1, hb1 + ksum);
+    std::vector<char> can(num_scans, 1);
+    size_t smem_alt = 0;
     for (int k = 0; k < ksum; ++k) {
-        const BpfPlan q = plan_bp_fast(b2[k].g, b2[k].num_pixels, b2[k].g.num_views, 1);
-        if (!q.ok || q.gx != b2[k].plan.gx || q.gy != b2[k].plan.gy || q.splits != 1) return MBX_OK;
-        b2[k].plan = q;
-        smem2 = std::max(smem2, q.smem);
+        const BpfPlan q = plan_bp_fast(alt[k].g, alt[k].num_pixels, alt[k].g.num_views, 1);
+        if (!q.ok || q.gx != alt[k].plan.gx || q.gy != alt[k].plan.gy || q.splits != 1) {
+            can[k / K] = 0;
+            continue;
+        }
+        alt[k].plan = q;
+        smem_alt = std::max(smem_alt, q.smem);
     }
     char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
-    std::vector<long long> key = {4, P.kind, num_scans};
+    std::vector<long long> key = {4, P.kind, num_scans, -1};
     for (int s = 0; s < num_scans; ++s) {
         const mbx_geom &g = scans[s].geom;
         key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
                                g.num_recon_slices, scans[s].num_subsets, scans[s].subset_size,
                                scans[s].weights ? 1 : 0});
     }
-    auto use_inline = [&]() -> int {
-        cudaError_t e = cudaMemcpyAsync(base + L.bpargs, b2.data(), sizeof(BpArgs) * ksum, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return set_cuda_error(e);
-        P.bp_smem = smem2;
-        P.bp_grid = (P.kind == MBX_GEOM_PARALLEL) ? occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, smem2, P.bp_total)
-                                                  : occupancy_grid(b_bp<MBX_GEOM_CONE>, smem2, P.bp_total);
-        return MBX_OK;
+    auto upload = [&]() -> cudaError_t {
+        cudaError_t e = cudaMemcpyAsync(base + L.bpargs, cur.data(), sizeof(BpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
     };
-    const int cached = autotune_forced() >= 0 ? (autotune_forced() >= 1 ? 1 : 0)
-                                              : autotune_lookup(key.data(), (int)key.size());
-    if (cached == 0) return MBX_OK;
-    if (cached == 1) return use_inline();
-    if (stream_is_capturing(st)) return MBX_OK;
-    int rc = MBX_OK;
-    auto run = [&]() {
-        rc = launch_stage(&P, 0, 0, st);
-        return rc == MBX_OK ? cudaSuccess : cudaErrorLaunchFailure;
+    auto apply_smem = [&]() {
+        size_t sm = 0;
+        for (int k = 0; k < ksum; ++k) sm = std::max(sm, cur[k].plan.smem);
+        P.bp_smem = sm;
+        P.bp_grid = (P.kind == MBX_GEOM_PARALLEL) ? occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, sm, P.bp_total)
+                                                  : occupancy_grid(b_bp<MBX_GEOM_CONE>, sm, P.bp_total);
     };
-    float t0 = 0.0f, t1 = 0.0f;
-    cudaError_t e = time_on_stream(run, st, t0);
-    if (rc != MBX_OK) return rc;
-    if (e != cudaSuccess) return set_cuda_error(e);
-    const BatchedPlanHost keep = P;
-    rc = use_inline();
-    if (rc != MBX_OK) return rc;
-    e = time_on_stream(run, st, t1);
-    if (rc != MBX_OK) return rc;
-    if (e != cudaSuccess) return set_cuda_error(e);
-    autotune_store(key.data(), (int)key.size(), t0 <= t1 ? 0 : 1);
-    if (t0 <= t1) {
-        P = keep;
-        e = cudaMemcpyAsync(base + L.bpargs, hb1, sizeof(BpArgs) * ksum, cudaMemcpyHostToDevice, st);
-        if (e == cudaSuccess) e = cudaStreamSynchronize(st);
-        if (e != cudaSuccess) return set_cuda_error(e);
+    auto use = [&](int s, int c) {
+        for (int j = 0; j < K; ++j) cur[s * K + j] = c ? alt[s * K + j] : hb1[s * K + j];
+    };
+    bool all_cached = true;
+    std::vector<int> choice(num_scans, 0);
+    for (int s = 0; s < num_scans; ++s) {
+        if (!can[s]) continue;
+        if (autotune_forced() >= 0) {
+            choice[s] = autotune_forced() >= 1 ? 1 : 0;
+        } else {
+            key[3] = s;
+            const int c = autotune_lookup(key.data(), (int)key.size());
+            if (c < 0) all_cached = false;
+            choice[s] = c == 1 ? 1 : 0;
+        }
     }
+    if (all_cached || autotune_forced() >= 0 || stream_is_capturing(st)) {
+        for (int s = 0; s < num_scans; ++s) use(s, can[s] ? choice[s] : 0);
+        cudaError_t e = upload();
+        if (e != cudaSuccess) return set_cuda_error(e);
+        apply_smem();
+        return MBX_OK;
+    }
+    P.bp_smem = std::max(P.bp_smem, smem_alt);  // tuning launches fit either plan
+    int *err = device_error_ptr();
+    for (int k = 0; k < num_scans; ++k) {
+        const int s = scan_of[k];
+        if (!can[s]) continue;
+        const int first = o_bp[k], last = o_bp[k + 1];
+        const int grid = std::min(P.bp_grid, last - first);
+        auto run = [&]() -> cudaError_t {
+            cudaError_t e = cudaMemsetAsync(P.t.counters, 0, sizeof(int), st);
+            if (e != cudaSuccess) return e;
+            if (P.kind == MBX_GEOM_PARALLEL)
+                b_bp<MBX_GEOM_PARALLEL><<<grid, BPF_THREADS, P.bp_smem, st>>>(P.t, num_scans, 0, first, last, err);
+            else
+                b_bp<MBX_GEOM_CONE><<<grid, BPF_THREADS, P.bp_smem, st>>>(P.t, num_scans, 0, first, last, err);
+            note_launch();
+            return cudaGetLastError();
+        };
+        float t[2] = {0.0f, 0.0f};
+        for (int c = 0; c < 2; ++c) {
+            use(s, c);
+            cudaError_t e = upload();
+            if (e == cudaSuccess) e = time_on_stream(run, st, t[c]);
+            if (e != cudaSuccess) return set_cuda_error(e);
+        }
+        choice[s] = t[1] < t[0] ? 1 : 0;
+        use(s, choice[s]);
+        key[3] = s;
+        autotune_store(key.data(), (int)key.size(), choice[s]);
+    }
+    cudaError_t e = upload();
+    if (e != cudaSuccess) return set_cuda_error(e);
+    apply_smem();
     return MBX_OK;
 }
 
@@ -771,7 +917,8 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     if (e != cudaSuccess) return set_cuda_error(e);
     if (autotune_enabled()) {  // (also in forced mode: the tune functions then apply the forced choice)
         int rc2 = tune_batched_fp(P, L, zs, scans, num_scans, hf, st);
-        if (rc2 == MBX_OK) rc2 = tune_batched_bp(P, L, scans, num_scans, hb, st);
+        if (rc2 == MBX_OK) rc2 = tune_batched_fp_layouts(P, L, scans, num_scans, o_fp, hscan_of, st);
+        if (rc2 == MBX_OK) rc2 = tune_batched_bp(P, L, scans, num_scans, hb, o_bp, hscan_of, st);
         if (rc2 != MBX_OK) return rc2;
     }
     P.magic = BT_MAGIC;
@@ -798,9 +945,9 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
                 if (me != cudaSuccess) return set_cuda_error(me);
             }
             if (P->kind == MBX_GEOM_PARALLEL)
-                b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
+                b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, 0, P->bp_total, err);
             else
-                b_bp<MBX_GEOM_CONE><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, P->bp_total, err);
+                b_bp<MBX_GEOM_CONE><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, 0, P->bp_total, err);
             break;
         case 1: b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err); break;
         case 2:
@@ -810,14 +957,14 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
             }
             if (P->kind == MBX_GEOM_PARALLEL) {
                 if (P->fp_minb >= 3)
-                    b_fp<MBX_GEOM_PARALLEL, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+                    b_fp<MBX_GEOM_PARALLEL, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
                 else
-                    b_fp<MBX_GEOM_PARALLEL, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+                    b_fp<MBX_GEOM_PARALLEL, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
             } else {
                 if (P->fp_minb >= 3)
-                    b_fp<MBX_GEOM_CONE, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+                    b_fp<MBX_GEOM_CONE, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
                 else
-                    b_fp<MBX_GEOM_CONE, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, P->fp_total, err);
+                    b_fp<MBX_GEOM_CONE, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
             }
             break;
         case 3: b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;
