@@ -71,6 +71,8 @@ def parse_args():
     ap.add_argument('--scans', type=int, default=None,
                     help='batched workload: the first N scans only (a small case for profiling; default 24)')
     ap.add_argument('--iterations', type=int, default=None, help='VCD iterations per scan (default 10 / 20 / 15)')
+    ap.add_argument('--autotune', type=int, default=1, choices=[0, 1],
+                    help='1: tune the projector plans (default); 0: default plans, no tuning launches (for profiling)')
     args = ap.parse_args()
     if args.scans is not None:
         BATCH['num_scans'] = args.scans
@@ -561,6 +563,7 @@ def run_gpu(args):
     world, rank, local = dist_setup(args.gpus)
     device = torch.device('cuda', local)
     lib = _capi.load_library()
+    _capi.set_autotune(args.autotune)
     peak_gbs, peak_kind = load_peaks()
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
