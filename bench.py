@@ -170,7 +170,9 @@ def max_over_ranks(value, world):
         return value
     import torch
     import torch.distributed as dist
-    t = torch.tensor([value], dtype=torch.float64, device='cuda')
+    # the NCCL group reduces device tensors; a gloo group (the CPU tests of this logic) host tensors
+    device = 'cuda' if dist.get_backend() == 'nccl' else 'cpu'
+    t = torch.tensor([value], dtype=torch.float64, device=device)
     dist.all_reduce(t, op=dist.ReduceOp.MAX)
     return float(t.item())
 
