@@ -55,9 +55,25 @@ def gen_partition_sequence(partition_sequence, max_iterations):
     return seq[:max_iterations]
 
 
+_FULL_INDICES = {}  # (rows, cols, use_ror_mask) -> sorted region of reconstruction
+
+
 def gen_full_indices(recon_shape, use_ror_mask=True):
-    """All pixels of the region of reconstruction, sorted (vcd_utils.py:310-318)."""
-    return gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask)[0]
+    """All pixels of the region of reconstruction, sorted (vcd_utils.py:310-318).
+
+    The reference draws them as a one-subset partition: a permutation of the N pixels (and an empty choice) from
+    the global np.random stream, then a sort, so the result is always the same sorted set while the stream
+    advances by one permutation of N.  After the first call for a grid, this returns a copy of the kept set and
+    advances the stream by shuffling N scratch entries, which draws exactly what that permutation draws."""
+    key = (int(recon_shape[0]), int(recon_shape[1]), bool(use_ror_mask))
+    hit = _FULL_INDICES.get(key)
+    if hit is None:
+        idx = gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask)[0]
+        _FULL_INDICES[key] = (idx, np.empty(len(idx), dtype=np.int32))
+        return idx.copy()
+    idx, scratch = hit
+    np.random.shuffle(scratch)
+    return idx.copy()
 
 
 def morton_order(pixel_indices, num_cols):
@@ -78,10 +94,33 @@ def morton_order(pixel_indices, num_cols):
     return np.argsort(code, kind='stable').astype(np.int32)
 
 
+_ZORDER_GRIDS = {}  # (rows rounded up to 64, cols) -> (every pixel of that grid in Z-order, its Z-order rank)
+
+
+def _zorder_grid(num_rows, num_cols):
+    key = (-(-num_rows // 64) * 64, num_cols)
+    hit = _ZORDER_GRIDS.get(key)
+    if hit is None:
+        allpix = np.arange(key[0] * key[1], dtype=np.int32)
+        z = allpix[morton_order(allpix, num_cols)]
+        rank = np.empty(z.size, dtype=np.int32)
+        rank[z] = np.arange(z.size, dtype=np.int32)
+        hit = _ZORDER_GRIDS[key] = (z, rank)
+    return hit
+
+
 def morton_sorted_partition(partition, num_cols):
     """Each subset (row) of a partition reordered by the Z-order code of its pixels.  A subset is a set: the
     VCD update does not depend on the order of its pixels, but the projectors run faster when consecutive
     pixels are close in the image (fewer sectors per gather, and whole chunks of the list can be skipped by
-    the channel blocks of the forward projector they cannot reach)."""
+    the channel blocks of the forward projector they cannot reach).
+
+    Every pixel's rank in the Z-order of its grid is computed once per grid size; a subset is then its sorted
+    ranks mapped back to pixels (the codes are distinct, so this is the order of sorting by code)."""
     partition = np.asarray(partition)
-    return np.stack([p[morton_order(p, num_cols)] for p in partition]).astype(np.int32)
+    if partition.size == 0:
+        return partition.astype(np.int32)
+    if partition.min() < 0:
+        return np.stack([p[morton_order(p, num_cols)] for p in partition]).astype(np.int32)
+    z, rank = _zorder_grid(int(partition.max()) // num_cols + 1, num_cols)
+    return z[np.sort(rank[partition], axis=1)].astype(np.int32)

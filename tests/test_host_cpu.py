@@ -140,6 +140,37 @@ def test_morton_sorted_partition_keeps_each_subset():
     assert np.mean(np.abs(np.diff(r)) + np.abs(np.diff(c))) < 6.0
 
 
+def test_zorder_sort_matches_sorting_by_code():
+    # the cached rank-table sort gives the order of sorting each subset by its Morton code, repeats included
+    from mbirjax_b200.vcd_utils import morton_order, morton_sorted_partition
+    for shape, k in (((61, 45, 2), 5), ((96, 512, 1), 3), ((5, 7, 1), 2)):
+        np.random.seed(4)
+        part = mb.gen_pixel_partition(shape, k)
+        want = np.stack([p[morton_order(p, shape[1])] for p in part])
+        np.testing.assert_array_equal(morton_sorted_partition(part, shape[1]), want)
+    rep = np.array([[3, 3, 1, 8], [2, 5, 7, 0]], dtype=np.int32)
+    np.testing.assert_array_equal(morton_sorted_partition(rep, 4),
+                                  np.stack([p[morton_order(p, 4)] for p in rep]))
+
+
+def test_full_indices_draw_as_a_one_subset_partition():
+    # repeated calls return the sorted region of reconstruction and leave np.random where the reference's
+    # one-subset partition (a permutation of N) leaves it, so later partitions are the reference's
+    for shape, mask in (((40, 40, 3), True), ((17, 23, 2), False)):
+        for seed in (0, 1):
+            np.random.seed(seed)
+            a = [O.gen_full_indices(shape, mask) for _ in range(3)]
+            after_oracle = np.random.permutation(10)
+            np.random.seed(seed)
+            b = [mb.gen_full_indices(shape, mask) for _ in range(3)]
+            after = np.random.permutation(10)
+            for x, y in zip(a, b):
+                np.testing.assert_array_equal(x, y)
+            np.testing.assert_array_equal(after, after_oracle)
+    b[0][0] = -1  # results are copies: the kept set is not changed by a caller
+    np.testing.assert_array_equal(mb.gen_full_indices((17, 23, 2), False), a[0])
+
+
 @pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
 def test_auto_regularization_matches_oracle(kind):
     model, geom = make_case(kind, views=40, rows=6, channels=32)
