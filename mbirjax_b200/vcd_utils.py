@@ -56,6 +56,14 @@ def gen_partition_sequence(partition_sequence, max_iterations):
 
 
 _FULL_INDICES = {}  # (rows, cols, use_ror_mask) -> sorted region of reconstruction
+_CACHE_GRIDS = 16    # grid sizes each host cache keeps (the oldest entry goes first)
+
+
+def _cache_put(cache, key, value):
+    if len(cache) >= _CACHE_GRIDS:
+        cache.pop(next(iter(cache)))
+    cache[key] = value
+    return value
 
 
 def gen_full_indices(recon_shape, use_ror_mask=True):
@@ -69,7 +77,7 @@ def gen_full_indices(recon_shape, use_ror_mask=True):
     hit = _FULL_INDICES.get(key)
     if hit is None:
         idx = gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask)[0]
-        _FULL_INDICES[key] = (idx, np.empty(len(idx), dtype=np.int32))
+        _cache_put(_FULL_INDICES, key, (idx, np.empty(len(idx), dtype=np.int32)))
         return idx.copy()
     idx, scratch = hit
     np.random.shuffle(scratch)
@@ -105,7 +113,7 @@ def _zorder_grid(num_rows, num_cols):
         z = allpix[morton_order(allpix, num_cols)]
         rank = np.empty(z.size, dtype=np.int32)
         rank[z] = np.arange(z.size, dtype=np.int32)
-        hit = _ZORDER_GRIDS[key] = (z, rank)
+        hit = _cache_put(_ZORDER_GRIDS, key, (z, rank))
     return hit
 
 
