@@ -140,6 +140,22 @@ def test_morton_sorted_partition_keeps_each_subset():
     assert np.mean(np.abs(np.diff(r)) + np.abs(np.diff(c))) < 6.0
 
 
+def test_prefetched_regularisation_views_give_the_same_statistics():
+    # the batched set-up hands auto_set_regularization_params the ~20 views it reads (copied to the host up
+    # front); subsampling that subsample again selects every view of it, so the statistics are the same
+    import torch
+    from mbirjax_b200.batched import _view_subsample
+    for views in (7, 20, 39, 40, 123, 720):
+        model, _ = make_case('parallel', views=views, rows=4, channels=24)
+        rng = np.random.default_rng(views)
+        sino = rng.random(model.get_params('sinogram_shape')).astype(np.float32)
+        w = rng.random(model.get_params('sinogram_shape')).astype(np.float32)
+        full = model.auto_set_regularization_params(sino, weights=w)
+        sub = model.auto_set_regularization_params(_view_subsample(torch.as_tensor(sino)),
+                                                   weights=_view_subsample(w))
+        assert sub == full
+
+
 def test_zorder_sort_matches_sorting_by_code():
     # the cached rank-table sort gives the order of sorting each subset by its Morton code, repeats included
     from mbirjax_b200.vcd_utils import morton_order, morton_sorted_partition
