@@ -75,6 +75,8 @@ typedef struct mbx_geom {
     const float *angles;                 /* parallel / cone: device pointer, num_views angles in radians */
     float delta_recon_row;               /* translation only: recon row pitch along the source axis (ALU) */
     const float *translations;           /* translation only: device pointer, num_views x 3 (tx, ty, tz) in ALU */
+    float max_magnification;             /* translation only: an upper bound of the pixel magnification over all
+                                            pixels and views (0: unknown; the general kernels are used) */
 } mbx_geom;
 
 /* qGGMRF prior parameters (b, sigma_x, p, q, T) as TomographyModel.create_vcd_subset_updater builds them

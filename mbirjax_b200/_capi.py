@@ -29,7 +29,7 @@ class MbxGeom(ctypes.Structure):
                 ('delta_det_channel', c_float), ('delta_det_row', c_float), ('det_channel_offset', c_float),
                 ('det_row_offset', c_float), ('delta_voxel', c_float), ('recon_slice_offset', c_float),
                 ('source_detector_dist', c_float), ('magnification', c_float), ('angles', c_void_p),
-                ('delta_recon_row', c_float), ('translations', c_void_p)]
+                ('delta_recon_row', c_float), ('translations', c_void_p), ('max_magnification', c_float)]
 
 
 class MbxQggmrfParams(ctypes.Structure):

@@ -4,9 +4,9 @@
 // ParallelBeamModel.back_project_one_view_to_pixel_batch (parallel_beam.py:180-221),
 // ConeBeamModel.back_project_one_view_to_pixel_batch (cone_beam.py:379-541) and
 // TranslationModel.back_project_one_view_to_pixel_batch (translation_model.py:382-542); coeff_power = 2 gives
-// the Hessian diagonal of TomographyModel.compute_hessian_diagonal (tomography_model.py:679-708).  Parallel
-// and cone beam run bp_fast.cuh when its plan fits; translation geometry and the other cases run the general
-// kernel of back_project.cuh, described here.
+// the Hessian diagonal of TomographyModel.compute_hessian_diagonal (tomography_model.py:679-708).  Radius-1
+// geometries run bp_fast.cuh when its plan fits (translation geometry when the caller gives a magnification
+// bound); the other cases run the general kernel of back_project.cuh, described here.
 //
 // One thread owns one pixel and a tile of ST slices.  Its ST accumulators stay in registers across all
 // views, so there are no global atomics and no per-view partial cylinders.  Lanes run along pixels, so the
@@ -75,11 +75,16 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
         const long long stride = num_pixels * (long long)g.num_recon_slices;
         const long long ss = fpl.splits > 1 ? stride : 0;
         auto run = [&](const BpfPlan &pl) -> cudaError_t {
-            cudaError_t e = (g.kind == MBX_GEOM_PARALLEL)
-                                ? launch_bp_fast<MBX_GEOM_PARALLEL>(g, pl, sino, w, pix, num_pixels, views, num_views_sel,
-                                                                    coeff_power, scale, dst, ss, st)
-                                : launch_bp_fast<MBX_GEOM_CONE>(g, pl, sino, w, pix, num_pixels, views, num_views_sel,
-                                                                coeff_power, scale, dst, ss, st);
+            cudaError_t e;
+            if (g.kind == MBX_GEOM_PARALLEL)
+                e = launch_bp_fast<MBX_GEOM_PARALLEL>(g, pl, sino, w, pix, num_pixels, views, num_views_sel,
+                                                      coeff_power, scale, dst, ss, st);
+            else if (g.kind == MBX_GEOM_CONE)
+                e = launch_bp_fast<MBX_GEOM_CONE>(g, pl, sino, w, pix, num_pixels, views, num_views_sel, coeff_power,
+                                                  scale, dst, ss, st);
+            else
+                e = launch_bp_fast<MBX_GEOM_TRANSLATION>(g, pl, sino, w, pix, num_pixels, views, num_views_sel,
+                                                         coeff_power, scale, dst, ss, st);
             if (e != cudaSuccess) return e;
             if (pl.splits > 1) {
                 launch_split_sum(dst, stride, pl.splits, scale, out, stride, st);

@@ -52,13 +52,34 @@ struct BpfPlan {
 // first, first+1, first+2; fb (cone) = {A0, A1, c2 = (mag/D)^2, 0}.
 template <int KIND>
 __device__ __forceinline__ void bpf_footprint(const mbx_geom &g, float cs, float sn, float x_tilde, float y_tilde,
-                                              int coeff_power, float4 &fa, float4 &fb) {
+                                              int coeff_power, float4 &fa, float4 &fb, float tz = 0.0f) {
     const float inv_dc = 1.0f / g.delta_det_channel;
     const int num_channels = g.num_det_channels;
     const float det_center_channel = 0.5f * (float)(num_channels - 1);
     float n_p, w, scale;  // scale = delta_voxel / cos_alpha
     fb = make_float4(0.f, 0.f, 0.f, 0.f);
-    if (KIND == MBX_GEOM_PARALLEL) {
+    if (KIND == MBX_GEOM_TRANSLATION) {
+        // (cs, sn) carry the view's (tx, ty); no rotation (translation_model.py:595-656).  Coefficient
+        // L / cos(theta_p), no delta_voxel factor; the vertical fan is the cone's with slice heights
+        // delta_voxel k + z0v, z0v = -tz - delta_voxel (S-1)/2, which fb.w carries.
+        const float x_p = x_tilde - cs;
+        const float y_p = y_tilde - sn;
+        const float inv_d = 1.0f / g.source_detector_dist;
+        const float mag = 1.0f / (1.0f / g.magnification - y_p * inv_d);
+        const float u = mag * x_p;
+        n_p = (u + g.det_channel_offset) * inv_dc + det_center_channel;
+        const float t = u * inv_d;
+        const float cos_tp = rsqrtf(fmaf(t, t, 1.0f));
+        w = mag * (g.delta_voxel * inv_dc);
+        scale = 1.0f / cos_tp;
+        const float inv_dr = 1.0f / g.delta_det_row;
+        const float z0v = -tz - g.delta_voxel * (0.5f * (float)(g.num_recon_slices - 1));
+        const float mr = mag * inv_d;
+        fb.x = (mag * z0v + g.det_row_offset) * inv_dr + 0.5f * (float)(g.num_det_rows - 1);
+        fb.y = mag * g.delta_voxel * inv_dr;
+        fb.z = mr * mr;
+        fb.w = z0v;
+    } else if (KIND == MBX_GEOM_PARALLEL) {
         const float x = cs * x_tilde - sn * y_tilde;
         n_p = (x + g.det_channel_offset) * inv_dc + det_center_channel;
         const float cos_alpha = fmaxf(fabsf(cs), fabsf(sn));
@@ -114,6 +135,20 @@ __device__ __forceinline__ void bpf_footprint(const mbx_geom &g, float cs, float
     fa = make_float4(__int_as_float(any ? first : -1), c[0], c[1], c[2]);
 }
 
+// Pixel position relative to the recon centre (ALU): x from the column, y from the row (translation geometry
+// spaces rows by delta_recon_row).
+template <int KIND>
+__device__ __forceinline__ void bpf_pixel(const mbx_geom &g, int idx, float &x_tilde, float &y_tilde) {
+    if (KIND == MBX_GEOM_TRANSLATION) {
+        const int row = idx / g.num_recon_cols;
+        const int col = idx - row * g.num_recon_cols;
+        x_tilde = g.delta_voxel * ((float)col - 0.5f * (float)(g.num_recon_cols - 1));
+        y_tilde = g.delta_recon_row * ((float)row - 0.5f * (float)(g.num_recon_rows - 1));
+    } else {
+        pixel_tilde(g, idx, x_tilde, y_tilde);
+    }
+}
+
 // Arguments of one back projection (one scan).
 struct BpArgs {
     mbx_geom g;
@@ -158,10 +193,11 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
     const int pcta = 1 << lg_pcta;                  // pixels per CTA
     float4 *s_fa = reinterpret_cast<float4 *>(smf);  // [chunk] = [view in chunk][pixel]
     float4 *s_fb = s_fa + chunk;                     // cone: [chunk]
-    float *s_cs = reinterpret_cast<float *>(s_fa + (KIND == MBX_GEOM_CONE ? 2 : 1) * chunk);
+    float *s_cs = reinterpret_cast<float *>(s_fa + (KIND != MBX_GEOM_PARALLEL ? 2 : 1) * chunk);
     float *s_sn = s_cs + vc;
     int *s_voff = reinterpret_cast<int *>(s_sn + vc);      // element offset of each view (-1: invalid view)
-    float *cache = reinterpret_cast<float *>(s_voff + vc);  // [BPF_CACHE_ROWS][BPF_THREADS] (cone)
+    float *s_tz = reinterpret_cast<float *>(s_voff + vc);   // translation: tz of each view
+    float *cache = s_tz + (KIND == MBX_GEOM_TRANSLATION ? vc : 0);  // [BPF_CACHE_ROWS][BPF_THREADS] (cone, transl.)
 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int pg = warp / nsl, stl = warp - pg * nsl;
@@ -187,7 +223,7 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
     if (fp_pixel < num_pixels) {
         const int idx = pix[fp_pixel];
         if (idx >= 0 && idx < npix_grid) {
-            pixel_tilde(g, idx, fxt, fyt);
+            bpf_pixel<KIND>(g, idx, fxt, fyt);
             fvalid = true;
         } else if (by == 0 && split == 0 && tid < pcta) {
             flag_error(err, MBX_ERRFLAG_PIXEL);
@@ -198,7 +234,7 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
     if (active) {
         const int idx = pix[p];
         active = idx >= 0 && idx < npix_grid;
-        if (active) pixel_tilde(g, idx, oxt, oyt);
+        if (active) bpf_pixel<KIND>(g, idx, oxt, oyt);
     }
 
     float acc[BPF_ST];
@@ -277,7 +313,7 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                     const float m_p = fmaf(k, A1, A0);
                     const int m_c = (int)rintf(m_p);
                     const float d = m_p - (float)m_c;
-                    const float z = fmaf(k, g.delta_voxel, z0);
+                    const float z = fmaf(k, g.delta_voxel, KIND == MBX_GEOM_TRANSLATION ? fb.w : z0);
                     const float q = fmaf(c2, z * z, 1.0f);
                     float sec = q * rsqrtf(q);                       // 1 / cos(phi_k)
                     const float l_m = fminf(fmaxf(half_w - fabsf(d + 1.0f), 0.0f), l_max);
@@ -302,10 +338,16 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             const int vi = views ? views[vb + t] : vb + t;
             const bool ok = vi >= 0 && vi < g.num_views;
             if (!ok && bx == 0 && by == 0) flag_error(err, MBX_ERRFLAG_VIEW);
-            const float ang = ok ? g.angles[vi] : 0.0f;
             s_voff[t] = ok ? vi * view_stride : -1;
-            s_cs[t] = cosf(ang);
-            s_sn[t] = sinf(ang);
+            if (KIND == MBX_GEOM_TRANSLATION) {  // (tx, ty) in the (cos, sin) slots, tz in its own table
+                s_cs[t] = ok ? g.translations[3 * vi] : 0.0f;
+                s_sn[t] = ok ? g.translations[3 * vi + 1] : 0.0f;
+                s_tz[t] = ok ? g.translations[3 * vi + 2] : 0.0f;
+            } else {
+                const float ang = ok ? g.angles[vi] : 0.0f;
+                s_cs[t] = cosf(ang);
+                s_sn[t] = sinf(ang);
+            }
         }
     };
 
@@ -320,7 +362,8 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 const int voff = s_voff[t];
                 if (voff < 0) continue;
                 float4 fa, fb;
-                bpf_footprint<KIND>(g, s_cs[t], s_sn[t], oxt, oyt, coeff_power, fa, fb);
+                bpf_footprint<KIND>(g, s_cs[t], s_sn[t], oxt, oyt, coeff_power, fa, fb,
+                                    KIND == MBX_GEOM_TRANSLATION ? s_tz[t] : 0.0f);
                 if (__float_as_int(fa.x) >= 0) gather(fa, fb, voff);
             }
         }
@@ -334,9 +377,11 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 const int t = f >> lg_pcta;
                 if (t < nv) {
                     float4 fa = make_float4(__int_as_float(-1), 0.f, 0.f, 0.f), fb = make_float4(0.f, 0.f, 0.f, 0.f);
-                    if (fvalid && s_voff[t] >= 0) bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb);
+                    if (fvalid && s_voff[t] >= 0)
+                        bpf_footprint<KIND>(g, s_cs[t], s_sn[t], fxt, fyt, coeff_power, fa, fb,
+                                            KIND == MBX_GEOM_TRANSLATION ? s_tz[t] : 0.0f);
                     s_fa[f] = fa;
-                    if (KIND == MBX_GEOM_CONE) s_fb[f] = fb;
+                    if (KIND != MBX_GEOM_PARALLEL) s_fb[f] = fb;
                 }
             }
             __syncthreads();
@@ -345,7 +390,7 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 const int f = (t << lg_pcta) + pl;
                 const float4 fa = s_fa[f];
                 if (__float_as_int(fa.x) < 0) continue;
-                gather(fa, KIND == MBX_GEOM_CONE ? s_fb[f] : make_float4(0.f, 0.f, 0.f, 0.f), s_voff[t]);
+                gather(fa, KIND != MBX_GEOM_PARALLEL ? s_fb[f] : make_float4(0.f, 0.f, 0.f, 0.f), s_voff[t]);
             }
         }
     }
@@ -373,7 +418,9 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
     BpfPlan pl;
     pl.inline_fp = inline_fp;
     // 32-bit element offsets address the sinogram
-    pl.ok = (g.kind == MBX_GEOM_PARALLEL || g.kind == MBX_GEOM_CONE) && (g.psf_radius == 1) && g.num_det_channels >= 3 &&
+    pl.ok = (g.kind == MBX_GEOM_PARALLEL || g.kind == MBX_GEOM_CONE ||
+             (g.kind == MBX_GEOM_TRANSLATION && g.max_magnification > 0.0f)) &&
+            (g.psf_radius == 1) && g.num_det_channels >= 3 &&
             (long long)g.num_views * g.num_det_rows * g.num_det_channels < (1LL << 31);
     const int S = g.num_recon_slices;
     // tile height: the fewest tiles of <= BPF_ST slices, rounded up to a power of two (<= 8) or a multiple of 8,
@@ -393,7 +440,7 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
     pl.lg_pcta = 5;
     while ((1 << pl.lg_pcta) < 32 * pl.npg) ++pl.lg_pcta;
     const int pcta = 32 * pl.npg;
-    pl.chunk = (g.kind == MBX_GEOM_CONE) ? MBX_BPF_CHUNK_CONE : MBX_BPF_CHUNK_PARALLEL;
+    pl.chunk = (g.kind != MBX_GEOM_PARALLEL) ? MBX_BPF_CHUNK_CONE : MBX_BPF_CHUNK_PARALLEL;
     if (pl.chunk < pcta) pl.chunk = pcta;
     pl.vc = pl.chunk / pcta;
     if (inline_fp) {  // no staged footprints; a view table of up to 1024 views per refill
@@ -410,6 +457,9 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
         const double max_mag = inv > 1e-6 ? 1.0 / inv : 1e6;
         const double slope = max_mag * g.delta_voxel / g.delta_det_row;
         if (pl.ts * slope + 4 > BPF_CACHE_ROWS) pl.ok = false;
+    } else if (g.kind == MBX_GEOM_TRANSLATION) {  // same bound from the host's magnification bound
+        const double slope = (double)g.max_magnification * g.delta_voxel / g.delta_det_row;
+        if (pl.ts * slope + 4 > BPF_CACHE_ROWS) pl.ok = false;
     }
     const long long base = (long long)pl.gx * pl.gy;
     const int sms = num_sms();
@@ -423,8 +473,9 @@ inline BpfPlan plan_bp_fast(const mbx_geom &g, long long num_pixels, int num_vie
     }
     pl.views_per_split = ceil_div(num_views_sel, splits);
     pl.splits = ceil_div(num_views_sel, pl.views_per_split);
-    pl.smem = (size_t)pl.chunk * 16 * (g.kind == MBX_GEOM_CONE ? 2 : 1) + (size_t)pl.vc * 12 +
-              (g.kind == MBX_GEOM_CONE ? (size_t)BPF_CACHE_ROWS * BPF_THREADS * 4 : 0);
+    pl.smem = (size_t)pl.chunk * 16 * (g.kind != MBX_GEOM_PARALLEL ? 2 : 1) +
+              (size_t)pl.vc * (g.kind == MBX_GEOM_TRANSLATION ? 16 : 12) +
+              (g.kind != MBX_GEOM_PARALLEL ? (size_t)BPF_CACHE_ROWS * BPF_THREADS * 4 : 0);
     pl.workspace = pl.splits > 1 ? align256((size_t)pl.splits * num_pixels * S * 4) : 0;
     return pl;
 }

@@ -119,6 +119,7 @@ class TomographyModel(ParameterHandler):
             if g.kind == _capi.MBX_GEOM_TRANSLATION:  # (num_views, 3) translation vectors
                 g.translations = self._angles_dev.data_ptr()
                 g.delta_recon_row = float(gp.delta_recon_row)
+                g.max_magnification = float(self._max_magnification())
             else:
                 g.angles = self._angles_dev.data_ptr()
             if g.psf_radius > _capi.MBX_MAX_PSF_RADIUS or g.bp_psf_radius > _capi.MBX_MAX_PSF_RADIUS:

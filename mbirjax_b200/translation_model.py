@@ -72,6 +72,17 @@ class TranslationModel(TomographyModel):
         values.append(self.entries_per_cylinder_batch)
         return namedtuple('GeometryParams', names)(*values)
 
+    def _max_magnification(self):
+        """An upper bound of mag = 1 / (1/M - y/D) over every pixel row and view, y = delta_recon_row (row -
+        (Nr-1)/2) - ty, with a small margin; 0 when some pixel reaches the source plane.  The fast back projector
+        sizes its detector-row cache from it."""
+        recon_shape, delta_recon_row, translation_vectors, sdd = self.get_params(
+            ['recon_shape', 'delta_recon_row', 'translation_vectors', 'source_detector_dist'])
+        ty = np.asarray(translation_vectors, dtype=np.float64)[:, 1]
+        y_max = delta_recon_row * 0.5 * (recon_shape[0] - 1) - float(np.min(ty))
+        inv = 1.0 / self.get_magnification() - y_max / sdd
+        return 0.0 if inv <= 1e-6 else 1.001 / inv
+
     def get_psf_radius(self):
         """translation_model.py:109-140 in float32 as the reference's jnp scalars: detector elements on either
         side of the centre one that the closest voxel (largest magnification) can reach."""
