@@ -78,6 +78,23 @@ def test_geometry_matches_oracle(kind, kw):
         assert g3.psf_radius == m2.get_geometry_parameters().psf_radius
 
 
+@pytest.mark.parametrize('y_spread,sid_factor', [(0.0, None), (6.0, None), (3.0, 2.0)])
+def test_translation_magnification_bound_covers_every_pixel_and_view(y_spread, sid_factor):
+    # the fast back projector sizes its detector-row cache from this bound: it must hold for every pixel row and
+    # every view's ty (mag = 1 / (1/M - y/D), y = delta_recon_row (row - (Nr-1)/2) - ty)
+    model, geom = make_case('translation', views=14, rows=8, channels=32, y_spread=y_spread, sid_factor=sid_factor)
+    bound = model._max_magnification()
+    nr = geom.recon_shape[0]
+    rows = np.arange(nr)
+    for tv in geom.angles:
+        y = geom.delta_recon_row * (rows - (nr - 1) / 2.0) - float(tv[1])
+        mag = 1.0 / (1.0 / geom.magnification - y / geom.source_detector_dist)
+        assert np.all(mag > 0) and np.all(mag <= bound)
+    assert bound <= 1.01 * np.max(1.0 / (1.0 / geom.magnification - (geom.delta_recon_row * (nr - 1) / 2.0 -
+                                                                      np.min(geom.angles[:, 1])) /
+                                         geom.source_detector_dist))
+
+
 def test_translation_model_reference_geometry():
     """The geometry TranslationModel derives for the reference's VCD test setup (tests/test_vcd.py:27-64:
     40 rows x 128 channels, source at 512 = detector distance, a 7 x 7 raster of translations 22 ALU apart,
