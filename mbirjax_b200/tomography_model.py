@@ -513,6 +513,13 @@ class TomographyModel(ParameterHandler):
             return 1.0 / (torch.abs(s) + 0.1)
         raise Exception('gen_weights: undefined weight_type {}'.format(weight_type))
 
+    def gen_modified_3d_sl_phantom(self):
+        """tomography_model.py:1766-1775: the low-dynamic-range 3D Shepp-Logan phantom of the recon shape, on the
+        model's GPU (on the host when none is visible, since it is test data rather than compute)."""
+        from .utilities import generate_3d_shepp_logan_low_dynamic_range
+        device = self._device() if torch.cuda.is_available() else torch.device('cpu')
+        return generate_3d_shepp_logan_low_dynamic_range(self.get_params('recon_shape'), device=device)
+
     def scale_recon_shape(self, row_scale=1.0, col_scale=1.0, slice_scale=1.0):
         old_rows, old_cols, old_slices = self.get_params('recon_shape')
         new = (int(old_rows * row_scale), int(old_cols * col_scale), int(old_slices * slice_scale))

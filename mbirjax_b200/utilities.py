@@ -6,9 +6,11 @@ voxels and densities uniform in [0.1, 1], summed where they overlap (the same co
 reference's ``add_ellipsoid``, ``utilities.py:856-895``, without rotation).  Generation runs with torch on
 whatever device the caller names (the CPU in tests, the GPU for the large configurations).
 
-Also here: the translation-vector raster of the reference's translation experiments and its HDF5 helpers
-``save_data_hdf5`` / ``load_data_hdf5`` (which need h5py).
+Also here: the reference's test phantoms (the low-dynamic-range 3D Shepp-Logan of
+``gen_modified_3d_sl_phantom`` and the sheared cube of ``gen_cube_phantom``), the translation-vector raster of
+its translation experiments and its HDF5 helpers ``save_data_hdf5`` / ``load_data_hdf5`` (which need h5py).
 """
+import math
 import os
 
 import numpy as np
@@ -36,6 +38,62 @@ def gen_ellipsoid_phantom(recon_shape, num_ellipsoids, seed, device='cpu', dtype
         inside = ((ii - c[0]) / a[0]) ** 2 + ((jj - c[1]) / a[1]) ** 2 + ((kk - c[2]) / a[2]) ** 2 <= 1.0
         out[lo[0]:hi[0], lo[1]:hi[1], lo[2]:hi[2]] += float(d) * inside.to(dtype)
     return out
+
+
+# (x0, y0, z0, a, b, c, angle in degrees, intensity) of the ellipsoids of the low-dynamic-range Shepp-Logan
+# phantom, in the order they are added (utilities.py:684-694 of the reference).  x runs along recon rows, y along
+# columns and z along slices, each over [-1, 1].
+_SHEPP_LOGAN_LOW_DYNAMIC_RANGE = (
+    (0.0, 0.0, 0.0, 0.69, 0.92, 0.9, 0.0, 1.0),
+    (0.0, 0.0184, 0.0, 0.6624, 0.874, 0.88, 0.0, -0.8),
+    (0.22, 0.0, 0.0, 0.41, 0.16, 0.21, 108.0, -0.2),
+    (-0.22, 0.0, 0.0, 0.31, 0.11, 0.22, 72.0, -0.2),
+    (0.0, 0.35, 0.0, 0.21, 0.25, 0.5, 0.0, 0.1),
+    (0.0, 0.1, 0.0, 0.046, 0.046, 0.046, 0.0, 0.1),
+    (0.0, -0.1, 0.0, 0.046, 0.046, 0.046, 0.0, 0.1),
+    (-0.08, -0.605, 0.0, 0.046, 0.023, 0.02, 0.0, 0.1),
+    (0.0, -0.605, 0.0, 0.023, 0.023, 0.02, 0.0, 0.1),
+)
+
+
+def generate_3d_shepp_logan_low_dynamic_range(phantom_shape, device='cpu'):
+    """The reference's low-dynamic-range 3D Shepp-Logan phantom (utilities.py:658-696): float32 (rows, cols,
+    slices), each ellipsoid adding its intensity where (xr/a)^2 + (yr/b)^2 + ((z-z0)/c)^2 <= 1, with (xr, yr) the
+    in-plane offset rotated by the ellipsoid's angle.  The slices are filled in blocks, so the peak extra memory
+    is about 64 M elements whatever the volume."""
+    nr, nc, ns = (int(v) for v in phantom_shape)
+    f32 = torch.float32
+    x = torch.linspace(-1, 1, nr, dtype=f32, device=device)[:, None]
+    y = torch.linspace(-1, 1, nc, dtype=f32, device=device)[None, :]
+    z = torch.linspace(-1, 1, ns, dtype=f32, device=device)
+    phantom = torch.zeros((nr, nc, ns), dtype=f32, device=device)
+    block = max(1, (1 << 26) // max(1, nr * nc))
+    for x0, y0, z0, a, b, c, angle, intensity in _SHEPP_LOGAN_LOW_DYNAMIC_RANGE:
+        t = torch.tensor(math.radians(angle), dtype=f32)
+        cos_t, sin_t = float(torch.cos(t)), float(torch.sin(t))
+        xr = cos_t * (x - x0) + sin_t * (y - y0)
+        yr = -sin_t * (x - x0) + cos_t * (y - y0)
+        xy_norm = (xr ** 2 / a ** 2 + yr ** 2 / b ** 2)[:, :, None]
+        z_norm = (z - z0) ** 2 / c ** 2
+        for k0 in range(0, ns, block):
+            k1 = min(ns, k0 + block)
+            phantom[:, :, k0:k1] += intensity * ((xy_norm + z_norm[k0:k1]) <= 1).to(f32)
+    return phantom
+
+
+def gen_cube_phantom(recon_shape, device='cpu'):
+    """The reference's cube phantom (utilities.py:1034-1056): a block of a quarter of the rows and columns,
+    centred, with value 1 / max(its rows, its cols), whose columns shift right by int(slice * cols / num_slices)
+    from slice to slice."""
+    nr, nc, ns = (int(v) for v in recon_shape[:3])
+    rows, cols = nr // 4, nc // 4
+    phantom = np.zeros((nr, nc, ns))
+    r0, r1 = (nr - rows) // 2, (nr + rows) // 2
+    c0, c1 = (nc - cols) // 2, (nc + cols) // 2
+    for k in range(ns):
+        shift = int(k * cols / ns)
+        phantom[r0:r1, shift + c0:shift + c1, k] = 1.0 / max(rows, cols)
+    return torch.as_tensor(phantom, dtype=torch.float32, device=device)
 
 
 def add_noise(sinogram, rel_sigma, seed):

@@ -65,3 +65,31 @@ def rel_l2(a, b):
     a = np.asarray(a, dtype=np.float64)
     b = np.asarray(b, dtype=np.float64)
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
+
+
+# The reference's FBP/FDK acceptance test (tests/test_fbp_fdk.py:14-47): 128 views of a 128 x 128 detector; parallel
+# beam over [-pi/2, pi/2), cone beam over [-pi, pi) with sdd = 4 * 128 and sid = sdd / 2; the recon of the forward
+# projection of the low-dynamic-range Shepp-Logan phantom must stay under these error bounds, which the reference
+# sets just above its own deterministic results.
+FBP_FDK_SIZE = 128
+FBP_TOLERANCES = {'nrmse': 0.21, 'max_diff': 0.41, 'pct_95': 0.064}
+FDK_TOLERANCES = {'nrmse': 0.27, 'max_diff': 0.51, 'pct_95': 0.1}
+
+
+def fbp_fdk_model(kind):
+    n = FBP_FDK_SIZE
+    if kind == 'parallel':
+        ang = np.linspace(-np.pi / 2, np.pi / 2, n, endpoint=False).astype(np.float32)
+        return mb.ParallelBeamModel((n, n, n), ang)
+    sdd = 4 * n
+    ang = np.linspace(-np.pi, np.pi, n, endpoint=False).astype(np.float32)
+    return mb.ConeBeamModel((n, n, n), ang, source_detector_dist=sdd, source_iso_dist=sdd / 2)
+
+
+def recon_error_stats(recon, phantom):
+    """max |x - x_true|, ||x - x_true|| / ||x_true|| and the 95th percentile of |x - x_true|, as the reference's
+    test computes them."""
+    recon, phantom = np.asarray(recon), np.asarray(phantom)
+    err = np.abs(recon - phantom)
+    return {'max_diff': float(np.amax(err)), 'nrmse': float(np.linalg.norm(recon - phantom) / np.linalg.norm(phantom)),
+            'pct_95': float(np.percentile(err, 95))}

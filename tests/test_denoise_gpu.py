@@ -62,3 +62,18 @@ def test_denoiser_reduces_noise(cuda):
     out = out.cpu().numpy()
     assert np.linalg.norm(out - clean) / np.linalg.norm(clean) < 0.2
     assert np.linalg.norm(out - clean) < np.linalg.norm(noisy - clean)
+
+
+def test_qggmrf_denoiser_reference_case(cuda):
+    """tests/test_denoiser.py::test_qggmrf_denoiser at its own size: a 100^3 Shepp-Logan phantom with noise of std
+    0.1, sharpness 0, at most 20 iterations, stop at 0.1%, denoised within 20% relative error."""
+    from mbirjax_b200.utilities import generate_3d_shepp_logan_low_dynamic_range
+    np.random.seed(0)
+    shape = (100, 100, 100)
+    phantom = generate_3d_shepp_logan_low_dynamic_range(shape).numpy()
+    noisy = phantom + 0.1 * np.random.randn(*shape)
+    den = mb.QGGMRFDenoiser(shape)
+    den.set_params(sharpness=0.0, verbose=0)
+    out, _ = den.denoise(noisy, 0.1, max_iterations=20, stop_threshold_change_pct=0.1, logfile_path=None,
+                         print_logs=False)
+    assert np.linalg.norm(out.cpu().numpy() - phantom) / np.linalg.norm(phantom) < 0.2

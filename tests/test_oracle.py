@@ -130,6 +130,67 @@ def test_oracle_fbp_recovers_phantom():
     assert abs(float(np.mean(rec[inner])) - 1.0) < 0.1
 
 
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_oracle_fbp_fdk_meets_the_reference_tolerances(kind):
+    """tests/test_fbp_fdk.py at its own size: the oracle's FBP / FDK of its forward projection of the Shepp-Logan
+    phantom stays under the error bounds the reference sets just above its own results (parallel lands at nrmse
+    0.2099 against 0.21), which pins the projector and filter scaling, not only their structure."""
+    from cases import fbp_fdk_model, oracle_geometry, recon_error_stats, FBP_TOLERANCES, FDK_TOLERANCES
+    from mbirjax_b200.utilities import generate_3d_shepp_logan_low_dynamic_range
+    geom = oracle_geometry(fbp_fdk_model(kind))
+    assert geom.recon_shape == (128, 128, 128)
+    phantom = generate_3d_shepp_logan_low_dynamic_range(geom.recon_shape).numpy()
+    sino = O.forward_project(geom, phantom)
+    if kind == 'parallel':
+        filtered, tol = O.fbp_filter(sino, geom.delta_voxel), FBP_TOLERANCES
+    else:
+        filtered, tol = O.fdk_filter(sino, geom.source_detector_dist, geom.magnification, geom.delta_voxel,
+                                     geom.delta_det_row, geom.delta_det_channel, geom.det_row_offset,
+                                     geom.det_channel_offset), FDK_TOLERANCES
+    stats = recon_error_stats(O.back_project(geom, filtered), phantom)
+    for name, bound in tol.items():
+        assert stats[name] < bound, (name, stats)
+
+
+def test_oracle_denoiser_meets_the_reference_tolerance():
+    """tests/test_denoiser.py::test_qggmrf_denoiser at its own size: the oracle's qGGMRF denoiser (sharpness 0,
+    16 subsets, at most 20 iterations, stop at 0.1%) brings a 100^3 Shepp-Logan phantom with noise of std 0.1
+    within 20% relative error."""
+    from oracle import denoise as OD
+    from mbirjax_b200.utilities import generate_3d_shepp_logan_low_dynamic_range
+    np.random.seed(0)
+    shape = (100, 100, 100)
+    phantom = generate_3d_shepp_logan_low_dynamic_range(shape).numpy()
+    noisy = (phantom + 0.1 * np.random.randn(*shape)).astype(np.float32)
+    small = noisy[::shape[0] // min(20, shape[0])]     # auto_set_regularization_params' view subsample
+    sigma_x = float(np.float32(0.2 * OD._neighbour_std(small, OD._support(small, 0.1))))
+    partition = O.gen_set_of_pixel_partitions(shape, [16], use_ror_mask=False)[0]
+    qp = (O.get_b_from_nbr_wts([1, 1, 1]), sigma_x, 2.0, 1.2, 1.0)
+    out, nmae, _ = OD.denoise(noisy, partition, 0.1, qp, 20, 0.1)
+    assert np.linalg.norm(out - phantom) / np.linalg.norm(phantom) < 0.2
+    assert len(nmae) < 20                               # the 0.1% stop ends it early
+
+
+def test_shepp_logan_and_cube_phantoms():
+    """The reference's test phantoms (utilities.py:658-696, 1034-1056) by known answers: the centre voxel of the
+    Shepp-Logan phantom is 1 - 0.8, the volume is symmetric in the slice axis, and its values are sums of the
+    listed intensities; the cube is a quarter block of value 1 / max(rows, cols), shifted a column per slice."""
+    from mbirjax_b200.utilities import generate_3d_shepp_logan_low_dynamic_range, gen_cube_phantom
+    p = generate_3d_shepp_logan_low_dynamic_range((65, 49, 33)).numpy()
+    assert p.dtype == np.float32 and p.shape == (65, 49, 33)
+    assert p[32, 24, 16] == np.float32(1.0) + np.float32(-0.8)
+    np.testing.assert_array_equal(p, p[:, :, ::-1])
+    levels = np.array([0.0, 0.1, 0.2, 0.3, 0.4, 1.0])
+    assert np.all(np.min(np.abs(np.unique(p)[:, None] - levels[None, :]), axis=1) < 1e-6)
+    assert p[0, 0, 0] == 0 and p[32, 24, 0] == 0          # corner and the slice ends lie outside the skull
+    c = gen_cube_phantom((16, 20, 5)).numpy()
+    assert c.shape == (16, 20, 5)
+    for k in range(5):
+        rows, cols = np.nonzero(c[:, :, k])
+        assert (rows.min(), rows.max()) == (6, 9) and (cols.min(), cols.max()) == (7 + k, 11 + k)
+    np.testing.assert_allclose(c[c > 0], 0.2)
+
+
 def test_oracle_prox_map_fixed_point():
     """The oracle's proximal map leaves a consistent input in place (the reference's tests/test_prox.py corner
     case, on a small volume)."""

@@ -79,3 +79,23 @@ def test_direct_recon_of_phantom(cuda, kind):
                          O.fdk_filter(O.forward_project(geom, ph), geom.source_detector_dist, geom.magnification,
                                       geom.delta_voxel, geom.delta_det_row, geom.delta_det_channel))
     assert rel_l2(rec, ref) <= 1e-5
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_fbp_fdk_meets_the_reference_tolerances(cuda, kind):
+    """tests/test_fbp_fdk.py through the model API at its own size: the Shepp-Logan phantom of the model, its
+    forward projection and the direct recon of that stay under the reference's error bounds; the parallel recon
+    also matches the oracle's."""
+    from cases import fbp_fdk_model, oracle_geometry, recon_error_stats, FBP_TOLERANCES, FDK_TOLERANCES
+    model = fbp_fdk_model(kind)
+    phantom = model.gen_modified_3d_sl_phantom()
+    assert tuple(phantom.shape) == (128, 128, 128)
+    recon = model.direct_recon(model.forward_project(phantom)).cpu().numpy()
+    phantom = phantom.cpu().numpy()
+    stats = recon_error_stats(recon, phantom)
+    for name, bound in (FBP_TOLERANCES if kind == 'parallel' else FDK_TOLERANCES).items():
+        assert stats[name] < bound, (name, stats)
+    if kind == 'parallel':
+        geom = oracle_geometry(model)
+        ref = O.back_project(geom, O.fbp_filter(O.forward_project(geom, phantom), geom.delta_voxel))
+        assert rel_l2(recon, ref) <= 1e-5
