@@ -93,3 +93,19 @@ def recon_error_stats(recon, phantom):
     err = np.abs(recon - phantom)
     return {'max_diff': float(np.amax(err)), 'nrmse': float(np.linalg.norm(recon - phantom) / np.linalg.norm(phantom)),
             'pct_95': float(np.percentile(err, 95))}
+
+
+# The reference's VCD acceptance test (tests/test_vcd.py:16-45, 80-120): 64 views of a 40 x 128 detector, angles of
+# the projector tests, cone beam with sdd = sid = 4 * 128, the model's default recon (sharpness 1, multi-granular
+# partitions, at most 15 iterations, stop at 0.2%) of the forward projection of the Shepp-Logan phantom.
+VCD_TOLERANCES = {'parallel': {'nrmse': 0.15, 'max_diff': 0.38, 'pct_95': 0.04},
+                  'cone': {'nrmse': 0.19, 'max_diff': 0.56, 'pct_95': 0.05}}
+
+
+def vcd_acceptance_model(kind):
+    views, rows, channels = 64, 40, 128
+    sdd = 4 * channels
+    ang = angles_for(kind, views, channels, sdd)
+    if kind == 'parallel':
+        return mb.ParallelBeamModel((views, rows, channels), ang)
+    return mb.ConeBeamModel((views, rows, channels), ang, source_detector_dist=sdd, source_iso_dist=sdd)

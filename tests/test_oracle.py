@@ -152,6 +152,26 @@ def test_oracle_fbp_fdk_meets_the_reference_tolerances(kind):
         assert stats[name] < bound, (name, stats)
 
 
+def test_oracle_vcd_meets_the_reference_tolerances():
+    """tests/test_vcd.py at its own size, parallel beam (the cone case takes minutes on the CPU and runs on the GPU
+    through the model API): the oracle's default multi-granular VCD recon of the Shepp-Logan phantom's forward
+    projection stays under the reference's error bounds (it lands at nrmse 0.089 against 0.15)."""
+    from cases import vcd_acceptance_model, oracle_geometry, recon_error_stats, VCD_TOLERANCES
+    from mbirjax_b200.utilities import generate_3d_shepp_logan_low_dynamic_range
+    model = vcd_acceptance_model('parallel')
+    geom = oracle_geometry(model)
+    phantom = generate_3d_shepp_logan_low_dynamic_range(geom.recon_shape).numpy()
+    sino = O.forward_project(geom, phantom)
+    np.random.seed(0)
+    granularity, sequence = model.get_params(['granularity', 'partition_sequence'])
+    rec, stats = O.vcd.recon(geom, sino, granularity=granularity, partition_sequence=sequence, max_iterations=15,
+                             sharpness=model.get_params('sharpness'), snr_db=model.get_params('snr_db'),
+                             stop_threshold_change_pct=0.2)
+    err = recon_error_stats(rec, phantom)
+    for name, bound in VCD_TOLERANCES['parallel'].items():
+        assert err[name] < bound, (name, err)
+
+
 def test_oracle_denoiser_meets_the_reference_tolerance():
     """tests/test_denoiser.py::test_qggmrf_denoiser at its own size: the oracle's qGGMRF denoiser (sharpness 0,
     16 subsets, at most 20 iterations, stop at 0.1%) brings a 100^3 Shepp-Logan phantom with noise of std 0.1

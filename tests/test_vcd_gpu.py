@@ -160,3 +160,21 @@ def test_prox_map_fixed_point(cuda):
     rec, _ = model.prox_map(phantom, sino, max_iterations=5, init_recon=phantom, logfile_path=None,
                             print_logs=False)
     assert float(torch.max(torch.abs(rec - phantom.to(rec.device)))) < 1e-5
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone'])
+def test_vcd_meets_the_reference_tolerances(cuda, kind):
+    """tests/test_vcd.py through the model API at its own size: the model's Shepp-Logan phantom, its forward
+    projection, and the default recon of that (sharpness 1, multi-granular partitions, at most 15 iterations,
+    stop at 0.2%) stay under the reference's error bounds."""
+    from cases import vcd_acceptance_model, recon_error_stats, VCD_TOLERANCES
+    model = vcd_acceptance_model(kind)
+    phantom = model.gen_modified_3d_sl_phantom()
+    sino = model.forward_project(phantom)
+    model.set_params(verbose=0)
+    np.random.seed(0)
+    rec, rdict = model.recon(sino, logfile_path=None, print_logs=False)
+    assert rdict['recon_params']['num_iterations'] <= 15
+    err = recon_error_stats(rec.cpu().numpy(), phantom.cpu().numpy())
+    for name, bound in VCD_TOLERANCES[kind].items():
+        assert err[name] < bound, (name, err)
