@@ -1,5 +1,8 @@
 """Geometry cases shared by the CPU and GPU tests: each builds a mbirjax_b200 model and the matching
 oracle geometry from the same arguments."""
+import json
+import os
+
 import numpy as np
 
 import mbirjax_b200 as mb
@@ -67,13 +70,19 @@ def rel_l2(a, b):
     return float(np.linalg.norm(a - b) / max(np.linalg.norm(b), 1e-300))
 
 
+# The error bounds of the reference's end-to-end tests, extracted from its test files by
+# tests/golden/make_acceptance_bounds.py.
+with open(os.path.join(os.path.dirname(os.path.abspath(__file__)), 'golden', 'acceptance_bounds.json')) as _f:
+    ACCEPTANCE_BOUNDS = json.load(_f)
+
+
 # The reference's FBP/FDK acceptance test (tests/test_fbp_fdk.py:14-47): 128 views of a 128 x 128 detector; parallel
 # beam over [-pi/2, pi/2), cone beam over [-pi, pi) with sdd = 4 * 128 and sid = sdd / 2; the recon of the forward
 # projection of the low-dynamic-range Shepp-Logan phantom must stay under these error bounds, which the reference
 # sets just above its own deterministic results.
 FBP_FDK_SIZE = 128
-FBP_TOLERANCES = {'nrmse': 0.21, 'max_diff': 0.41, 'pct_95': 0.064}
-FDK_TOLERANCES = {'nrmse': 0.27, 'max_diff': 0.51, 'pct_95': 0.1}
+FBP_TOLERANCES = ACCEPTANCE_BOUNDS['fbp']
+FDK_TOLERANCES = ACCEPTANCE_BOUNDS['fdk']
 
 
 def fbp_fdk_model(kind):
@@ -98,8 +107,7 @@ def recon_error_stats(recon, phantom):
 # The reference's VCD acceptance test (tests/test_vcd.py:16-45, 80-120): 64 views of a 40 x 128 detector, angles of
 # the projector tests, cone beam with sdd = sid = 4 * 128, the model's default recon (sharpness 1, multi-granular
 # partitions, at most 15 iterations, stop at 0.2%) of the forward projection of the Shepp-Logan phantom.
-VCD_TOLERANCES = {'parallel': {'nrmse': 0.15, 'max_diff': 0.38, 'pct_95': 0.04},
-                  'cone': {'nrmse': 0.19, 'max_diff': 0.56, 'pct_95': 0.05}}
+VCD_TOLERANCES = ACCEPTANCE_BOUNDS['vcd']
 
 
 def vcd_acceptance_model(kind):

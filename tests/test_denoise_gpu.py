@@ -76,4 +76,5 @@ def test_qggmrf_denoiser_reference_case(cuda):
     den.set_params(sharpness=0.0, verbose=0)
     out, _ = den.denoise(noisy, 0.1, max_iterations=20, stop_threshold_change_pct=0.1, logfile_path=None,
                          print_logs=False)
-    assert np.linalg.norm(out.cpu().numpy() - phantom) / np.linalg.norm(phantom) < 0.2
+    from cases import ACCEPTANCE_BOUNDS
+    assert np.linalg.norm(out.cpu().numpy() - phantom) / np.linalg.norm(phantom) < ACCEPTANCE_BOUNDS['denoiser_nrmse']
