@@ -5,7 +5,8 @@ Drop-in for ``mbirjax.ConeBeamModel`` (``cone_beam.py:16-871``): constructor
 (``:68-80``), ``verify_valid_params`` (``:82-108``), ``get_geometry_parameters`` (``:110-136``),
 ``get_psf_radius`` with ``bp_psf_radius`` (``:138-172``), ``auto_set_recon_size`` (``:174-187``) and
 ``fdk_filter`` / ``fdk_recon`` (= ``direct_filter`` / ``direct_recon``, ``:762-871``).  The separable
-vertical/horizontal fan projectors (``:189-707``) run in the CUDA library.
+vertical/horizontal fan projectors (``:189-707``) run in the CUDA library, for all views at once or, through
+the reference's per-view plugin functions, on a one-view geometry.
 """
 from collections import namedtuple
 import math
@@ -14,7 +15,7 @@ import warnings
 import numpy as np
 
 from . import _capi
-from .tomography_model import TomographyModel
+from .tomography_model import TomographyModel, back_project_one_view, forward_project_one_view
 from .parallel_beam import _host
 
 
@@ -90,6 +91,21 @@ class ConeBeamModel(TomographyModel):
         num_recon_slices = int(round(num_det_rows * ((delta_det_row / delta_voxel) / mag)))
         self.set_params(no_compile=no_compile, no_warning=no_warning,
                         recon_shape=(num_recon_rows, num_recon_rows, num_recon_slices))
+
+    @staticmethod
+    def forward_project_pixel_batch_to_one_view(voxel_values, pixel_indices, angle, projector_params):
+        """cone_beam.py:189-217: (N, S) voxel cylinders at pixel_indices -> the (R, C) view at angle (vertical
+        then horizontal fan), on the CUDA projector (a one-view geometry)."""
+        return forward_project_one_view(_capi.MBX_GEOM_CONE, voxel_values, pixel_indices, angle, projector_params)
+
+    @staticmethod
+    def back_project_one_view_to_pixel_batch(sinogram_view, pixel_indices, single_view_params, projector_params,
+                                             coeff_power=1):
+        """cone_beam.py:379-407: the (R, C) view at angle single_view_params -> (N, S) voxel cylinders at
+        pixel_indices (horizontal then vertical fan), with coefficients A ** coeff_power, on the CUDA projector
+        (a one-view geometry)."""
+        return back_project_one_view(_capi.MBX_GEOM_CONE, sinogram_view, pixel_indices, single_view_params,
+                                     projector_params, coeff_power)
 
     def fdk_filter(self, sinogram, filter_name='ramp', view_batch_size=100):
         return self.direct_filter(sinogram, filter_name=filter_name, view_batch_size=view_batch_size)

@@ -3,9 +3,10 @@
 Drop-in for ``mbirjax.ParallelBeamModel`` (``parallel_beam.py:13-373``): constructor
 ``ParallelBeamModel(sinogram_shape, angles)``, ``get_magnification`` (1), ``verify_valid_params``,
 ``get_geometry_parameters``, ``get_psf_radius``, ``auto_set_recon_size``, ``fbp_filter`` / ``fbp_recon``
-(= ``direct_filter`` / ``direct_recon``).  The per-view projector functions of the reference
-(``forward_project_pixel_batch_to_one_view`` / ``back_project_one_view_to_pixel_batch``) are replaced by the
-batched kernels behind ``mbx_sparse_forward_project`` / ``mbx_sparse_back_project``.
+(= ``direct_filter`` / ``direct_recon``).  The model's projections run the batched kernels behind
+``mbx_sparse_forward_project`` / ``mbx_sparse_back_project`` over all views at once; the reference's per-view
+plugin functions (``forward_project_pixel_batch_to_one_view`` / ``back_project_one_view_to_pixel_batch``) keep
+their signatures and run the same kernels on a one-view geometry.
 """
 from collections import namedtuple
 import math
@@ -13,7 +14,7 @@ import math
 import numpy as np
 
 from . import _capi
-from .tomography_model import TomographyModel
+from .tomography_model import TomographyModel, back_project_one_view, forward_project_one_view
 
 
 class ParallelBeamModel(TomographyModel):
@@ -62,6 +63,20 @@ class ParallelBeamModel(TomographyModel):
         num_recon_slices = int(round(num_det_rows * ((delta_det_row / delta_voxel) / mag)))
         self.set_params(no_compile=no_compile, no_warning=no_warning,
                         recon_shape=(num_recon_rows, num_recon_rows, num_recon_slices))
+
+    @staticmethod
+    def forward_project_pixel_batch_to_one_view(voxel_values, pixel_indices, angle, projector_params):
+        """parallel_beam.py:138-178: (N, S) voxel cylinders at pixel_indices -> the (R, C) view at angle, on the
+        CUDA projector (a one-view geometry)."""
+        return forward_project_one_view(_capi.MBX_GEOM_PARALLEL, voxel_values, pixel_indices, angle,
+                                        projector_params)
+
+    @staticmethod
+    def back_project_one_view_to_pixel_batch(sinogram_view, pixel_indices, angle, projector_params, coeff_power=1):
+        """parallel_beam.py:180-221: the (R, C) view at angle -> (N, S) voxel cylinders at pixel_indices, with
+        coefficients A ** coeff_power, on the CUDA projector (a one-view geometry)."""
+        return back_project_one_view(_capi.MBX_GEOM_PARALLEL, sinogram_view, pixel_indices, angle, projector_params,
+                                     coeff_power)
 
     def fbp_filter(self, sinogram, filter_name='ramp', view_batch_size=100):
         return self.direct_filter(sinogram, filter_name=filter_name, view_batch_size=view_batch_size)

@@ -85,6 +85,25 @@ class TomographyModel(ParameterHandler):
     def get_geometry_parameters(self):
         raise NotImplementedError
 
+    def get_projector_params(self):
+        """(sinogram_shape, recon_shape, geometry_params): the projector_params argument of the per-view plugin
+        functions, as the reference's Projectors builds it (projectors.py:44-53)."""
+        sinogram_shape, recon_shape = self.get_params(['sinogram_shape', 'recon_shape'])
+        return ProjectorParams(tuple(sinogram_shape), tuple(recon_shape), self.get_geometry_parameters())
+
+    @staticmethod
+    def forward_project_pixel_batch_to_one_view(voxel_values, pixel_indices, view_params, projector_params):
+        """tomography_model.py:486-505: a geometry overrides this; the base class warns and returns None."""
+        warnings.warn('Forward projector not implemented for TomographyModel.')
+        return None
+
+    @staticmethod
+    def back_project_one_view_to_pixel_batch(sinogram_view, pixel_indices, single_view_params, projector_params,
+                                             coeff_power=1):
+        """tomography_model.py:507-529: a geometry overrides this; the base class warns and returns None."""
+        warnings.warn('Back projector not implemented for TomographyModel.')
+        return None
+
     def _kind(self):
         raise NotImplementedError
 
@@ -544,3 +563,95 @@ def _to_numpy(x):
     if isinstance(x, torch.Tensor):
         return x.detach().cpu().numpy()
     return np.asarray(x)
+
+
+# ---------------------------------------------------------------------- the reference's per-view plugin functions
+ProjectorParams = namedtuple('ProjectorParams', ['sinogram_shape', 'recon_shape', 'geometry_params'])
+
+
+def translation_max_magnification(delta_recon_row, num_recon_rows, min_ty, magnification, source_detector_dist):
+    """An upper bound of mag = 1 / (1/M - y/D) over every pixel row of a translation geometry, y = delta_recon_row
+    (row - (Nr-1)/2) - ty, for views whose smallest ty is min_ty, with a small margin; 0 when some pixel reaches
+    the source plane.  The fast back projector sizes its detector-row cache from it."""
+    y_max = delta_recon_row * 0.5 * (num_recon_rows - 1) - float(min_ty)
+    inv = 1.0 / magnification - y_max / source_detector_dist
+    return 0.0 if inv <= 1e-6 else 1.001 / inv
+
+
+def one_view_geometry(kind, projector_params, view_params):
+    """The mbx_geom record of one view of a geometry, from the arguments of the reference's per-view plugin
+    functions: projector_params = (sinogram_shape, recon_shape, geometry_params), the namedtuple the reference's
+    Projectors builds (projectors.py:44-53), and the view's angle or translation vector.  Geometry parameters the
+    namedtuple of a geometry does not carry take their defaults (a parallel beam has no row spacing or offset).
+    Returns (record, the device tensor of the view parameters that the record points to)."""
+    sinogram_shape, recon_shape, gp = projector_params
+    translation = kind == _capi.MBX_GEOM_TRANSLATION
+    vp = np.asarray(_to_numpy(view_params), dtype=np.float32).reshape(-1)
+    if translation and vp.shape != (3,):
+        raise ValueError('translation_vector must hold (x, y, z); got {} values'.format(vp.size))
+    if not translation and vp.shape != (1,):
+        raise ValueError('angle must be one value; got {} values'.format(vp.size))
+    view_dev = torch.as_tensor(vp.reshape(1, -1) if translation else vp, device=_cuda_device()).contiguous()
+    g = _capi.MbxGeom()
+    g.kind = kind
+    g.num_views = 1
+    g.num_det_rows, g.num_det_channels = int(sinogram_shape[1]), int(sinogram_shape[2])
+    g.num_recon_rows, g.num_recon_cols, g.num_recon_slices = (int(v) for v in recon_shape)
+    g.psf_radius = int(gp.psf_radius)
+    g.bp_psf_radius = int(getattr(gp, 'bp_psf_radius', 1))
+    g.entries_per_cylinder_batch = int(getattr(gp, 'entries_per_cylinder_batch', 128))
+    g.delta_det_channel = float(gp.delta_det_channel)
+    g.delta_det_row = float(getattr(gp, 'delta_det_row', 1.0))
+    g.det_channel_offset = float(gp.det_channel_offset)
+    g.det_row_offset = float(getattr(gp, 'det_row_offset', 0.0))
+    g.delta_voxel = float(gp.delta_voxel)
+    g.recon_slice_offset = float(getattr(gp, 'recon_slice_offset', 0.0))
+    g.source_detector_dist = float(getattr(gp, 'source_detector_dist', np.inf))
+    g.magnification = float(getattr(gp, 'magnification', 1.0))
+    if translation:
+        g.translations = view_dev.data_ptr()
+        g.delta_recon_row = float(gp.delta_recon_row)
+        g.max_magnification = float(translation_max_magnification(gp.delta_recon_row, recon_shape[0], vp[1],
+                                                                   gp.magnification, gp.source_detector_dist))
+    else:
+        g.angles = view_dev.data_ptr()
+    if g.psf_radius > _capi.MBX_MAX_PSF_RADIUS or g.bp_psf_radius > _capi.MBX_MAX_PSF_RADIUS:
+        raise ValueError('psf radius %d / %d exceeds the supported maximum %d' % (
+            g.psf_radius, g.bp_psf_radius, _capi.MBX_MAX_PSF_RADIUS))
+    return g, view_dev
+
+
+def forward_project_one_view(kind, voxel_values, pixel_indices, view_params, projector_params):
+    """The reference's forward_project_pixel_batch_to_one_view: (N, S) voxel cylinders at pixel_indices ->
+    the (R, C) view, through mbx_sparse_forward_project on a one-view geometry."""
+    g, view_dev = one_view_geometry(kind, projector_params, view_params)
+    dev = view_dev.device
+    vox = _on_device(voxel_values, dev, torch.float32)
+    pix = _on_device(pixel_indices, dev, torch.int32)
+    if vox.ndim != 2 or pix.ndim != 1 or vox.shape[0] != pix.shape[0] or vox.shape[1] != g.num_recon_slices:
+        raise ValueError('voxel_values must have shape[0:2] = (num_indices, num_slices)')
+    return _capi.forward_project(g, vox, pix)[0]
+
+
+def back_project_one_view(kind, sinogram_view, pixel_indices, view_params, projector_params, coeff_power=1):
+    """The reference's back_project_one_view_to_pixel_batch: the (R, C) view -> (N, S) voxel cylinders at
+    pixel_indices with coefficients A_ij ** coeff_power, through mbx_sparse_back_project on a one-view
+    geometry."""
+    g, view_dev = one_view_geometry(kind, projector_params, view_params)
+    dev = view_dev.device
+    view = _on_device(sinogram_view, dev, torch.float32)
+    pix = _on_device(pixel_indices, dev, torch.int32)
+    if tuple(view.shape) != (g.num_det_rows, g.num_det_channels):
+        raise ValueError('sinogram_view must have shape {}, got {}'.format(
+            (g.num_det_rows, g.num_det_channels), tuple(view.shape)))
+    if pix.ndim != 1:
+        raise ValueError('pixel_indices must be a 1D array')
+    if coeff_power not in (1, 2):
+        raise ValueError('coeff_power must be 1 or 2')
+    return _capi.back_project(g, view.reshape((1,) + tuple(view.shape)), pix, coeff_power=coeff_power)
+
+
+def _on_device(x, device, dtype):
+    if isinstance(x, torch.Tensor):
+        return x.to(device=device, dtype=dtype).contiguous()
+    return torch.as_tensor(np.ascontiguousarray(x), device=device).to(dtype).contiguous()

@@ -27,7 +27,8 @@ import numpy as np
 import torch
 
 from . import _capi
-from .tomography_model import TomographyModel
+from .tomography_model import (TomographyModel, back_project_one_view, forward_project_one_view,
+                               translation_max_magnification)
 from .parallel_beam import _host
 
 
@@ -79,9 +80,23 @@ class TranslationModel(TomographyModel):
         recon_shape, delta_recon_row, translation_vectors, sdd = self.get_params(
             ['recon_shape', 'delta_recon_row', 'translation_vectors', 'source_detector_dist'])
         ty = np.asarray(translation_vectors, dtype=np.float64)[:, 1]
-        y_max = delta_recon_row * 0.5 * (recon_shape[0] - 1) - float(np.min(ty))
-        inv = 1.0 / self.get_magnification() - y_max / sdd
-        return 0.0 if inv <= 1e-6 else 1.001 / inv
+        return translation_max_magnification(delta_recon_row, recon_shape[0], float(np.min(ty)),
+                                             self.get_magnification(), sdd)
+
+    @staticmethod
+    def forward_project_pixel_batch_to_one_view(voxel_values, pixel_indices, translation_vector, projector_params):
+        """translation_model.py:190-242: (N, S) voxel cylinders at pixel_indices -> the (R, C) view of the object
+        translated by translation_vector, on the CUDA projector (a one-view geometry)."""
+        return forward_project_one_view(_capi.MBX_GEOM_TRANSLATION, voxel_values, pixel_indices, translation_vector,
+                                        projector_params)
+
+    @staticmethod
+    def back_project_one_view_to_pixel_batch(sinogram_view, pixel_indices, single_view_params, projector_params,
+                                             coeff_power=1):
+        """translation_model.py:382-410: the (R, C) view -> (N, S) voxel cylinders at pixel_indices, with
+        coefficients A ** coeff_power, on the CUDA projector (a one-view geometry)."""
+        return back_project_one_view(_capi.MBX_GEOM_TRANSLATION, sinogram_view, pixel_indices, single_view_params,
+                                     projector_params, coeff_power)
 
     def get_psf_radius(self):
         """translation_model.py:109-140 in float32 as the reference's jnp scalars: detector elements on either

@@ -12,14 +12,15 @@ imports it: its compute path is the CUDA library and fails loudly when that libr
 Parity pins: the qGGMRF restatement is checked against the reference's golden gradient/Hessian
 vectors (``tests/golden/qggmrf_golden.json``, extracted from the reference test file by
 ``tests/golden/make_qggmrf_golden.py``).  The projectors are pinned by the reference's structural
-tests (adjointness, Hessian finite difference, view batching) because the reference itself (JAX) is
-not installable offline.
+tests (adjointness, Hessian finite difference, view batching) and by its end-to-end acceptance bounds (FBP,
+FDK, VCD and the denoiser against their phantoms at the reference's own sizes,
+``tests/golden/acceptance_bounds.json``), because the reference itself (JAX) is not installable offline.
 """
 
 from .geometry import OracleGeometry, parallel_geometry, cone_geometry, translation_geometry  # noqa: F401
 from .projectors import (  # noqa: F401
     sparse_forward_project, sparse_back_project, forward_project, back_project,
-    compute_hessian_diagonal,
+    compute_hessian_diagonal, forward_project_one_view, back_project_one_view,
 )
 from .qggmrf import (  # noqa: F401
     get_b_from_nbr_wts, get_2_b_tilde, qggmrf_gradient_and_hessian_at_indices, qggmrf_loss,

@@ -229,3 +229,72 @@ def test_batched_scan_shapes_are_in_range():
     assert len(shapes) == 24
     for v, r, c in shapes:
         assert 60 <= v <= 720 and 8 <= r <= 64 and 96 <= c <= 512
+
+
+def _host_device(monkeypatch):
+    """Point the models' device at the CPU, so the host logic up to the CUDA library runs here (the library
+    refuses host tensors before any launch)."""
+    import torch
+    import mbirjax_b200.tomography_model as tm
+    monkeypatch.setattr(tm, '_cuda_device', lambda: torch.device('cpu'))
+    return tm
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
+def test_one_view_geometry_matches_the_model_record(monkeypatch, kind):
+    """The per-view plugin functions (forward_project_pixel_batch_to_one_view / back_project_one_view_to_pixel_batch)
+    build, from the reference's projector_params and one view's angle or translation, the same geometry record as
+    the model's own projections, with one view."""
+    tm = _host_device(monkeypatch)
+    extra = {'det_channel_offset': 0.25} if kind == 'parallel' else {'det_channel_offset': 0.25, 'det_row_offset': -0.5}
+    model, _ = make_case(kind, views=6, rows=4, channels=20, y_spread=2.0 if kind == 'translation' else 0.0, **extra)
+    full = model._geometry()
+    view_params = np.asarray(model.get_params(model.get_params('view_params_name')), dtype=np.float32)
+    g, view_dev = tm.one_view_geometry(model._kind(), model.get_projector_params(), view_params[2])
+    for name, _ in _capi.MbxGeom._fields_:
+        if name not in ('num_views', 'angles', 'translations', 'max_magnification'):
+            assert getattr(g, name) == getattr(full, name), name
+    assert g.num_views == 1
+    assert (g.translations if kind == 'translation' else g.angles) == view_dev.data_ptr()
+    np.testing.assert_array_equal(view_dev.numpy().reshape(-1), view_params[2].reshape(-1))
+    if kind == 'translation':
+        gp = model.get_geometry_parameters()
+        assert g.max_magnification == pytest.approx(tm.translation_max_magnification(
+            gp.delta_recon_row, model.get_params('recon_shape')[0], view_params[2, 1], gp.magnification,
+            gp.source_detector_dist), rel=1e-6)
+        assert 0 < g.max_magnification <= full.max_magnification   # one view's bound within all views'
+
+
+def test_one_view_plugin_functions_check_their_arguments(monkeypatch):
+    tm = _host_device(monkeypatch)
+    model, _ = make_case('parallel', views=6, rows=4, channels=20)
+    pp = model.get_projector_params()
+    nr, nc, ns = model.get_params('recon_shape')
+    fp = mb.ParallelBeamModel.forward_project_pixel_batch_to_one_view
+    bp = mb.ParallelBeamModel.back_project_one_view_to_pixel_batch
+    idx = np.arange(5, dtype=np.int32)
+    with pytest.raises(ValueError):
+        fp(np.zeros((5, ns + 1), np.float32), idx, 0.3, pp)              # slices do not match the recon
+    with pytest.raises(ValueError):
+        fp(np.zeros((4, ns), np.float32), idx, 0.3, pp)                  # one cylinder per index
+    with pytest.raises(ValueError):
+        fp(np.zeros((5, ns), np.float32), idx, np.zeros(2), pp)          # one angle per view
+    with pytest.raises(ValueError):
+        bp(np.zeros((4, 21), np.float32), idx, 0.3, pp)                  # (rows, channels) of the detector
+    with pytest.raises(ValueError):
+        bp(np.zeros((4, 20), np.float32), idx, 0.3, pp, coeff_power=3)
+    tmodel, _ = make_case('translation', views=6, rows=4, channels=20)
+    with pytest.raises(ValueError):
+        mb.TranslationModel.forward_project_pixel_batch_to_one_view(
+            np.zeros((5, tmodel.get_params('recon_shape')[2]), np.float32), idx, np.zeros(2),
+            tmodel.get_projector_params())
+    # valid arguments reach the CUDA library, which refuses host tensors before any launch
+    with pytest.raises(mb.MbxError):
+        fp(np.zeros((5, ns), np.float32), idx, 0.3, pp)
+    with pytest.raises(mb.MbxError):
+        bp(np.zeros((4, 20), np.float32), idx, 0.3, pp, coeff_power=2)
+    # the base class has no projector: it warns and returns None, as the reference's
+    with pytest.warns(UserWarning):
+        assert mb.TomographyModel.forward_project_pixel_batch_to_one_view(None, None, None, pp) is None
+    with pytest.warns(UserWarning):
+        assert mb.TomographyModel.back_project_one_view_to_pixel_batch(None, None, None, pp) is None

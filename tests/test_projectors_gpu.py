@@ -233,3 +233,31 @@ def test_autotuned_plans_agree_with_default(cuda):
             _capi.set_autotune(old)
         np.testing.assert_allclose(fp0, O.sparse_forward_project(geom, vox, sub), rtol=2e-4,
                                    atol=2e-5 * np.abs(fp0).max())
+
+
+@pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
+def test_one_view_plugin_functions(cuda, kind):
+    """The reference's per-view plugin functions (forward_project_pixel_batch_to_one_view /
+    back_project_one_view_to_pixel_batch, with projector_params as its Projectors builds them) on a one-view
+    geometry: the same view as the model's projection restricted to that view, and the oracle's one-view
+    projectors, for both coefficient powers."""
+    model, geom = make_case(kind, views=9, rows=6, channels=28)
+    nr, nc, ns = geom.recon_shape
+    rng = np.random.default_rng(11)
+    idx = rng.permutation(nr * nc)[: nr * nc // 2].astype(np.int32)
+    x = rng.standard_normal((len(idx), ns)).astype(np.float32)
+    view = rng.standard_normal(geom.sinogram_shape[1:]).astype(np.float32)
+    pp = model.get_projector_params()
+    cls = type(model)
+    view_params = np.asarray(model.get_params(model.get_params('view_params_name')), dtype=np.float32)
+    for j in (0, 4):
+        fp = cls.forward_project_pixel_batch_to_one_view(x, idx, view_params[j], pp).cpu().numpy()
+        assert fp.shape == geom.sinogram_shape[1:]
+        sub = model.sparse_forward_project(x, idx, view_indices=np.array([j], np.int32)).cpu().numpy()[0]
+        assert rel_l2(fp, sub) <= 1e-6
+        assert rel_l2(fp, O.forward_project_one_view(geom, x, idx, geom.angles[j])) <= TOL
+        for power in (1, 2):
+            bp = cls.back_project_one_view_to_pixel_batch(view, idx, view_params[j], pp, coeff_power=power)
+            bp = bp.cpu().numpy()
+            assert bp.shape == (len(idx), ns)
+            assert rel_l2(bp, O.back_project_one_view(geom, view, idx, geom.angles[j], coeff_power=power)) <= TOL
