@@ -96,6 +96,71 @@ def gen_cube_phantom(recon_shape, device='cpu'):
     return torch.as_tensor(phantom, dtype=torch.float32, device=device)
 
 
+def gen_translation_phantom(recon_shape, option, words, fill_rate=0.05, font_size=20):
+    """The reference's translation-tomography phantoms (utilities.py:696-717): 'dots' (gen_dot_phantom) or
+    'text' (gen_text_phantom); float32 NumPy (rows, cols, slices)."""
+    if option == 'dots':
+        return gen_dot_phantom(recon_shape, fill_rate)
+    if option == 'text':
+        return gen_text_phantom(recon_shape, words, font_size)
+    raise ValueError(f"Unsupported phantom option: {option}")
+
+
+def gen_dot_phantom(recon_shape, fill_rate):
+    """utilities.py:720-747: the middle two thirds of the recon rows (a sixth of the rows left empty at each end)
+    each get int(cols * slices * fill_rate) ones at distinct random (col, slice) positions.  Like the reference it
+    seeds np.random with 42 and draws with np.random.choice, so the volume (and the global np.random state after
+    it) is the reference's."""
+    np.random.seed(42)
+    phantom = np.zeros(recon_shape, dtype=np.float32)
+    pad = recon_shape[0] // 6
+    row_size = recon_shape[1] * recon_shape[2]
+    ones_per_row = int(row_size * fill_rate)
+    for r in range(pad, recon_shape[0] - pad):
+        flat = phantom[r].reshape(-1)
+        flat[np.random.choice(row_size, ones_per_row, replace=False)] = 1.0
+    return phantom
+
+
+_FALLBACK_FONTS = ("/System/Library/Fonts/Supplemental/Arial.ttf", "/Library/Fonts/Arial.ttf",
+                   "/usr/share/fonts/truetype/dejavu/DejaVuSans.ttf")
+
+
+def gen_text_phantom(recon_shape, words, font_size, font_path="DejaVuSans.ttf"):
+    """utilities.py:750-825: each word rendered in a TrueType font, binarised, rotated onto the (col, slice) plane
+    and written into one recon row; the rows are evenly spaced (row = Nr // (len(words) + 1) * (i + 1)) and the
+    words centred in columns and slices.  Needs PIL and a font (font_path, else the reference's fallback paths);
+    FileNotFoundError when there is none."""
+    from PIL import Image, ImageDraw, ImageFont
+    try:
+        font = ImageFont.truetype(font_path, size=font_size)
+    except OSError:
+        for path in _FALLBACK_FONTS:
+            if os.path.exists(path):
+                font = ImageFont.truetype(path, size=font_size)
+                break
+        else:
+            raise FileNotFoundError('Could not find a usable font. Tried the following paths:\n' +
+                                    '\n'.join(_FALLBACK_FONTS) +
+                                    '\nPlease install one of these fonts or specify a valid font_path.')
+    nr, nc, ns = recon_shape
+    size = int(min(nc, ns))
+    phantom = np.zeros(recon_shape, dtype=np.float32)
+    for i, word in enumerate(words):
+        r, c, s = nr // (len(words) + 1) * (i + 1), nc // 2, ns // 2
+        img = Image.new('L', (size, size), 0)
+        draw = ImageDraw.Draw(img)
+        left, top, right, bottom = draw.textbbox((0, 0), word, font=font)
+        draw.text(((size - (right - left)) // 2 - left, (size - (bottom - top)) // 2 - top), word, fill=1, font=font)
+        glyphs = (np.array(img.rotate(-90, expand=True).transpose(Image.FLIP_LEFT_RIGHT)) > 0).astype(np.float32)
+        c0 = max(0, c - size // 2)
+        c1 = min(nc, c0 + size)
+        s0 = max(0, s - size // 2)
+        s1 = min(ns, s0 + size)
+        phantom[max(0, r):min(nr, r + 1), c0:c1, s0:s1] = glyphs[:c1 - c0, :s1 - s0]
+    return phantom
+
+
 def add_noise(sinogram, rel_sigma, seed):
     """sinogram + N(0, (rel_sigma * max|sinogram|)^2), seeded."""
     g = torch.Generator(device=sinogram.device).manual_seed(int(seed) + 1000)

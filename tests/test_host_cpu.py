@@ -298,3 +298,36 @@ def test_one_view_plugin_functions_check_their_arguments(monkeypatch):
         assert mb.TomographyModel.forward_project_pixel_batch_to_one_view(None, None, None, pp) is None
     with pytest.warns(UserWarning):
         assert mb.TomographyModel.back_project_one_view_to_pixel_batch(None, None, None, pp) is None
+
+
+def test_translation_phantoms(monkeypatch):
+    """gen_translation_phantom (utilities.py:696-825 of the reference): 'dots' seeds np.random with 42 and fills
+    the middle rows with exactly int(cols * slices * fill_rate) distinct ones each; 'text' needs a TrueType font
+    and says so when there is none; other options are refused."""
+    from mbirjax_b200.utilities import gen_translation_phantom
+    shape = (12, 10, 8)
+    p = gen_translation_phantom(shape, 'dots', None, fill_rate=0.25)
+    assert p.dtype == np.float32 and p.shape == shape
+    assert set(np.unique(p)) <= {0.0, 1.0}
+    counts = p.reshape(12, -1).sum(axis=1)
+    np.testing.assert_array_equal(counts, [0, 0] + [20] * 8 + [0, 0])       # pad 12 // 6 = 2 rows each side
+    after = np.random.rand()
+    np.testing.assert_array_equal(gen_translation_phantom(shape, 'dots', None, fill_rate=0.25), p)
+    assert np.random.rand() == after                                          # same draws from seed 42 each call
+    with pytest.raises(ValueError):
+        gen_translation_phantom(shape, 'squares', None)
+    try:
+        t = gen_translation_phantom((40, 48, 48), 'text', ['ab', 'cd'], font_size=12)
+    except FileNotFoundError as e:
+        assert 'font' in str(e)                                                  # no TrueType font on this machine
+    else:
+        assert t.shape == (40, 48, 48) and set(np.unique(t)) <= {0.0, 1.0}
+    # the rendering itself, with PIL's built-in scalable font standing in for a TrueType file
+    from PIL import ImageFont
+    builtin = ImageFont.load_default(size=12)
+    monkeypatch.setattr(ImageFont, 'truetype', lambda *args, **kwargs: builtin)
+    t = gen_translation_phantom((40, 48, 48), 'text', ['ab', 'cd'], font_size=12)
+    assert t.shape == (40, 48, 48) and set(np.unique(t)) <= {0.0, 1.0}
+    assert np.flatnonzero(t.reshape(40, -1).sum(axis=1)).tolist() == [13, 26]   # rows 40 // 3 * (1, 2)
+    cols, slices = np.nonzero(t[13])
+    assert 10 < cols.mean() < 38 and 10 < slices.mean() < 38                       # centred in the plane
