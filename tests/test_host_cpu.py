@@ -331,3 +331,18 @@ def test_translation_phantoms(monkeypatch):
     assert np.flatnonzero(t.reshape(40, -1).sum(axis=1)).tolist() == [13, 26]   # rows 40 // 3 * (1, 2)
     cols, slices = np.nonzero(t[13])
     assert 10 < cols.mean() < 38 and 10 < slices.mean() < 38                       # centred in the plane
+
+
+def test_geometry_validation_as_the_reference():
+    """verify_valid_params of the geometries (parallel_beam.py:72-92, cone_beam.py:82-108): one angle per view, a
+    parallel recon with one slice per detector row, and a warning (not an error) for a cone angle over 45
+    degrees."""
+    with pytest.raises(ValueError, match='view dependent'):
+        mb.ParallelBeamModel((8, 4, 16), np.zeros(7))
+    with pytest.raises(ValueError, match='view dependent'):
+        mb.ConeBeamModel((8, 4, 16), np.zeros(9), source_detector_dist=64, source_iso_dist=32)
+    with pytest.warns(UserWarning, match='45 degrees'):
+        mb.ConeBeamModel((8, 40, 16), np.zeros(8), source_detector_dist=10, source_iso_dist=5)
+    model = mb.ParallelBeamModel((8, 4, 16), np.zeros(8))
+    with pytest.raises(ValueError, match='slices'):
+        model.set_params(recon_shape=(16, 16, 5))
