@@ -85,6 +85,10 @@ class TomographyModel(ParameterHandler):
     def get_geometry_parameters(self):
         raise NotImplementedError
 
+    def auto_set_recon_size(self, sinogram_shape, no_compile=True, no_warning=False):
+        """tomography_model.py:858-861: each geometry sets its own default recon size."""
+        raise NotImplementedError('auto_set_recon_size must be implemented by each specific geometry model.')
+
     def get_projector_params(self):
         """(sinogram_shape, recon_shape, geometry_params): the projector_params argument of the per-view plugin
         functions, as the reference's Projectors builds it (projectors.py:44-53)."""
