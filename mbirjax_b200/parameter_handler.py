@@ -215,6 +215,35 @@ class ParameterHandler:
         return Param(val, flag)
 
     @staticmethod
+    def convert_arrays_to_strings(cur_params):
+        """{name: Param}: array values become the ':ARRAY:' string of their flattened values (7 decimals) with a
+        ``shape`` attribute on the Param, other values lose their NumPy scalar types (parameter_handler.py:122-145).
+        The reference's loop assigns the original value back after the string, so there arrays stay arrays; here
+        they become strings, as its docstring says and as its file writer (serialize_parameter) does."""
+        for entry in cur_params.values():
+            val = entry.val
+            if isinstance(val, np.ndarray) or _is_tensor(val):
+                arr = _as_numpy(val)
+                entry.val = ParameterHandler.array_prefix + " ".join(f"{x:.7f}" for x in arr.flatten())
+                entry.shape = arr.shape
+            else:
+                entry.val = _normalize_scalar(val)
+        return cur_params
+
+    @staticmethod
+    def convert_strings_to_arrays(cur_params):
+        """{name: Param}: ':ARRAY:' strings become arrays of the Param's ``shape`` attribute, which is then
+        removed (parameter_handler.py:147-172)."""
+        prefix = ParameterHandler.array_prefix
+        for entry in cur_params.values():
+            val = entry.val
+            if isinstance(val, str) and val.startswith(prefix):
+                body = val[len(prefix):].replace('[', '').replace(']', '').split()
+                entry.val = np.array([float(v) for v in body]).reshape(entry.shape)
+                del entry.shape
+        return cur_params
+
+    @staticmethod
     def is_flat_iterable(x):
         return isinstance(x, Iterable) and isinstance(x, Sized) and not isinstance(x, (str, bytes))
 

@@ -145,3 +145,17 @@ def test_hdf5_without_h5py_says_so(monkeypatch, tmp_path):
     model, _ = make_case('parallel', views=8, rows=4, channels=16)
     with pytest.raises(ImportError, match='h5py'):
         model.save_recon_hdf5(tmp_path / 'r.h5', np.zeros(model.get_params('recon_shape'), np.float32))
+
+
+def test_array_string_conversions_round_trip():
+    """ParameterHandler.convert_arrays_to_strings / convert_strings_to_arrays (parameter_handler.py:122-172): arrays
+    to ':ARRAY:' strings with their shape and back, scalars normalised, other entries untouched."""
+    ph = mb.ParameterHandler
+    params = {'angles': mb.Param(np.linspace(0, 1, 6).reshape(2, 3), True), 'sharpness': mb.Param(np.float32(0.5), False),
+              'granularity': mb.Param([1, 2], False)}
+    out = ph.convert_arrays_to_strings(params)
+    assert out['angles'].val.startswith(ph.array_prefix) and out['angles'].shape == (2, 3)
+    assert type(out['sharpness'].val) is float and out['granularity'].val == [1, 2]
+    back = ph.convert_strings_to_arrays(out)
+    np.testing.assert_allclose(back['angles'].val, np.linspace(0, 1, 6).reshape(2, 3), atol=1e-7)
+    assert not hasattr(back['angles'], 'shape')
