@@ -1,8 +1,8 @@
 """CPU tests of the models' host logic end to end, with the oracle answering the library calls
 (``fake_library.oracle_library``): the VCD iteration loop of ``recon`` / ``prox_map`` (partitions and the
 np.random order of their subsets, the initial alpha, the statistics and the stopping rule), the denoiser's loop,
-FBP/FDK, and the geometry records of the per-view plugin functions.  The GPU tests check the same host code
-with the CUDA library underneath."""
+FBP/FDK, the geometry records of the per-view plugin functions and the autograd wrappers.  The GPU tests check
+the same host code with the CUDA library underneath."""
 import numpy as np
 import pytest
 
@@ -73,8 +73,9 @@ def test_prox_map_host_loop_matches_oracle(oracle_library):
     model, geom = make_case('parallel', views=16, rows=4, channels=24)
     ph, sino, _ = _phantom_and_sino(geom, 4, False)
     sigma_y, sigma_x, sigma_prox = O.auto_regularization(geom, sino, None, 30.0, 0.0)
-    model.set_params(sigma_y=float(sigma_y), sigma_x=float(sigma_x), sigma_prox=float(sigma_prox), granularity=[2],
-                     partition_sequence=[0], verbose=0, positivity_flag=True)
+    with pytest.warns(UserWarning, match='regularization'):
+        model.set_params(sigma_y=float(sigma_y), sigma_x=float(sigma_x), sigma_prox=float(sigma_prox),
+                         granularity=[2], partition_sequence=[0], verbose=0, positivity_flag=True)
     prox = (ph + np.random.default_rng(9).normal(0, 0.05, ph.shape)).astype(np.float32)
     np.random.seed(4)
     rec, loss = model.prox_map(prox, sino, max_iterations=2, stop_threshold_change_pct=0, logfile_path=None,
@@ -140,3 +141,48 @@ def test_one_view_records_give_the_oracle_view(oracle_library, kind):
         bp = cls.back_project_one_view_to_pixel_batch(view, idx, views[j], pp, coeff_power=2).numpy()
         np.testing.assert_allclose(bp, O.back_project_one_view(geom, view, idx, geom.angles[j], coeff_power=2),
                                    rtol=1e-6, atol=1e-6)
+
+
+def test_autograd_pair_host_logic(oracle_library):
+    """mbirjax_b200.autograd on the host: the gradient of <A x, y> is A^T y on the region of reconstruction (zero
+    outside), the view-chunked backward adds the same chunks, and the gradient of the weighted least-squares +
+    qGGMRF loss matches central differences of the float64 oracle loss."""
+    import torch
+    from mbirjax_b200 import autograd as AG
+    model, geom = make_case('cone', views=10, rows=4, channels=16)
+    rng = np.random.default_rng(0)
+    x = torch.tensor(rng.random(geom.recon_shape), dtype=torch.float32, requires_grad=True)
+    y = torch.tensor(rng.random(geom.sinogram_shape), dtype=torch.float32)
+    (gx,) = torch.autograd.grad(torch.sum(AG.forward_project(x, model) * y), x)
+    aty = AG.back_project(y, model)
+    torch.testing.assert_close(gx, aty, rtol=1e-6, atol=1e-6)
+    mask = O.get_2d_ror_mask(geom.recon_shape)[:, :, None].astype(bool)
+    assert not np.any(gx.numpy()[~np.broadcast_to(mask, geom.recon_shape)])
+    (gx3,) = torch.autograd.grad(torch.sum(AG.forward_project(x, model, 3) * y), x)
+    torch.testing.assert_close(gx3, gx, rtol=1e-5, atol=1e-5)
+
+    params = (O.get_b_from_nbr_wts([1, 1, 1]), 0.3, 2.0, 1.2, 1.0)
+    x64 = (rng.random(geom.recon_shape) * mask).astype(np.float64)
+    y64 = O.forward_project(geom, (0.8 * x64).astype(np.float32), dtype=np.float64)
+    w64 = np.exp(-y64 / y64.max())
+
+    def loss64(v):
+        r = O.forward_project(geom, v, dtype=np.float64) - y64
+        return 0.5 * float(np.sum(w64 * r * r)) + O.qggmrf_loss(v, params)
+
+    xt = torch.tensor(x64, dtype=torch.float32, requires_grad=True)
+    loss = AG.weighted_ls_qggmrf_loss(xt, model, torch.tensor(y64, dtype=torch.float32),
+                                      torch.tensor(w64, dtype=torch.float32), params)
+    (grad,) = torch.autograd.grad(loss, xt)
+    assert float(loss.detach()) == pytest.approx(loss64(x64.astype(np.float32).astype(np.float64)), rel=1e-4)
+    ror = np.argwhere(np.broadcast_to(mask, geom.recon_shape))
+    picks = ror[rng.choice(len(ror), 12, replace=False)]
+    eps = 1e-3
+    fd, ag = [], []
+    for i, j, k in picks:
+        xp, xm = x64.copy(), x64.copy()
+        xp[i, j, k] += eps
+        xm[i, j, k] -= eps
+        fd.append((loss64(xp) - loss64(xm)) / (2 * eps))
+        ag.append(float(grad[i, j, k]))
+    assert np.linalg.norm(np.array(ag) - np.array(fd)) <= 1e-3 * np.linalg.norm(fd)
