@@ -134,7 +134,9 @@ MBX_API size_t mbx_back_project_workspace_bytes(const mbx_geom *g, int64_t num_p
 /* Sparse back projection of a full sinogram (num_views, R, C) to out (num_pixels, S) (overwritten):
  *   out = scale * sum_views A^coeff_power^T (weights * sinogram)
  * over views view_indices[0..num_views_sel) (or all).  weights may be NULL (all ones); scale is 1 for the
- * reference's sparse_back_project.  coeff_power is 1 (back projection) or 2 (Hessian diagonal).
+ * reference's sparse_back_project.  coeff_power is 1 (back projection) or 2 (Hessian diagonal).  sinogram may be
+ * NULL: the values back-projected are then the weights, or 1 everywhere when weights is NULL too, which gives the
+ * Hessian diagonal of unit weights (coeff_power 2) without a sinogram-sized buffer of ones.
  * Replaces Projectors.sparse_back_project (projectors.py:131-209) over
  * ParallelBeamModel.back_project_one_view_to_pixel_batch (parallel_beam.py:180-221) /
  * ConeBeamModel.back_project_one_view_to_pixel_batch (cone_beam.py:379-541), as called by

@@ -16,6 +16,8 @@ MBX_GEOM_PARALLEL = 0
 MBX_GEOM_CONE = 1
 MBX_GEOM_TRANSLATION = 2
 MBX_MAX_PSF_RADIUS = 4
+MBX_OK, MBX_ERR_INVALID_ARG, MBX_ERR_UNSUPPORTED, MBX_ERR_CUDA, MBX_ERR_WORKSPACE = 0, -1, -2, -3, -4
+MBX_NOALLOC_SCRATCH_BYTES = 16 << 20
 
 c_int32, c_int64, c_float, c_size_t, c_void_p = (ctypes.c_int32, ctypes.c_int64, ctypes.c_float, ctypes.c_size_t,
                                                  ctypes.c_void_p)
@@ -196,15 +198,16 @@ def forward_project(geom, voxel_values, pixel_indices, view_indices=None, out=No
 
 
 def back_project(geom, sinogram, pixel_indices, view_indices=None, coeff_power=1, weights=None, scale=1.0, out=None):
-    """Full sinogram (V, R, C) -> (N, S) at pixel_indices."""
+    """Full sinogram (V, R, C) -> (N, S) at pixel_indices.  sinogram None: back-projects the weights, or ones when
+    weights is None too (the unit-weight Hessian diagonal with coeff_power=2, with no buffer of ones)."""
     lib = load_library()
     _require_cuda(sinogram, pixel_indices, view_indices, weights)
     n = int(pixel_indices.shape[0])
     nv = int(view_indices.shape[0]) if view_indices is not None else geom.num_views
     if out is None:
-        out = torch.empty((n, geom.num_recon_slices), dtype=torch.float32, device=sinogram.device)
+        out = torch.empty((n, geom.num_recon_slices), dtype=torch.float32, device=pixel_indices.device)
     nbytes = lib.mbx_back_project_workspace_bytes(ctypes.byref(geom), n, nv)
-    ws, nbytes = _workspace(nbytes, sinogram.device)
+    ws, nbytes = _workspace(nbytes, pixel_indices.device)
     rc = lib.mbx_sparse_back_project(ctypes.byref(geom), _ptr(sinogram), _ptr(weights), _ptr(pixel_indices), n,
                                      _ptr(view_indices), nv, int(coeff_power), float(scale), _ptr(out), _ptr(ws),
                                      nbytes, _stream())
@@ -222,7 +225,7 @@ def back_project_noalloc(geom, sinogram, pixel_indices, view_indices=None, coeff
     n = int(pixel_indices.shape[0])
     nv = int(view_indices.shape[0]) if view_indices is not None else geom.num_views
     if out is None:
-        out = torch.empty((n, geom.num_recon_slices), dtype=torch.float32, device=sinogram.device)
+        out = torch.empty((n, geom.num_recon_slices), dtype=torch.float32, device=pixel_indices.device)
     rc = lib.mbx_sparse_back_project_noalloc(ctypes.byref(geom), _ptr(sinogram), _ptr(weights), _ptr(pixel_indices),
                                              n, _ptr(view_indices), nv, int(coeff_power), float(scale), _ptr(out),
                                              _stream())

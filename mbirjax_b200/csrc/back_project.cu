@@ -34,14 +34,8 @@ static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const fl
                                   const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
                                   float *dst, long long ss, cudaStream_t st) {
     auto kern = bp_fast_kernel<KIND>;
-    static bool attr_set[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) attr_set[dev] = true;
-    }
+    cudaError_t ea = set_max_dynamic_smem(reinterpret_cast<const void *>(kern), 100 * 1024);
+    if (ea != cudaSuccess) return ea;
     BpArgs A;
     A.g = g;
     A.sino = sino;
@@ -160,10 +154,14 @@ extern "C" int mbx_sparse_back_project(const mbx_geom *g, const float *sinogram,
                                        void *workspace, size_t workspace_bytes, void *stream) {
     int rc = mbx::validate_geom(g);
     if (rc != MBX_OK) return rc;
-    if (num_pixels < 0 || num_views_sel <= 0 || !sinogram) return MBX_ERR_INVALID_ARG;
+    if (num_pixels < 0 || num_views_sel <= 0) return MBX_ERR_INVALID_ARG;
     if (num_pixels > 0 && (!pixel_indices || !out)) return MBX_ERR_INVALID_ARG;
     if (coeff_power != 1 && coeff_power != 2) return MBX_ERR_UNSUPPORTED;
     if (!view_indices && num_views_sel > g->num_views) return MBX_ERR_INVALID_ARG;
+    if (!sinogram) {  // no sinogram: the values are the weights, or 1 everywhere when there are none either
+        sinogram = weights;
+        weights = nullptr;
+    }
     return mbx::back_project(*g, sinogram, weights, pixel_indices, num_pixels, view_indices, num_views_sel,
                              coeff_power, scale, out, workspace, workspace_bytes, static_cast<cudaStream_t>(stream));
 }

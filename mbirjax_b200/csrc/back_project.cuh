@@ -16,7 +16,7 @@ constexpr int BP_MAX_CACHE_ROWS = 96;
 __device__ __forceinline__ float gather_row(const float *__restrict__ row, const float *__restrict__ wrow, int n,
                                             int num_channels) {
     const int nn = min(max(n, 0), num_channels - 1);  // clamped gather, as the reference's jnp indexing
-    float v = __ldg(row + nn);
+    float v = row ? __ldg(row + nn) : 1.0f;            // no sinogram: every value is 1 (unit-weight Hessian)
     if (wrow) v *= __ldg(wrow + nn);
     return v;
 }
@@ -25,7 +25,7 @@ template <int MAXR>
 __device__ __forceinline__ float horizontal_row_sum(const float *__restrict__ view, const float *__restrict__ wview,
                                                     int m, int num_channels, int n_c, const float (&a)[2 * MAXR + 1]) {
     const long long off = (long long)m * num_channels;
-    const float *row = view + off;
+    const float *row = view ? view + off : nullptr;
     const float *wrow = wview ? wview + off : nullptr;
     float c = 0.0f;
 #pragma unroll
@@ -121,7 +121,7 @@ bp_kernel(const mbx_geom g, const float *__restrict__ sino, const float *__restr
                                                                  : channel_coeff(g, f, k);
                 a[k + MAXR] = (coeff_power == 2) ? c * c : c;
             }
-            const float *view = sino + (long long)vi * num_rows * num_channels;
+            const float *view = sino ? sino + (long long)vi * num_rows * num_channels : nullptr;
             const float *wview = wts ? wts + (long long)vi * num_rows * num_channels : nullptr;
             if (KIND == MBX_GEOM_PARALLEL) {
 #pragma unroll
@@ -240,13 +240,8 @@ static cudaError_t launch_bp_t(const mbx_geom &g, const BpPlan &pl, const float 
                                const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
                                float *dst, long long ss, cudaStream_t st) {
     auto kern = bp_kernel<KIND, MAXR, ST>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             BP_MAX_CACHE_ROWS * BP_THREADS * 4);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    cudaError_t ea = set_max_dynamic_smem(reinterpret_cast<const void *>(kern), BP_MAX_CACHE_ROWS * BP_THREADS * 4);
+    if (ea != cudaSuccess) return ea;
     dim3 grid(pl.gx, pl.gy, pl.splits);
     kern<<<grid, BP_THREADS, pl.smem, st>>>(g, sino, w, pix, n, views, nv, pl.views_per_split, cp, scale, dst, ss,
                                             pl.cache_rows, device_error_ptr());

@@ -250,7 +250,11 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
         if (KIND == MBX_GEOM_PARALLEL) {
             // three taps at constant offsets from one 32-bit element offset, one detector row per slice
             int o = voff + s0c + first;
-            if (wts) {
+            if (!sino) {  // unit sinogram: the same additions as gathering ones (unit-weight Hessian)
+#pragma unroll
+                for (int s = 0; s < BPF_ST; ++s)
+                    if (s < ns) acc[s] = fa.y + (fa.z + (fa.w + acc[s]));
+            } else if (wts) {
 #pragma unroll
                 for (int s = 0; s < BPF_ST; ++s) {
                     if (s < ns) {
@@ -297,7 +301,9 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 if (m >= 0 && m < num_rows) {
                     const int o = voff + m * num_channels + first;
                     const float *q = sino + o;
-                    if (wts) {
+                    if (!sino) {  // unit sinogram
+                        c = fa.y + (fa.z + fa.w);
+                    } else if (wts) {
                         const float *qw = wts + o;
                         c = fmaf(fa.y, __ldg(q) * __ldg(qw), fmaf(fa.z, __ldg(q + 1) * __ldg(qw + 1), fa.w * (__ldg(q + 2) * __ldg(qw + 2))));
                     } else {

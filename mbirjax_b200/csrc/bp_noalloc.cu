@@ -51,11 +51,15 @@ extern "C" int mbx_sparse_back_project_noalloc(const mbx_geom *g, const float *s
                                                int32_t coeff_power, float scale, float *out, void *stream) {
     int rc = mbx::validate_geom(g);
     if (rc != MBX_OK) return rc;
-    if (num_pixels < 0 || num_views_sel <= 0 || !sinogram) return MBX_ERR_INVALID_ARG;
+    if (num_pixels < 0 || num_views_sel <= 0) return MBX_ERR_INVALID_ARG;
     if (num_pixels > 0 && (!pixel_indices || !out)) return MBX_ERR_INVALID_ARG;
     if (coeff_power != 1 && coeff_power != 2) return MBX_ERR_UNSUPPORTED;
     if (!view_indices && num_views_sel > g->num_views) return MBX_ERR_INVALID_ARG;
     if (num_pixels == 0) return MBX_OK;
+    if (!sinogram) {  // as mbx_sparse_back_project: the weights, or 1 everywhere
+        sinogram = weights;
+        weights = nullptr;
+    }
     const size_t need = mbx::bp_workspace_bytes(*g, num_pixels, num_views_sel);
     if (need > MBX_NOALLOC_SCRATCH_BYTES) return MBX_ERR_WORKSPACE;  // more scratch than the static array holds
     void *scratch = nullptr;

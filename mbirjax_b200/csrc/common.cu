@@ -4,6 +4,8 @@
 #include <cstdio>
 #include <map>
 #include <mutex>
+#include <set>
+#include <utility>
 #include <vector>
 
 #include "mbx_common.cuh"
@@ -15,21 +17,38 @@ __device__ int g_mbx_device_error = 0;
 namespace mbx {
 
 int *device_error_ptr() {
-    static int *cache[64] = {nullptr};
+    static std::atomic<int *> cache[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
         return nullptr;
     }
-    if (!cache[dev]) {
+    int *c = cache[dev].load(std::memory_order_acquire);
+    if (!c) {
         void *p = nullptr;
         if (cudaGetSymbolAddress(&p, g_mbx_device_error) != cudaSuccess) {
             cudaGetLastError();
             return nullptr;
         }
-        cache[dev] = static_cast<int *>(p);
+        c = static_cast<int *>(p);
+        cache[dev].store(c, std::memory_order_release);  // every thread that races here stores the same address
     }
-    return cache[dev];
+    return c;
+}
+
+static std::mutex g_attr_mutex;
+static std::set<std::pair<const void *, int>> g_attr_done;
+
+cudaError_t set_max_dynamic_smem(const void *func, int bytes) {
+    int dev = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e != cudaSuccess) return e;
+    std::lock_guard<std::mutex> lock(g_attr_mutex);
+    const auto key = std::make_pair(func, dev);
+    if (g_attr_done.count(key)) return cudaSuccess;
+    e = cudaFuncSetAttribute(func, cudaFuncAttributeMaxDynamicSharedMemorySize, bytes);
+    if (e == cudaSuccess) g_attr_done.insert(key);
+    return e;
 }
 
 static std::atomic<int> g_autotune{1};
@@ -83,21 +102,21 @@ int set_cuda_error(cudaError_t e) {
 }
 
 int num_sms() {
-    static int cache[64] = {0};
+    static std::atomic<int> cache[64] = {};
     int dev = 0;
     if (cudaGetDevice(&dev) != cudaSuccess || dev < 0 || dev >= 64) {
         cudaGetLastError();
         return kNumSMsDefault;
     }
-    if (cache[dev] == 0) {
-        int n = 0;
+    int n = cache[dev].load(std::memory_order_relaxed);
+    if (n == 0) {
         if (cudaDeviceGetAttribute(&n, cudaDevAttrMultiProcessorCount, dev) != cudaSuccess || n <= 0) {
             cudaGetLastError();
             n = kNumSMsDefault;
         }
-        cache[dev] = n;
+        cache[dev].store(n, std::memory_order_relaxed);
     }
-    return cache[dev];
+    return n;
 }
 
 int validate_geom(const mbx_geom *g) {

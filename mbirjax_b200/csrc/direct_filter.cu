@@ -98,12 +98,10 @@ extern "C" int mbx_direct_filter(const mbx_geom *g, const float *sinogram, float
     const int C = g->num_det_channels, R = g->num_det_rows;
     const size_t smem = ((size_t)C * mbx::FILT_ROWS + 2 * (size_t)C - 1) * sizeof(float);
     if (smem > 200 * 1024) return MBX_ERR_UNSUPPORTED;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(mbx::direct_filter_kernel, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             200 * 1024);
+    {
+        cudaError_t e = mbx::set_max_dynamic_smem(reinterpret_cast<const void *>(mbx::direct_filter_kernel),
+                                                  200 * 1024);
         if (e != cudaSuccess) return mbx::set_cuda_error(e);
-        attr_set = true;
     }
     const long long rows_total = (long long)g->num_views * R;
     const double pi = 3.14159265358979323846;

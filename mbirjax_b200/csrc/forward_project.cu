@@ -203,12 +203,8 @@ static cudaError_t launch_fp_t(const mbx_geom &g, const FpPlan &pl, const float 
                                long long num_pixels, const int32_t *views, int num_views_sel, float *dst,
                                long long split_stride, cudaStream_t st) {
     auto kern = fp_kernel<KIND, MAXR, MAXRBP>;
-    static bool attr_set = false;
-    if (!attr_set) {
-        cudaError_t e = cudaFuncSetAttribute(kern, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        if (e != cudaSuccess) return e;
-        attr_set = true;
-    }
+    cudaError_t ea = set_max_dynamic_smem(reinterpret_cast<const void *>(kern), 200 * 1024);
+    if (ea != cudaSuccess) return ea;
     dim3 grid(num_views_sel, pl.tiles, pl.splits), block(pl.bx, pl.by);
     kern<<<grid, block, pl.smem, st>>>(g, vox, pix, num_pixels, views, dst, pl.row_tile, pl.c_pad,
                                        pl.pixels_per_split, split_stride, device_error_ptr());
@@ -239,15 +235,8 @@ size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views
 
 template <int KIND, int MINB>
 static cudaError_t launch_fp_cb_v(const FpArgs &A, cudaStream_t st) {
-    static bool attr_set[64] = {false};
-    int dev = 0;
-    cudaGetDevice(&dev);
-    if (dev < 0 || dev >= 64 || !attr_set[dev]) {
-        cudaError_t e = cudaFuncSetAttribute(fp_cb_kernel<KIND, MINB>, cudaFuncAttributeMaxDynamicSharedMemorySize,
-                                             200 * 1024);
-        if (e != cudaSuccess) return e;
-        if (dev >= 0 && dev < 64) attr_set[dev] = true;
-    }
+    cudaError_t ea = set_max_dynamic_smem(reinterpret_cast<const void *>(fp_cb_kernel<KIND, MINB>), 200 * 1024);
+    if (ea != cudaSuccess) return ea;
     dim3 grid(A.num_views_sel, A.plan.cblocks);
     fp_cb_kernel<KIND, MINB><<<grid, CB_THREADS, A.plan.smem, st>>>(A, device_error_ptr());
     note_launch();

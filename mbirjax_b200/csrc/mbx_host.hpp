@@ -26,6 +26,11 @@ int validate_geom(const mbx_geom *g);
 // Device address of the error word of the current device (cached per device; NULL if unavailable).
 int *device_error_ptr();
 
+// cudaFuncSetAttribute(func, MaxDynamicSharedMemorySize, bytes) once per (kernel, device), under a mutex, so that
+// host threads launching the same kernel on one or several devices neither race on the record of what is set
+// nor skip a device.
+cudaError_t set_max_dynamic_smem(const void *func, int bytes);
+
 size_t fp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel);
 size_t bp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views_sel);
 

@@ -886,15 +886,15 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     P.fp_minb = 2;
     // kernel attributes and resident-CTA grids
     if (P.kind == MBX_GEOM_PARALLEL) {
-        cudaFuncSetAttribute(b_bp<MBX_GEOM_PARALLEL>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-        cudaFuncSetAttribute(b_fp<MBX_GEOM_PARALLEL, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(b_fp<MBX_GEOM_PARALLEL, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        set_max_dynamic_smem(reinterpret_cast<const void *>(b_bp<MBX_GEOM_PARALLEL>), 100 * 1024);
+        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 2>), 200 * 1024);
+        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>), 200 * 1024);
         P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, smem_bp, L.bp_total);
         P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, smem_fp, L.fp_total);
     } else {
-        cudaFuncSetAttribute(b_bp<MBX_GEOM_CONE>, cudaFuncAttributeMaxDynamicSharedMemorySize, 100 * 1024);
-        cudaFuncSetAttribute(b_fp<MBX_GEOM_CONE, 2>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
-        cudaFuncSetAttribute(b_fp<MBX_GEOM_CONE, 3>, cudaFuncAttributeMaxDynamicSharedMemorySize, 200 * 1024);
+        set_max_dynamic_smem(reinterpret_cast<const void *>(b_bp<MBX_GEOM_CONE>), 100 * 1024);
+        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 2>), 200 * 1024);
+        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>), 200 * 1024);
         P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_CONE>, smem_bp, L.bp_total);
         P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, smem_fp, L.fp_total);
     }

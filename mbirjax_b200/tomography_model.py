@@ -226,9 +226,8 @@ class TomographyModel(ParameterHandler):
                                                                                            sinogram_shape))
         nr, nc, ns = recon_shape
         idx = torch.arange(nr * nc, dtype=torch.int32, device=self._device())
-        if w is None:
-            w = torch.ones(tuple(sinogram_shape), dtype=torch.float32, device=self._device())
-        return _capi.back_project(self._geometry(), w, idx, coeff_power=2).reshape((nr, nc, ns))
+        # no sinogram: the library back-projects the weights, or ones for unit weights without a buffer of ones
+        return _capi.back_project(self._geometry(), None, idx, coeff_power=2, weights=w).reshape((nr, nc, ns))
 
     # ------------------------------------------------------------------ direct recon
     def direct_filter(self, sinogram, filter_name='ramp', view_batch_size=DIRECT_RECON_VIEW_BATCH_SIZE):

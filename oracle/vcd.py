@@ -6,7 +6,9 @@
 * ``vcd_partition_iterator``: ``tomography_model.py:1257-1308`` (``np.random.permutation`` subset order)
 * subset update: ``tomography_model.py:1343-1542`` and ``get_forward_lin_quad`` ``:1546-1631``
 
-Everything is float32, as the reference computes it; reductions are float32 sums.
+Everything is float32, as the reference computes it; reductions are float32 sums.  Every function takes the
+projector implementation as ``proj`` (default: the single-process ``oracle.projectors``; an
+``oracle.pool.OraclePool`` spreads the views over the host cores).
 """
 import numpy as np
 
@@ -39,7 +41,7 @@ def auto_regularization(geom, sinogram, weights=None, snr_db=30.0, sharpness=1.0
     return float(sigma_y), float(sigma_x), float(sigma_x)
 
 
-def direct_recon(geom, sinogram):
+def direct_recon(geom, sinogram, proj=P):
     if geom.kind == 'translation':  # no direct recon: the base model's zeros (tomography_model.py:934-949)
         return np.zeros(geom.recon_shape, dtype=np.float32)
     if geom.kind == 'parallel':
@@ -48,7 +50,7 @@ def direct_recon(geom, sinogram):
         filtered = fdk_filter(sinogram, geom.source_detector_dist, geom.magnification, geom.delta_voxel,
                               geom.delta_det_row, geom.delta_det_channel, geom.det_row_offset,
                               geom.det_channel_offset)
-    return P.back_project(geom, filtered)
+    return proj.back_project(geom, filtered)
 
 
 def forward_model_loss(error_sinogram, sigma_y, weights=None):
@@ -59,7 +61,7 @@ def forward_model_loss(error_sinogram, sigma_y, weights=None):
 
 
 def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pixel_indices, fm_constant,
-                      qggmrf_params, prox_input=None, sigma_prox=None, positivity=False):
+                      qggmrf_params, prox_input=None, sigma_prox=None, positivity=False, proj=P):
     """One subset step; returns (flat_recon, error_sinogram, ell1, alpha).
 
     prox_input (flat, like flat_recon): the proximal-map prior of tomography_model.py:1388-1391 instead of qGGMRF,
@@ -75,12 +77,12 @@ def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pix
                       (flat_recon[pixel_indices] - prox_input[pixel_indices])).astype(f32)
         prior_hess = f32(sigma_prox) ** 2
     wes = error_sinogram if weights is None else (weights * error_sinogram).astype(f32)
-    forward_grad = (-fm_constant * P.sparse_back_project(geom, wes, pixel_indices)).astype(f32)
+    forward_grad = (-fm_constant * proj.sparse_back_project(geom, wes, pixel_indices)).astype(f32)
     forward_hess = (fm_constant * fm_hessian[pixel_indices]).astype(f32)
     delta = (-((forward_grad + prior_grad) / (forward_hess + prior_hess))).astype(f32)
     prior_linear = np.sum(prior_grad * delta, dtype=f32)
     prior_quad = f32(0.5) * np.sum(prior_hess * delta ** 2, dtype=f32)
-    delta_sino = P.sparse_forward_project(geom, delta, pixel_indices)
+    delta_sino = proj.sparse_forward_project(geom, delta, pixel_indices)
     forward_linear = f32(fm_constant) * np.sum(wes * delta_sino, dtype=f32)
     w = 1 if weights is None else weights
     forward_quad = f32(fm_constant) * np.sum(delta_sino * delta_sino * w, dtype=f32)
@@ -89,7 +91,7 @@ def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pix
     if positivity:
         pos_constant = f32(1.0) / (alpha + EPS_F32)
         delta = np.maximum(-pos_constant * flat_recon[pixel_indices], delta).astype(f32)
-        delta_sino = P.sparse_forward_project(geom, delta, pixel_indices)
+        delta_sino = proj.sparse_forward_project(geom, delta, pixel_indices)
     delta = (alpha * delta).astype(f32)
     flat_recon = flat_recon.copy()
     np.add.at(flat_recon, pixel_indices, delta)
@@ -100,22 +102,22 @@ def vcd_subset_update(geom, flat_recon, error_sinogram, weights, fm_hessian, pix
 
 def vcd_recon(geom, sinogram, partitions, partition_sequence, *, sigma_y, sigma_x, p=2.0, q=1.2, T=1.0,
               qggmrf_nbr_wts=(1.0, 1.0, 1.0), weights=None, init_recon=None, stop_threshold_change_pct=0.0,
-              prox_input=None, sigma_prox=None, positivity=False):
+              prox_input=None, sigma_prox=None, positivity=False, proj=P):
     """Returns (recon, dict(fm_rmse, nmae_update, alpha_values))."""
     f32 = np.float32
     sinogram = np.asarray(sinogram, dtype=f32)
     if init_recon is None:
-        init_recon = direct_recon(geom, sinogram)
+        init_recon = direct_recon(geom, sinogram, proj)
     elif isinstance(init_recon, int) and init_recon == 0:
         init_recon = np.zeros(geom.recon_shape, dtype=f32)
     init_recon = np.asarray(init_recon, dtype=f32)
-    es = P.forward_project(geom, init_recon)
+    es = proj.forward_project(geom, init_recon)
     wes = es if weights is None else (weights * es).astype(f32)
     norm = np.sum(wes * es, dtype=f32)
     alpha = np.sum(wes * sinogram, dtype=f32) / norm if norm > 0 else f32(1)
     error_sinogram = (sinogram - alpha * es).astype(f32)
     recon = (alpha * init_recon).astype(f32)
-    fm_hessian = P.compute_hessian_diagonal(geom, weights).reshape((-1, geom.recon_shape[2]))
+    fm_hessian = proj.compute_hessian_diagonal(geom, weights).reshape((-1, geom.recon_shape[2]))
     fm_constant = 1.0 / (sigma_y ** 2.0)
     b = get_b_from_nbr_wts(list(qggmrf_nbr_wts))
     qparams = (b, sigma_x, p, q, T)
@@ -128,7 +130,7 @@ def vcd_recon(geom, sinogram, partitions, partition_sequence, *, sigma_y, sigma_
         for index in np.random.permutation(partition.shape[0]):
             flat_recon, error_sinogram, ell1, a = vcd_subset_update(
                 geom, flat_recon, error_sinogram, weights, fm_hessian, partition[index], fm_constant, qparams,
-                prox_flat, sigma_prox, positivity)
+                prox_flat, sigma_prox, positivity, proj)
             ell1_sum += ell1
             alpha_sum += a
         fm_rmse.append(forward_model_loss(error_sinogram, sigma_y, weights))
@@ -142,14 +144,14 @@ def vcd_recon(geom, sinogram, partitions, partition_sequence, *, sigma_y, sigma_
 
 def recon(geom, sinogram, *, granularity, partition_sequence, max_iterations, weights=None, init_recon=None,
           snr_db=30.0, sharpness=1.0, p=2.0, q=1.2, T=1.0, qggmrf_nbr_wts=(1.0, 1.0, 1.0),
-          stop_threshold_change_pct=0.2, positivity=False):
+          stop_threshold_change_pct=0.2, positivity=False, proj=P):
     """tomography_model.py:966-1084 with the reference's np.random call order."""
     sigma_y, sigma_x, _ = auto_regularization(geom, sinogram, weights, snr_db, sharpness)
     partitions = gen_set_of_pixel_partitions(geom.recon_shape, granularity)
     seq = gen_partition_sequence(partition_sequence, max_iterations)
     out, stats = vcd_recon(geom, sinogram, partitions, seq, sigma_y=sigma_y, sigma_x=sigma_x, p=p, q=q, T=T,
                            qggmrf_nbr_wts=qggmrf_nbr_wts, weights=weights, init_recon=init_recon,
-                           stop_threshold_change_pct=stop_threshold_change_pct, positivity=positivity)
+                           stop_threshold_change_pct=stop_threshold_change_pct, positivity=positivity, proj=proj)
     stats['sigma_y'], stats['sigma_x'] = sigma_y, sigma_x
     return out, stats
 

@@ -55,6 +55,9 @@ def forward_project(geom, voxel_values, pixel_indices, view_indices=None, out=No
 
 def back_project(geom, sinogram, pixel_indices, view_indices=None, coeff_power=1, weights=None, scale=1.0, out=None):
     og = oracle_geometry_of(geom)
+    if sinogram is None:  # the library's convention: the weights, or ones when there are none either
+        sinogram = torch.ones(og.sinogram_shape, dtype=torch.float32) if weights is None else weights
+        weights = None
     sino = _np(sinogram) if weights is None else _np(weights * sinogram)
     res = O.sparse_back_project(og, sino, _np(pixel_indices), _np(view_indices), coeff_power=coeff_power)
     return torch.as_tensor(np.float32(scale) * res if scale != 1.0 else res)

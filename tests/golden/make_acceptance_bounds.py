@@ -10,7 +10,7 @@ literal bounds:
 This script reads those files as text (they are never imported or executed), pulls the literals out with
 ``ast``, and writes them as a fixture, so the tests here hold exactly the reference's numbers.
 
-Usage: python tests/golden/make_acceptance_bounds.py [path/to/reference/root]
+Usage: python tests/golden/make_acceptance_bounds.py <path/to/reference/root>  (or MBIRJAX_REFERENCE_ROOT=<root>)
 """
 import ast
 import json
@@ -65,7 +65,9 @@ def extract(reference_root):
 
 
 if __name__ == '__main__':
-    root = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MBIRJAX_REFERENCE_ROOT')
+    if not root:
+        sys.exit('usage: %s <mbirjax reference root> (or set MBIRJAX_REFERENCE_ROOT)' % sys.argv[0])
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'acceptance_bounds.json')
     with open(out, 'w') as f:
         json.dump(extract(root), f, indent=1)

@@ -4,7 +4,7 @@ The reference test ``tests/test_denoiser.py`` (``test_median_filter_3d``) filter
 3)`` and compares with a literal 3x3x3 array.  This script reads that file as text (it is never imported or
 executed), pulls the literal out with ``ast``, and writes input and expected output as a fixture.
 
-Usage: python tests/golden/make_median_golden.py [path/to/reference/root]
+Usage: python tests/golden/make_median_golden.py <path/to/reference/root>  (or MBIRJAX_REFERENCE_ROOT=<root>)
 """
 import ast
 import json
@@ -33,7 +33,9 @@ def extract(reference_root):
 
 
 if __name__ == '__main__':
-    root = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MBIRJAX_REFERENCE_ROOT')
+    if not root:
+        sys.exit('usage: %s <mbirjax reference root> (or set MBIRJAX_REFERENCE_ROOT)' % sys.argv[0])
     out = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'median_golden.json')
     with open(out, 'w') as f:
         json.dump(extract(root), f, indent=1)

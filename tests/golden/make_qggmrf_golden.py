@@ -6,7 +6,7 @@ produced for them.  This script reads that file as text (it is never imported or
 literal arrays and scalars out of the function body with ``ast``, and writes them as a fixture so that the
 tests can run where the reference tree is absent.
 
-Usage: python tests/golden/make_qggmrf_golden.py [path/to/reference/root]
+Usage: python tests/golden/make_qggmrf_golden.py <path/to/reference/root>  (or MBIRJAX_REFERENCE_ROOT=<root>)
 """
 import ast
 import json
@@ -41,7 +41,9 @@ def extract(reference_root):
 
 
 if __name__ == '__main__':
-    root = sys.argv[1] if len(sys.argv) > 1 else '/root/reference'
+    root = sys.argv[1] if len(sys.argv) > 1 else os.environ.get('MBIRJAX_REFERENCE_ROOT')
+    if not root:
+        sys.exit('usage: %s <mbirjax reference root> (or set MBIRJAX_REFERENCE_ROOT)' % sys.argv[0])
     data = extract(root)
     dst = os.path.join(os.path.dirname(os.path.abspath(__file__)), 'qggmrf_golden.json')
     with open(dst, 'w') as f:

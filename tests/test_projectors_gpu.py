@@ -27,6 +27,10 @@ CASES = [
     ('cone', dict(views=10, rows=7, channels=27, det_row_offset=0.7, det_channel_offset=-1.1,
                   recon_slice_offset=0.4)),
     ('cone', dict(views=12, rows=10, channels=30, delta_voxel=2.2)),        # psf radius 2
+    # more than 128 detector rows: several 128-row batches, each with its own row anchor, in the forward
+    # projection (cone_beam.py:336-358) and several 128-slice batches in the back projection (cone_beam.py:500-541)
+    ('cone', dict(views=8, rows=300, channels=24, sdd_factor=40.0)),
+    ('cone', dict(views=6, rows=260, channels=20, sdd_factor=30.0, sid_factor=15.0, det_row_offset=0.3)),  # mag. 2
     ('translation', dict(views=16, rows=8, channels=32)),
     ('translation', dict(views=12, rows=10, channels=30, sid_factor=2.0)),  # magnification 2
     ('translation', dict(views=10, rows=7, channels=27, det_row_offset=0.7, det_channel_offset=-1.1,
@@ -72,6 +76,9 @@ def test_forward_back_parity(cuda, kind, kw):
     h_gpu = model.sparse_back_project(y, idx, coeff_power=2).cpu().numpy()
     h_ref = O.sparse_back_project(geom, y, idx, coeff_power=2)
     assert rel_l2(h_gpu, h_ref) <= TOL
+
+    # the unit-weight Hessian diagonal, back-projected from no sinogram at all (the library's unit mode)
+    assert rel_l2(model.compute_hessian_diagonal().cpu().numpy(), O.compute_hessian_diagonal(geom)) <= TOL
 
     # adjointness against the float64 oracle
     ref64 = np.sum(O.sparse_forward_project(geom, x, idx, dtype=np.float64) * y)
