@@ -122,8 +122,10 @@ def _channel_matrix(geom, pixel_indices, angle, dt, coeff_power):
     num_det_channels = geom.sinogram_shape[2]
     l_max = np.minimum(dt(1), w)
     num_pixels = n_p.shape[0]
-    rows, cols, vals = [], [], []
-    for n_offset in range(-geom.psf_radius, geom.psf_radius + 1):
+    taps = 2 * geom.psf_radius + 1
+    rows = np.empty((num_pixels, taps), dtype=np.int64)
+    vals = np.empty((num_pixels, taps), dtype=dt)
+    for t, n_offset in enumerate(range(-geom.psf_radius, geom.psf_radius + 1)):
         n = n_c + n_offset
         abs_delta = np.abs(n_p - n.astype(dt))
         l_pcn = np.clip((w + dt(1)) / dt(2) - abs_delta, dt(0), l_max)
@@ -132,12 +134,11 @@ def _channel_matrix(geom, pixel_indices, angle, dt, coeff_power):
         a = a * valid.astype(dt)
         if coeff_power != 1:
             a = a ** coeff_power
-        keep = valid & (a != 0)
-        rows.append(n[keep])
-        cols.append(np.arange(num_pixels)[keep])
-        vals.append(a[keep].astype(dt))
-    rows, cols, vals = np.concatenate(rows), np.concatenate(cols), np.concatenate(vals)
-    return sp.csr_matrix((vals, (rows, cols)), shape=(num_det_channels, num_pixels), dtype=dt)
+        rows[:, t] = np.clip(n, 0, num_det_channels - 1)  # a tap off the detector has coefficient 0
+        vals[:, t] = a
+    # one column per pixel holding its taps (rows ascending), built directly in compressed-column form
+    indptr = np.arange(0, taps * num_pixels + 1, taps, dtype=np.int64)
+    return sp.csc_matrix((vals.ravel(), rows.ravel(), indptr), shape=(num_det_channels, num_pixels), dtype=dt)
 
 
 def _cone_pixel_mag(geom, pixel_indices, angle, dt):

@@ -24,3 +24,19 @@ def test_reference_arm_prints_one_contract_line():
     assert d['cpu_baseline']['value'] == d['value']
     assert d['e2e'] == {'value': d['value'], 'unit': d['unit'], 'h2d_bytes_per_step': 0, 'd2h_bytes_per_step': 0}
     assert 'workload' in d['config']
+
+
+def test_batched_reference_arm_times_a_whole_reconstruction():
+    """The batched workload's reference arm: each timed step is one whole oracle reconstruction of one batch scan
+    (here the smallest, scan 3), scaled across scans only."""
+    cmd = [sys.executable, os.path.join(ROOT, 'bench.py'), '--impl', 'reference', '--workload', 'batched',
+           '--steps', '1', '--warmup', '1', '--cpu-sample-scan', '3']
+    res = subprocess.run(cmd, capture_output=True, text=True, timeout=900, cwd=ROOT)
+    assert res.returncode == 0, res.stderr[-2000:]
+    lines = [ln for ln in res.stdout.splitlines() if ln.startswith('{')]
+    assert len(lines) == 1
+    d = json.loads(lines[0])
+    assert d['impl'] == 'reference' and d['value'] > 0 and d['steps'] == 1
+    sample = d['cpu_baseline']['sample']
+    assert 'whole reconstruction of scan 3' in sample and 'across scans' in sample
+    assert d['config']['num_scans'] == 24
