@@ -13,6 +13,11 @@ path (``ParallelBeamModel.recon`` scan after scan) measured the same way, and th
 ``--workload cone``: plain cone-beam VCD on one scan (256 views x 128 rows x 256 channels, sdd = sid = 1024,
 recon 256x256x128 from 20 ellipsoids, 20 iterations x 4 subsets, FDK init).
 
+``--workload large``: plain cone-beam VCD at the large size (720 views x 512 rows x 1024 channels, about 1.5 GB,
+sdd = sid = 4096, recon 1024x1024x512 (2 GiB) from 40 ellipsoids, 10 iterations x 8 subsets, FDK init), plus one FDK
+direct recon and one autograd gradient of the differentiable loss with 32-view backward chunks; the line adds the
+peak device memory.  Defaults to 1 warm-up and 1 timed step (a step takes tens of seconds).
+
 ``--workload translation``: plain translation-geometry VCD on the setup of the reference's translation experiment
 (experiments/translation/exp_translation.py: a 7 x 7 raster of translations 22 ALU apart = 49 views, 128 x 128
 detector, sdd = sid = 64, recon 21x196x196 from the model's own sizing, sharpness 1, zero init, 15 iterations),
@@ -55,6 +60,8 @@ METRIC = 'batched vs plain recons/s at 1e-4 NRMSE; proj HBM GB/s; autograd/fwd t
 CONE = dict(views=256, rows=128, channels=256, sdd=1024.0, sid=1024.0, ellipsoids=20, seed=1, subsets=4,
             iterations=20)
 BATCH = dict(num_scans=24, ellipsoids=10, subsets=4, iterations=10, cpu_sample_scan=0)
+LARGE = dict(views=720, rows=512, channels=1024, sdd=4096.0, sid=4096.0, ellipsoids=40, seed=2, subsets=8,
+             iterations=10)
 TRANS = dict(nx=7, nz=7, spacing=22.0, rows=128, channels=128, sdd=64.0, sid=64.0, ellipsoids=10, seed=2, subsets=4,
              iterations=15, sharpness=1.0)
 
@@ -62,10 +69,10 @@ TRANS = dict(nx=7, nz=7, spacing=22.0, rows=128, channels=128, sdd=64.0, sid=64.
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
-    ap.add_argument('--steps', type=int, default=5)
-    ap.add_argument('--warmup', type=int, default=3)
+    ap.add_argument('--steps', type=int, default=None, help='timed steps (default 5; 1 for --workload large)')
+    ap.add_argument('--warmup', type=int, default=None, help='warm-up steps (default 3; 1 for --workload large)')
     ap.add_argument('--impl', default='mbirjax_b200', choices=['mbirjax_b200', 'reference'])
-    ap.add_argument('--workload', default='batched', choices=['batched', 'cone', 'translation'])
+    ap.add_argument('--workload', default='batched', choices=['batched', 'cone', 'translation', 'large'])
     ap.add_argument('--no-e2e', action='store_true')
     ap.add_argument('--no-cpu-baseline', action='store_true')
     ap.add_argument('--scans', type=int, default=None,
@@ -77,6 +84,10 @@ def parse_args():
     ap.add_argument('--autotune', type=int, default=1, choices=[0, 1],
                     help='1: tune the projector plans (default); 0: default plans, no tuning launches (for profiling)')
     args = ap.parse_args()
+    if args.steps is None:
+        args.steps = 1 if args.workload == 'large' else 5
+    if args.warmup is None:
+        args.warmup = 1 if args.workload == 'large' else 3
     if args.scans is not None:
         BATCH['num_scans'] = args.scans
     if args.cpu_sample_scan is not None:
@@ -85,6 +96,7 @@ def parse_args():
         BATCH['iterations'] = args.iterations
         CONE['iterations'] = args.iterations
         TRANS['iterations'] = args.iterations
+        LARGE['iterations'] = args.iterations
     return args
 
 
@@ -183,26 +195,31 @@ def max_over_ranks(value, world):
 
 
 # ----------------------------------------------------------------------------------------------- workload
-def cone_angles():
-    return np.linspace(0, 2 * np.pi, CONE['views'], endpoint=False).astype(np.float32)
+def cone_angles(spec=CONE):
+    return np.linspace(0, 2 * np.pi, spec['views'], endpoint=False).astype(np.float32)
 
 
-def build_cone_workload(device):
-    import torch
+def cone_model(spec=CONE):
     import mbirjax_b200 as mb
+    return mb.ConeBeamModel((spec['views'], spec['rows'], spec['channels']), cone_angles(spec),
+                            source_detector_dist=spec['sdd'], source_iso_dist=spec['sid'])
+
+
+def build_cone_workload(device, spec=CONE):
+    """The cone model, its noisy sinogram (forward projection of the seeded ellipsoid phantom + 1% noise) and the
+    phantom."""
     from mbirjax_b200.utilities import gen_ellipsoid_phantom, add_noise
-    model = mb.ConeBeamModel((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(),
-                             source_detector_dist=CONE['sdd'], source_iso_dist=CONE['sid'])
-    model.set_params(sharpness=0.0, snr_db=30.0, granularity=[CONE['subsets']], partition_sequence=[0], verbose=0)
-    phantom = gen_ellipsoid_phantom(model.get_params('recon_shape'), CONE['ellipsoids'], CONE['seed'], device=device)
-    np.random.seed(CONE['seed'])
-    sino = add_noise(model.forward_project(phantom), 0.01, CONE['seed']).contiguous()
+    model = cone_model(spec)
+    model.set_params(sharpness=0.0, snr_db=30.0, granularity=[spec['subsets']], partition_sequence=[0], verbose=0)
+    phantom = gen_ellipsoid_phantom(model.get_params('recon_shape'), spec['ellipsoids'], spec['seed'], device=device)
+    np.random.seed(spec['seed'])
+    sino = add_noise(model.forward_project(phantom), 0.01, spec['seed']).contiguous()
     return model, sino, phantom
 
 
-def recon_once(model, sino):
-    np.random.seed(CONE['seed'])
-    rec, _ = model.recon(sino, max_iterations=CONE['iterations'], stop_threshold_change_pct=0, logfile_path=None,
+def recon_once(model, sino, spec=CONE):
+    np.random.seed(spec['seed'])
+    rec, _ = model.recon(sino, max_iterations=spec['iterations'], stop_threshold_change_pct=0, logfile_path=None,
                          print_logs=False)
     return rec
 
@@ -380,21 +397,18 @@ def timed_steps(step_fn, steps, warmup, world, flush):
     return start.elapsed_time(end)
 
 
-def autograd_cost():
+def autograd_cost(model, sino, phantom, reps=10, label='cone 256x128x256, recon 256x256x128'):
     """One gradient of 0.5 ||W^(1/2) (A x - y)||^2 + qGGMRF(x) through torch.autograd (forward projection, loss,
     backward through the matched back projector in 32-view chunks and the qGGMRF gradient kernel) against one
-    forward projection of the same recon, on the cone geometry of the cone workload (256 views x 128 rows x 256
-    channels, recon 256x256x128, W = exp(-y / max y)).  CUDA events, 10 repetitions each after 3 warm-ups."""
+    forward projection of the same recon.  Data as in the differentiable configuration: y the workload's noisy
+    sinogram of its phantom, W = exp(-y / max y), x = half the phantom (an iterate away from the solution).  CUDA
+    events, reps repetitions each after warm-ups."""
     import torch
     import mbirjax_b200 as mb
     from mbirjax_b200 import autograd as AG
-    model = mb.ConeBeamModel((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(), CONE['sdd'],
-                             CONE['sid'])
-    shape = tuple(model.get_params('recon_shape'))
-    gen = torch.Generator(device='cuda').manual_seed(2)
-    x = (torch.rand(shape, device='cuda', generator=gen) * 0.1).requires_grad_(True)
-    y = torch.rand((CONE['views'], CONE['rows'], CONE['channels']), device='cuda', generator=gen)
+    y = sino
     w = torch.exp(-y / y.max())
+    x = (0.5 * phantom).detach().clone().requires_grad_(True)
     params = (mb.get_b_from_nbr_wts([1, 1, 1]), 0.3, 2.0, 1.2, 1.0)
 
     def fwd():
@@ -407,22 +421,22 @@ def autograd_cost():
 
     res = {}
     for name, fn in (('fp_ms', fwd), ('grad_ms', grad)):
-        for _ in range(3):
+        for _ in range(2 if reps < 10 else 3):
             fn()
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
         s.record()
-        for _ in range(10):
+        for _ in range(reps):
             fn()
         e.record()
         torch.cuda.synchronize()
-        res[name] = round(s.elapsed_time(e) / 10, 4)
+        res[name] = round(s.elapsed_time(e) / reps, 4)
     res['grad_over_fp'] = round(res['grad_ms'] / res['fp_ms'], 3)
-    res['config'] = 'cone 256x128x256, recon 256x256x128, backward in 32-view chunks'
+    res['config'] = label + ', W = exp(-y / max y), x = phantom / 2, backward in 32-view chunks'
     return res
 
 
-def kernel_roofline(model, sino, peak_gbs, peak_kind, prefix='cone', spec=CONE):
+def kernel_roofline(model, sino, peak_gbs, peak_kind, prefix='cone', spec=CONE, reps=20):
     """Average duration of one VCD subset's back and forward projection (CUDA events, 20 launches each)."""
     import torch
     from mbirjax_b200 import _capi
@@ -447,7 +461,6 @@ def kernel_roofline(model, sino, peak_gbs, peak_kind, prefix='cone', spec=CONE):
             fn()
         torch.cuda.synchronize()
         s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-        reps = 20
         s.record()
         for _ in range(reps):
             fn()
@@ -489,6 +502,11 @@ def cpu_reference_sample(workers=None, workload='cone'):
         tv = translation_vectors()
         geom = O.translation_geometry((tv.shape[0], TRANS['rows'], TRANS['channels']), tv, TRANS['sdd'], TRANS['sid'])
         spec = TRANS
+    elif workload == 'large':  # evenly spaced views of the large scan: the per-view work is the same
+        ang = cone_angles(LARGE)[:: LARGE['views'] // LARGE_CPU_VIEWS][:LARGE_CPU_VIEWS]
+        geom = O.cone_geometry((len(ang), LARGE['rows'], LARGE['channels']), ang, LARGE['sdd'], LARGE['sid'],
+                               recon_shape=(1024, 1024, 512))
+        spec = LARGE
     else:
         geom = O.cone_geometry((CONE['views'], CONE['rows'], CONE['channels']), cone_angles(), CONE['sdd'],
                                CONE['sid'])
@@ -512,9 +530,14 @@ def cpu_reference_sample(workers=None, workload='cone'):
     return dt, pool.workers
 
 
-def cpu_recons_per_s(subset_seconds):
-    # one recon = subsets x iterations subset updates (the FDK initialisation and Hessian are not counted)
-    return 1.0 / (subset_seconds * CONE['subsets'] * CONE['iterations'])
+def cpu_sample_scale(workload):
+    """Subset updates of a whole reconstruction per sampled one (the initialisation and Hessian are not counted),
+    times the views left out of the large scan's sample."""
+    spec = single_scan_spec(workload)[0]
+    scale = spec['subsets'] * spec['iterations']
+    if workload == 'large':
+        scale *= LARGE['views'] / LARGE_CPU_VIEWS
+    return scale
 
 
 # ----------------------------------------------------------------------------------------------- arms
@@ -541,7 +564,21 @@ def single_scan_spec(workload):
     """(spec, config function, cpu sample label) of a single-scan workload."""
     if workload == 'translation':
         return TRANS, translation_config, 'the translation scan'
+    if workload == 'large':
+        return LARGE, large_config, 'the large cone scan on %d of its %d views' % (LARGE_CPU_VIEWS, LARGE['views'])
     return CONE, cone_config, 'the cone scan'
+
+
+LARGE_CPU_VIEWS = 16  # views of the large cone scan in its CPU sample (evenly spaced; scaled by views)
+
+
+def large_config(world):
+    return {'workload': 'plain cone-beam VCD, sinogram 720x512x1024, recon 1024x1024x512 of 40 ellipsoids, '
+                        '%d iterations x %d subsets, FDK init, sdd=sid=4096; plus one FDK and one autograd gradient'
+                        % (LARGE['iterations'], LARGE['subsets']),
+            'views': LARGE['views'], 'det_rows': LARGE['rows'], 'det_channels': LARGE['channels'],
+            'recon_shape': [1024, 1024, 512], 'iterations': LARGE['iterations'], 'subsets': LARGE['subsets'],
+            'parallelism': 'replicas x%d' % world, 'l2': 'inputs (1.5 GB sinogram, 2 GiB recon) exceed L2'}
 
 
 def cone_config(world):
@@ -577,7 +614,7 @@ def run_reference(args):
         for i in range(args.warmup + args.steps):
             spec = single_scan_spec(args.workload)[0]
             dt, cores = cpu_reference_sample(workload=args.workload)
-            scale = spec['subsets'] * spec['iterations']
+            scale = cpu_sample_scale(args.workload)
             if i >= args.warmup:
                 samples.append(dt)
         mean = float(np.mean(samples))
@@ -620,6 +657,16 @@ def run_gpu(args):
         units = 1
         config = translation_config(world)
         recon_fn = translation_recon_once
+
+        def step():
+            recon_fn(model, sino)
+    elif args.workload == 'large':
+        model, sino, phantom = build_cone_workload(device, LARGE)
+        units = 1
+        config = large_config(world)
+
+        def recon_fn(m, y):
+            return recon_once(m, y, LARGE)
 
         def step():
             recon_fn(model, sino)
@@ -691,10 +738,29 @@ def run_gpu(args):
         line['roofline'] = batched_roofline(models, sinos, peak_gbs, peak_kind)
     else:
         line['roofline'] = kernel_roofline(model, sino, peak_gbs, peak_kind, args.workload,
-                                           single_scan_spec(args.workload)[0])
+                                           single_scan_spec(args.workload)[0],
+                                           reps=5 if args.workload == 'large' else 20)
 
-    if args.workload != 'translation':
-        line['autograd'] = autograd_cost()
+    if args.workload == 'large':
+        # one FDK direct recon at this size, the peak device memory of the whole run, and the gradient below
+        for _ in range(1):
+            model.direct_recon(sino)
+        torch.cuda.synchronize()
+        s_, e_ = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s_.record()
+        model.direct_recon(sino)
+        e_.record()
+        torch.cuda.synchronize()
+        line['fdk_ms'] = round(s_.elapsed_time(e_), 3)
+        line['autograd'] = autograd_cost(model, sino, phantom, reps=2,
+                                         label='cone 720x512x1024, recon 1024x1024x512')
+        line['peak_memory_gb'] = round(torch.cuda.max_memory_allocated(device) / 1e9, 3)
+    elif args.workload == 'cone':
+        line['autograd'] = autograd_cost(model, sino, phantom)
+    elif args.workload == 'batched':
+        c_model, c_sino, c_phantom = build_cone_workload(device)
+        line['autograd'] = autograd_cost(c_model, c_sino, c_phantom)
+        del c_model, c_sino, c_phantom
 
     if rank == 0 and world == 1 and not args.no_cpu_baseline:
         if args.workload == 'batched':
@@ -708,7 +774,7 @@ def run_gpu(args):
         else:
             spec = single_scan_spec(args.workload)[0]
             dt, cores = cpu_reference_sample(workload=args.workload)
-            scale = spec['subsets'] * spec['iterations']
+            scale = cpu_sample_scale(args.workload)
             line['cpu_baseline'] = {'value': round(units / (dt * scale), 6), 'unit': 'recons/s', 'cores': cores,
                                     'kind': 'port',
                                     'sample': 'one VCD subset update of %s (oracle NumPy port, %d processes), %.2f s, '

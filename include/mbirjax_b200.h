@@ -251,11 +251,15 @@ typedef struct mbx_scan {
     int32_t subset_size;
     float fm_constant;              /* 1 / sigma_y^2 */
     mbx_qggmrf_params qp;
+    /* Inputs of the batched set-up (mbx_vcd_batched_setup); NULL / 0 when the caller sets the state up itself. */
+    const float *sinogram;          /* (V, R, C) measured sinogram y */
+    const int32_t *full_indices;    /* the region-of-reconstruction pixels, gen_full_indices (vcd_utils.py:310-318) */
+    int32_t num_full_indices;
 } mbx_scan;
 
 /* Opaque host-side record of a prepared batch (filled by mbx_vcd_batched_prepare). */
 typedef struct mbx_batched_plan {
-    uint64_t opaque[64];
+    uint64_t opaque[128];
 } mbx_batched_plan;
 
 /* Workspace for a batch with num_steps subset steps in its schedule (0 if the batch is not supported). */
@@ -289,6 +293,30 @@ MBX_API int mbx_vcd_batched_stage(const mbx_batched_plan *plan, int32_t step, in
 /* Per-scan iteration statistics into iter_stats[iteration] (inputs of the reference's fm_rmse and NMAE,
  * tomography_model.py:1219-1220). */
 MBX_API int mbx_vcd_batched_iteration_stats(const mbx_batched_plan *plan, int32_t iteration, void *stream);
+
+/* The VCD set-up of every scan of the batch, as batched stages (no host synchronisation; capturable): direct
+ * recon initialisation (FBP / FDK filter of the scan's sinogram into its error sinogram, back projection over its
+ * full_indices into its flat recon, zero elsewhere), forward projection of that recon, the alpha rescale that
+ * minimises ||y - alpha A x||_W (float64 sums), error sinogram y - alpha A x and recon alpha x, and the Hessian
+ * diagonal (back projection of the weights, or of ones, with squared coefficients over every pixel).  Replaces
+ * the set-up of vcd_recon (tomography_model.py:1110-1152) with direct_recon (:934-964) and
+ * compute_hessian_diagonal (:679-708), run once per scan in the reference.  Needs every scan's sinogram and
+ * full_indices at prepare time (else MBX_ERR_UNSUPPORTED). */
+MBX_API int mbx_vcd_batched_setup(const mbx_batched_plan *plan, void *stream);
+
+/* New per-call parameters of a prepared batch: each scan's fm_constant and qp, and the subset schedule
+ * (num_steps * num_scans entries, as at prepare).  scans must describe the same batch as at prepare (same count,
+ * sizes and buffers); only fm_constant and qp are read from it.  Enqueues host-to-device copies on the stream
+ * (from pageable host memory: not capturable; call it between graph replays).  With mbx_vcd_batched_refresh this
+ * lets one prepared plan, and graphs captured from it, reconstruct new data of the same batch shape: the
+ * reference recomputes regularisation, partitions and subset orders on every recon call
+ * (tomography_model.py:1024-1035, 1281). */
+MBX_API int mbx_vcd_batched_update(const mbx_batched_plan *plan, const mbx_scan *scans, int32_t num_scans,
+                                   const int32_t *schedule, void *stream);
+
+/* Recomputes the chunk bounding boxes of every scan's subsets from the partition buffers, after the caller has
+ * written new partitions into them (one launch; capturable). */
+MBX_API int mbx_vcd_batched_refresh(const mbx_batched_plan *plan, void *stream);
 
 /* ---- FBP / FDK filtering ---------------------------------------------------------------------- */
 

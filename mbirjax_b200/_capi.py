@@ -44,12 +44,13 @@ class MbxScan(ctypes.Structure):
     _fields_ = [('geom', MbxGeom), ('flat_recon', c_void_p), ('error_sinogram', c_void_p), ('weights', c_void_p),
                 ('fm_hessian', c_void_p), ('partition', c_void_p), ('partition_order', c_void_p),
                 ('num_subsets', c_int32), ('subset_size', c_int32), ('fm_constant', c_float),
-                ('qp', MbxQggmrfParams)]
+                ('qp', MbxQggmrfParams), ('sinogram', c_void_p), ('full_indices', c_void_p),
+                ('num_full_indices', c_int32)]
 
 
 class MbxBatchedPlan(ctypes.Structure):
     """Mirror of ``mbx_batched_plan`` (opaque)."""
-    _fields_ = [('opaque', ctypes.c_uint64 * 64)]
+    _fields_ = [('opaque', ctypes.c_uint64 * 128)]
 
 
 # name -> (restype, argtypes); must match include/mbirjax_b200.h
@@ -94,6 +95,10 @@ _SIGNATURES = {
     'mbx_vcd_batched_step': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_void_p]),
     'mbx_vcd_batched_iteration_stats': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_void_p]),
     'mbx_vcd_batched_stage': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_int32, c_int32, c_void_p]),
+    'mbx_vcd_batched_setup': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_void_p]),
+    'mbx_vcd_batched_update': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), ctypes.POINTER(MbxScan), c_int32,
+                                              c_void_p, c_void_p]),
+    'mbx_vcd_batched_refresh': (ctypes.c_int, [ctypes.POINTER(MbxBatchedPlan), c_void_p]),
     'mbx_direct_filter': (ctypes.c_int, [ctypes.POINTER(MbxGeom), c_void_p, c_void_p, c_void_p]),
 }
 
@@ -362,6 +367,25 @@ def vcd_batched_step(plan, step):
 def vcd_batched_iteration_stats(plan, iteration):
     _check(load_library().mbx_vcd_batched_iteration_stats(ctypes.byref(plan), int(iteration), _stream()),
            'mbx_vcd_batched_iteration_stats')
+
+
+def vcd_batched_setup(plan):
+    _check(load_library().mbx_vcd_batched_setup(ctypes.byref(plan), _stream()), 'mbx_vcd_batched_setup')
+
+
+def vcd_batched_update(plan, scans, schedule):
+    """New fm constants / qGGMRF parameters (read from the MbxScan records) and subset schedule of a prepared
+    batch, copied to its device tables on the current stream."""
+    import numpy as np
+    n = len(scans)
+    arr = (MbxScan * n)(*scans)
+    sched = np.ascontiguousarray(schedule, dtype=np.int32)
+    _check(load_library().mbx_vcd_batched_update(ctypes.byref(plan), arr, n, sched.ctypes.data_as(c_void_p),
+                                                  _stream()), 'mbx_vcd_batched_update')
+
+
+def vcd_batched_refresh(plan):
+    _check(load_library().mbx_vcd_batched_refresh(ctypes.byref(plan), _stream()), 'mbx_vcd_batched_refresh')
 
 
 BATCHED_STAGES = ('bp', 'delta', 'fp', 'linquad', 'alpha', 'apply', 'error', 'l1')

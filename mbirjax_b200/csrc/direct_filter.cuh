@@ -1,0 +1,100 @@
+// Ramp filtering of detector rows for FBP / FDK (sm_100a): the device function shared by the plain entry point
+// (direct_filter.cu) and the batched VCD set-up (vcd_batched.cu).  See direct_filter.cu for the arithmetic.
+#pragma once
+
+#include <cmath>
+
+#include "mbx_common.cuh"
+
+namespace mbx {
+
+constexpr int FILT_ROWS = 8;
+constexpr int FILT_THREADS = 256;
+
+// Scales of the ramp filter for a geometry: the filter times 1/delta_voxel^2 (FBP, parallel_beam.py:325-327) or
+// delta_det_row / (delta_voxel^3 magnification) after the FDK pre-weight (cone_beam.py:825-827), and pi / views.
+inline void direct_filter_scales(const mbx_geom &g, float &filter_scale, float &out_scale, int &fdk) {
+    const double pi = 3.14159265358979323846;
+    out_scale = (float)(pi / g.num_views);
+    if (g.kind == MBX_GEOM_PARALLEL) {
+        filter_scale = (float)(1.0 / ((double)g.delta_voxel * g.delta_voxel));
+        fdk = 0;
+    } else {
+        filter_scale = (float)((double)g.delta_det_row /
+                               ((double)g.delta_voxel * g.delta_voxel * g.delta_voxel * g.magnification));
+        fdk = 1;
+    }
+}
+
+// Shared memory of one filter tile for rows of C channels.
+inline size_t filter_smem_bytes(int C) { return ((size_t)C * FILT_ROWS + 2 * (size_t)C - 1) * sizeof(float); }
+
+// Filters rows row0 .. row0 + FILT_ROWS - 1 (fewer at the end) of a (num_rows_total, C) stack of detector rows
+// (R rows per view) with the whole block; sm holds filter_smem_bytes(C).
+__device__ __forceinline__ void direct_filter_rows(const float *__restrict__ sino, float *__restrict__ out,
+                                                   long long row0, long long num_rows_total, int R, int C,
+                                                   float filter_scale, float out_scale, int fdk, float D,
+                                                   float delta_det_channel, float delta_det_row,
+                                                   float det_channel_offset, float det_row_offset, float *sm) {
+    float *rows_t = sm;                         // [C][FILT_ROWS]
+    float *filt = sm + (size_t)C * FILT_ROWS;   // [2C-1]
+    const int nrows = (int)min((long long)FILT_ROWS, num_rows_total - row0);
+
+    const double kInvPi2 = 0.10132118364233778;  // 1 / pi^2
+    for (int t = threadIdx.x; t < 2 * C - 1; t += blockDim.x) {
+        const int d = t - (C - 1);
+        float h;
+        if (d == 0)
+            h = 0.25f;
+        else if (d & 1)
+            h = (float)(-kInvPi2 / ((double)d * (double)d));
+        else
+            h = 0.0f;
+        filt[t] = filter_scale * h;
+    }
+    const float det_center_row = 0.5f * (float)(R - 1);
+    const float det_center_channel = 0.5f * (float)(C - 1);
+    for (int t = threadIdx.x; t < C * FILT_ROWS; t += blockDim.x) {
+        const int rr = t / C;
+        const int j = t - rr * C;
+        float v = 0.0f;
+        if (rr < nrows) {
+            const long long grow = row0 + rr;
+            v = sino[grow * C + j];
+            if (fdk && isfinite(D)) {
+                const int m = (int)(grow % R);
+                const float vv = ((float)m - det_center_row) * delta_det_row - det_row_offset;
+                const float uu = ((float)j - det_center_channel) * delta_det_channel - det_channel_offset;
+                v *= D / sqrtf(D * D + uu * uu + vv * vv);
+            }
+        }
+        rows_t[j * FILT_ROWS + rr] = v;
+    }
+    __syncthreads();
+    for (int i = threadIdx.x; i < C; i += blockDim.x) {
+        float acc[FILT_ROWS];
+        {
+            const float h0 = filt[C - 1];
+            const float4 a = *reinterpret_cast<const float4 *>(rows_t + i * FILT_ROWS);
+            const float4 b = *reinterpret_cast<const float4 *>(rows_t + i * FILT_ROWS + 4);
+            acc[0] = h0 * a.x; acc[1] = h0 * a.y; acc[2] = h0 * a.z; acc[3] = h0 * a.w;
+            acc[4] = h0 * b.x; acc[5] = h0 * b.y; acc[6] = h0 * b.z; acc[7] = h0 * b.w;
+        }
+        // odd differences i - j only
+        for (int j = (i + 1) & 1; j < C; j += 2) {
+            const float h = filt[i - j + C - 1];
+            const float4 a = *reinterpret_cast<const float4 *>(rows_t + j * FILT_ROWS);
+            const float4 b = *reinterpret_cast<const float4 *>(rows_t + j * FILT_ROWS + 4);
+            acc[0] = fmaf(h, a.x, acc[0]); acc[1] = fmaf(h, a.y, acc[1]);
+            acc[2] = fmaf(h, a.z, acc[2]); acc[3] = fmaf(h, a.w, acc[3]);
+            acc[4] = fmaf(h, b.x, acc[4]); acc[5] = fmaf(h, b.y, acc[5]);
+            acc[6] = fmaf(h, b.z, acc[6]); acc[7] = fmaf(h, b.w, acc[7]);
+        }
+#pragma unroll
+        for (int rr = 0; rr < FILT_ROWS; ++rr)
+            if (rr < nrows) out[(row0 + rr) * C + i] = out_scale * acc[rr];
+    }
+    __syncthreads();  // the block may stage its next tile into sm
+}
+
+}  // namespace mbx

@@ -255,12 +255,13 @@ inline size_t fp_chunk_box_bytes(long long num_pixels) {
     return align256((size_t)((num_pixels + CB_CHUNK - 1) / CB_CHUNK) * sizeof(int4));
 }
 
-// Bounding box of the grid pixels of each CB_CHUNK list entries (one CTA of CB_CHUNK threads per chunk).
-static __global__ void __launch_bounds__(CB_CHUNK) fp_chunk_bounds_kernel(const int32_t *__restrict__ pix,
-                                                                    long long num_pixels, int num_rows, int num_cols,
-                                                                    int4 *__restrict__ box) {
+// Bounding box of the grid pixels of list entries chunk * CB_CHUNK .. + CB_CHUNK - 1, by a block of CB_CHUNK
+// threads, into box[chunk].
+__device__ __forceinline__ void fp_chunk_bounds_block(const int32_t *__restrict__ pix, long long num_pixels,
+                                                      int num_rows, int num_cols, int4 *__restrict__ box,
+                                                      long long chunk) {
     __shared__ int red[4][CB_CHUNK / 32];
-    const long long p = (long long)blockIdx.x * CB_CHUNK + threadIdx.x;
+    const long long p = chunk * CB_CHUNK + threadIdx.x;
     int rmin = INT_MAX, rmax = INT_MIN, cmin = INT_MAX, cmax = INT_MIN, bad = 0;
     if (p < num_pixels) {
         const int idx = pix[p];
@@ -296,8 +297,16 @@ static __global__ void __launch_bounds__(CB_CHUNK) fp_chunk_bounds_kernel(const 
             cmax = max(cmax, red[3][w]);
         }
         if (rmin < 0) rmin = -1;  // an off-grid index: the projector must see every entry to flag it
-        box[blockIdx.x] = make_int4(rmin, rmax, cmin, cmax);
+        box[chunk] = make_int4(rmin, rmax, cmin, cmax);
     }
+    __syncthreads();  // red may be reused by the block's next chunk
+}
+
+// Bounding box of the grid pixels of each CB_CHUNK list entries (one CTA of CB_CHUNK threads per chunk).
+static __global__ void __launch_bounds__(CB_CHUNK) fp_chunk_bounds_kernel(const int32_t *__restrict__ pix,
+                                                                    long long num_pixels, int num_rows, int num_cols,
+                                                                    int4 *__restrict__ box) {
+    fp_chunk_bounds_block(pix, num_pixels, num_rows, num_cols, box, blockIdx.x);
 }
 
 // True when no pixel of the box can have a centre channel in [n0 - 1, n0 + nb] (one rounding step of slack

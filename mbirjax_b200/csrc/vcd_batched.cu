@@ -17,12 +17,19 @@
 // The subset each scan updates at each step comes from a schedule table in device memory, and every per-(scan,
 // subset) argument record is built once in mbx_vcd_batched_prepare, so the launches of a step depend only on
 // the step number: the whole multi-iteration reconstruction can be captured once in a CUDA graph and replayed.
+// The set-up of every scan (direct-recon initialisation, alpha rescale, Hessian diagonal) runs as batched stages
+// too (mbx_vcd_batched_setup), over three more projection work lists (initial back and forward projection over
+// each scan's region of reconstruction, Hessian back projection over every pixel).  The per-call parameters
+// (regularisation, schedule, partitions) live in device tables that mbx_vcd_batched_update and
+// mbx_vcd_batched_refresh rewrite, so a prepared plan, and graphs captured from it, serve every call of a batch
+// shape.
 #include <algorithm>
 #include <cstring>
 #include <vector>
 
 #include "back_project.cuh"
 #include "bp_fast.cuh"
+#include "direct_filter.cuh"
 #include "fp_cb.cuh"
 #include "mbx_common.cuh"
 #include "mbx_host.hpp"
@@ -40,42 +47,90 @@ struct VcdScan {
     float *recon;               // flat (Nr*Nc, S)
     float *err;                 // (V, R, C)
     const float *wts;           // (V, R, C) or NULL
-    const float *hess;          // flat (Nr*Nc, S)
+    float *hess;                // flat (Nr*Nc, S)
     const int32_t *partition;   // (K, M)
     float *bp, *delta, *dsino;  // workspace slices
+    const float *y;             // measured sinogram (set-up input) or NULL
     long long nsino, nrecon;
     int K, M, nr, nc, ns;
-    float fm_constant;
-    QParams q;
 };
+
+// Direct-recon filtering of one scan in the set-up: rows of y into err.
+struct FiltScan {
+    const float *in;
+    float *out;
+    long long rows;
+    int R, C, fdk;
+    float filter_scale, out_scale, D, ddc, ddr, dco, dro;
+};
+
+// A work list of projection tiles over the scans of a batch: per scan, its argument record(s) and tile count.
+// Tiles are numbered over the scans in `order` (decreasing per-tile cost) and handed out dynamically.
+struct ProjList {
+    const BpArgs *bp;      // back-projection records (or NULL)
+    const FpArgs *fp;      // forward-projection records (or NULL)
+    const int *off;        // [num_scans + 1] tile prefix over the positions of `order`
+    const int *dim;        // [num_scans] per scan: gx (back projection) or channel blocks (forward)
+    const int *order;      // [num_scans] scan at each position
+    const int *schedule;   // [num_steps][num_scans] record of each scan at each step, or NULL (record 0)
+    int stride;            // records per scan
+    int *counter;          // next tile (reset by a memset before each launch)
+};
+
+// Projection work lists of a batch.
+enum { PL_BP = 0, PL_FP, PL_INIT_BP, PL_INIT_FP, PL_HESS, PL_COUNT };
 
 struct BatchedTables {
     VcdScan *scans;
+    float *fm;          // [scan] 1 / sigma_y^2 (per call)
+    QParams *qp;        // [scan] qGGMRF parameters (per call)
     BpArgs *bpargs;     // [scan][subset]
     FpArgs *fpargs;     // [scan][subset]
-    int *bp_off, *fp_off, *el_off, *sn_off, *rc_off;  // [num_scans + 1] tile prefix offsets
-    int *fp_cblocks;    // [num_scans]
-    int *bp_gx;         // [num_scans]
-    int *bp_scan, *fp_scan;  // [num_scans]: scan at each position of the (cost-sorted) bp / fp work lists
-    int *counters;      // [2]: next bp / fp tile to hand out (reset before each launch)
+    BpArgs *init_bp;    // [scan]: filtered sinogram -> recon over the region of reconstruction
+    FpArgs *init_fp;    // [scan]: recon -> dsino over the region of reconstruction
+    BpArgs *hess_bp;    // [scan]: weights (or ones) -> Hessian over every pixel, squared coefficients
+    FiltScan *filt;     // [scan]
+    int *pl_off;        // [PL_COUNT][num_scans + 1]
+    int *pl_dim;        // [PL_COUNT][num_scans]
+    int *pl_order;      // [PL_COUNT][num_scans]
+    int *el_off, *sn_off, *rc_off, *flt_off;  // [num_scans + 1] tile prefix offsets (scan order)
+    int *box_first;     // [num_scans * K + 1] chunk prefix over (scan, subset) records
+    int *counters;      // [PL_COUNT]
     int *schedule;      // [num_steps][num_scans]
-    double *p_prior, *p_fwd, *p_l1, *p_iter;
+    double *p_prior, *p_fwd, *p_l1, *p_iter, *p_init;
     float *alpha;       // [num_scans]
+    float *alpha_init;  // [num_scans]
     double *step_stats; // [num_steps][num_scans][4]
     double *iter_stats; // [num_iterations][num_scans][4]
 };
 
 struct BatchedPlanHost {
     BatchedTables t;
-    int num_scans, kind, num_steps, num_iterations;
-    int bp_total, fp_total, el_total, sn_total, rc_total;
-    int bp_grid, fp_grid, el_grid, sn_grid, rc_grid;
-    size_t bp_smem, fp_smem;
-    int fp_minb;  // b_fp variant: 2 or 3 resident CTAs per SM
+    int num_scans, kind, num_steps, num_iterations, ksum, has_setup;
+    int pl_total[PL_COUNT], pl_grid[PL_COUNT];
+    size_t pl_smem[PL_COUNT];
+    int el_total, sn_total, rc_total, flt_total, box_total;
+    int el_grid, sn_grid, rc_grid, flt_grid, box_grid;
+    size_t flt_smem;
+    int fp_minb;  // b_fp variant of the subset stage: 2 or 3 resident CTAs per SM
     int magic;
 };
 static_assert(sizeof(BatchedPlanHost) <= sizeof(mbx_batched_plan), "plan record too large");
-constexpr int BT_MAGIC = 0x6d627862;
+constexpr int BT_MAGIC = 0x6d627863;
+
+static ProjList proj_list(const BatchedTables &T, int which, int num_scans) {
+    ProjList L;
+    L.bp = which == PL_BP ? T.bpargs : which == PL_INIT_BP ? T.init_bp : which == PL_HESS ? T.hess_bp : nullptr;
+    L.fp = which == PL_FP ? T.fpargs : which == PL_INIT_FP ? T.init_fp : nullptr;
+    L.off = T.pl_off + which * (num_scans + 1);
+    L.dim = T.pl_dim + which * num_scans;
+    L.order = T.pl_order + which * num_scans;
+    const bool subsets = which == PL_BP || which == PL_FP;
+    L.schedule = subsets ? T.schedule : nullptr;
+    L.stride = 0;  // set by the caller (the number of subsets for the subset lists)
+    L.counter = T.counters + which;
+    return L;
+}
 
 __device__ __forceinline__ int find_scan(const int *__restrict__ off, int num_scans, int t) {
     int lo = 0, hi = num_scans;  // off[lo] <= t < off[hi]
@@ -117,35 +172,39 @@ __device__ __forceinline__ int fetch_tile(int *counter) {
     return s_next;
 }
 
-template <int KIND>
 #ifndef MBX_BBP_MIN_BLOCKS
 #define MBX_BBP_MIN_BLOCKS 3  // resident CTAs per SM the batched back projection is compiled for
 #endif
-__global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(BatchedTables T, int num_scans, int step, int first, int total, int *err) {
+
+// Record of scan s in a work list at a step.
+template <class A>
+__device__ __forceinline__ const A &list_record(const A *recs, const ProjList &L, int num_scans, int step, int s) {
+    const int r = L.schedule ? __ldg(L.schedule + step * num_scans + s) : 0;
+    return recs[s * L.stride + r];
+}
+
+template <int KIND>
+__global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(ProjList L, int num_scans, int step, int first, int total, int *err) {
     extern __shared__ __align__(16) float smb[];
-    for (int t = first + fetch_tile(T.counters); t < total; t = first + fetch_tile(T.counters)) {
-        const int k = find_scan(T.bp_off, num_scans, t);
-        const int s = __ldg(T.bp_scan + k);
-        const int local = t - __ldg(T.bp_off + k);
-        const int sub = __ldg(T.schedule + step * num_scans + s);
-        const int K = T.scans[s].K;
-        const int gx = __ldg(T.bp_gx + s);
-        bp_fast_tile<KIND>(T.bpargs[s * K + sub], local % gx, local / gx, 0, smb, err);
+    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
+        const int k = find_scan(L.off, num_scans, t);
+        const int s = __ldg(L.order + k);
+        const int local = t - __ldg(L.off + k);
+        const int gx = __ldg(L.dim + s);
+        bp_fast_tile<KIND>(list_record(L.bp, L, num_scans, step, s), local % gx, local / gx, 0, smb, err);
     }
 }
 
 // MINB: resident CTAs per SM the variant is compiled for (2 or 3, matching the plans' fp_cb minb).
 template <int KIND, int MINB>
-__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(BatchedTables T, int num_scans, int step, int first, int total, int *err) {
+__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(ProjList L, int num_scans, int step, int first, int total, int *err) {
     extern __shared__ __align__(16) float smf2[];
-    for (int t = first + fetch_tile(T.counters + 1); t < total; t = first + fetch_tile(T.counters + 1)) {
-        const int k = find_scan(T.fp_off, num_scans, t);
-        const int s = __ldg(T.fp_scan + k);
-        const int local = t - __ldg(T.fp_off + k);
-        const int sub = __ldg(T.schedule + step * num_scans + s);
-        const int K = T.scans[s].K;
-        const int cbs = __ldg(T.fp_cblocks + s);
-        fp_cb_tile<KIND, MINB>(T.fpargs[s * K + sub], local / cbs, local % cbs, smf2, err);
+    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
+        const int k = find_scan(L.off, num_scans, t);
+        const int s = __ldg(L.order + k);
+        const int local = t - __ldg(L.off + k);
+        const int cbs = __ldg(L.dim + s);
+        fp_cb_tile<KIND, MINB>(list_record(L.fp, L, num_scans, step, s), local / cbs, local % cbs, smf2, err);
     }
 }
 
@@ -160,6 +219,8 @@ __global__ void __launch_bounds__(BT_THREADS) b_delta(BatchedTables T, int num_s
         const long long e0 = (long long)local * BT_ELEM_TILE;
         const long long e1 = min(n, e0 + BT_ELEM_TILE);
         const int npix = sc.nr * sc.nc;
+        const QParams q = T.qp[s];
+        const float fm = T.fm[s];
         double pl = 0.0, pq = 0.0;
         for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
             const long long p = i / sc.ns;
@@ -170,9 +231,9 @@ __global__ void __launch_bounds__(BT_THREADS) b_delta(BatchedTables T, int num_s
                 flag_error(err, MBX_ERRFLAG_PIXEL);
             } else {
                 float gp, hp;
-                qggmrf_voxel(sc.recon, sc.nr, sc.nc, sc.ns, idx, k, sc.q, gp, hp);
-                const float gf = -sc.fm_constant * sc.bp[i];
-                const float hf = sc.fm_constant * __ldg(sc.hess + (long long)idx * sc.ns + k);
+                qggmrf_voxel(sc.recon, sc.nr, sc.nc, sc.ns, idx, k, q, gp, hp);
+                const float gf = -fm * sc.bp[i];
+                const float hf = fm * __ldg(sc.hess + (long long)idx * sc.ns + k);
                 d = -((gf + gp) / (hf + hp));
                 pl += (double)(gp * d);
                 pq += (double)(hp * (d * d));
@@ -214,12 +275,11 @@ __device__ __forceinline__ double warp_range_sum(const double *__restrict__ p, i
 __global__ void b_alpha(BatchedTables T, int num_scans, int step) {
     const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
     if (s >= num_scans) return;
-    const VcdScan &sc = T.scans[s];
     const int eb = __ldg(T.el_off + s), ee = __ldg(T.el_off + s + 1);
     const int sb = __ldg(T.sn_off + s), se = __ldg(T.sn_off + s + 1);
     const double pl = warp_range_sum(T.p_prior, eb, ee, 2, 0);
     const double pq = 0.5 * warp_range_sum(T.p_prior, eb, ee, 2, 1);
-    const double fm = (double)sc.fm_constant;
+    const double fm = (double)T.fm[s];
     const double fl = fm * warp_range_sum(T.p_fwd, sb, se, 2, 0);
     const double fq = fm * warp_range_sum(T.p_fwd, sb, se, 2, 1);
     if ((threadIdx.x & 31) == 0) {
@@ -323,12 +383,106 @@ __global__ void b_iter_final(BatchedTables T, int num_scans, int iteration, int 
     }
 }
 
+// ------------------------------------------------------------------------------------------------ set-up stages
+// The reference's vcd_recon set-up (tomography_model.py:1110-1152) for every scan: x0 = direct recon, then
+// alpha = <W A x0, y> / <W A x0, A x0> (1 when the denominator is 0), e = y - alpha A x0, x = alpha x0, and the
+// Hessian diagonal.  The float32 products match TomographyModel._vcd_setup (W A x0 rounded to float32, sums in
+// float64, alpha rounded to float32, then y - (alpha A x0) and alpha x0 each rounded once, without contraction).
+
+// Zero every scan's flat recon (the direct recon is zero outside the region of reconstruction).
+__global__ void __launch_bounds__(BT_THREADS) b_zero_recon(BatchedTables T, int num_scans, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.rc_off, num_scans, t);
+        const int local = t - __ldg(T.rc_off + s);
+        const VcdScan &sc = T.scans[s];
+        const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nrecon, e0 + BT_SINO_TILE);
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) sc.recon[i] = 0.0f;
+    }
+}
+
+// FBP / FDK filtering of every scan's sinogram, FILT_ROWS detector rows per tile (direct_filter_rows).
+__global__ void __launch_bounds__(FILT_THREADS) b_filter(BatchedTables T, int num_scans, int total) {
+    extern __shared__ __align__(16) float smflt[];
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.flt_off, num_scans, t);
+        const int local = t - __ldg(T.flt_off + s);
+        const FiltScan &f = T.filt[s];
+        direct_filter_rows(f.in, f.out, (long long)local * FILT_ROWS, f.rows, f.R, f.C, f.filter_scale, f.out_scale,
+                           f.fdk, f.D, f.ddc, f.ddr, f.dco, f.dro, smflt);
+    }
+}
+
+// float64 partials of <W A x0, A x0> and <W A x0, y> per sinogram tile (A x0 is in dsino).
+__global__ void __launch_bounds__(BT_THREADS) b_init_partials(BatchedTables T, int num_scans, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.sn_off, num_scans, t);
+        const int local = t - __ldg(T.sn_off + s);
+        const VcdScan &sc = T.scans[s];
+        const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nsino, e0 + BT_SINO_TILE);
+        double den = 0.0, num = 0.0;
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
+            const float ax = sc.dsino[i];
+            const float wes = sc.wts ? __fmul_rn(sc.wts[i], ax) : ax;
+            den += (double)wes * (double)ax;
+            num += (double)wes * (double)sc.y[i];
+        }
+        const double v[2] = {den, num};
+        tile_reduce<2>(v, T.p_init + 2 * t);
+    }
+}
+
+__global__ void b_init_alpha(BatchedTables T, int num_scans) {
+    const int s = blockIdx.x * (blockDim.x >> 5) + (threadIdx.x >> 5);
+    if (s >= num_scans) return;
+    const int sb = __ldg(T.sn_off + s), se = __ldg(T.sn_off + s + 1);
+    const double den = warp_range_sum(T.p_init, sb, se, 2, 0);
+    const double num = warp_range_sum(T.p_init, sb, se, 2, 1);
+    if ((threadIdx.x & 31) == 0) T.alpha_init[s] = den > 0.0 ? (float)(num / den) : 1.0f;
+}
+
+// e = y - alpha A x0 over the sinogram tiles, then x = alpha x0 over the recon tiles.
+__global__ void __launch_bounds__(BT_THREADS) b_init_apply(BatchedTables T, int num_scans, int total_sn,
+                                                           int total_rc) {
+    for (int t = blockIdx.x; t < total_sn + total_rc; t += gridDim.x) {
+        if (t < total_sn) {
+            const int s = find_scan(T.sn_off, num_scans, t);
+            const int local = t - __ldg(T.sn_off + s);
+            const VcdScan &sc = T.scans[s];
+            const float a = T.alpha_init[s];
+            const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nsino, e0 + BT_SINO_TILE);
+            for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS)
+                sc.err[i] = __fsub_rn(sc.y[i], __fmul_rn(a, sc.dsino[i]));
+        } else {
+            const int tr = t - total_sn;
+            const int s = find_scan(T.rc_off, num_scans, tr);
+            const int local = tr - __ldg(T.rc_off + s);
+            const VcdScan &sc = T.scans[s];
+            const float a = T.alpha_init[s];
+            const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nrecon, e0 + BT_SINO_TILE);
+            for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) sc.recon[i] = __fmul_rn(a, sc.recon[i]);
+        }
+    }
+}
+
+// Chunk bounding boxes of every (scan, subset) record's pixel list (after new partitions are written).
+__global__ void __launch_bounds__(CB_CHUNK) b_chunk_bounds(BatchedTables T, int ksum, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int k = find_scan(T.box_first, ksum, t);
+        const FpArgs &f = T.fpargs[k];
+        fp_chunk_bounds_block(f.pix, f.num_pixels, f.g.num_recon_rows, f.g.num_recon_cols,
+                              const_cast<int4 *>(f.chunk_box), t - __ldg(T.box_first + k));
+    }
+}
+
 // ------------------------------------------------------------------------------------------------ host side
 struct ScanSizes {
-    long long ncyl, nsino, nrecon;
-    int bp_tiles, bp_gx, fp_tiles, el_tiles, sn_tiles, rc_tiles;
-    BpfPlan bpp;
-    CbPlan fpp;
+    long long ncyl, nsino, nrecon, npix;
+    int el_tiles, sn_tiles, rc_tiles, flt_tiles;
+    BpfPlan bpp;  // subset back projection
+    CbPlan fpp;   // subset (and initial) forward projection
+    BpfPlan ibp;  // initial back projection over the region of reconstruction
+    BpfPlan hbp;  // Hessian back projection over every pixel
+    bool setup;   // the scan carries the set-up inputs
 };
 
 static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
@@ -345,57 +499,116 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
     if (sc.subset_size > (1 << 24)) return MBX_ERR_UNSUPPORTED;  // list positions share a word with the bin
     z.ncyl = (long long)sc.subset_size * g.num_recon_slices;
     z.nsino = (long long)g.num_views * g.num_det_rows * g.num_det_channels;
-    z.nrecon = (long long)g.num_recon_rows * g.num_recon_cols * g.num_recon_slices;
-    z.bp_gx = z.bpp.gx;
-    z.bp_tiles = z.bpp.gx * z.bpp.gy;
-    z.fp_tiles = g.num_views * z.fpp.cblocks;
+    z.npix = (long long)g.num_recon_rows * g.num_recon_cols;
+    z.nrecon = z.npix * g.num_recon_slices;
     z.el_tiles = (int)((z.ncyl + BT_ELEM_TILE - 1) / BT_ELEM_TILE);
     z.sn_tiles = (int)((z.nsino + BT_SINO_TILE - 1) / BT_SINO_TILE);
     z.rc_tiles = (int)((z.nrecon + BT_SINO_TILE - 1) / BT_SINO_TILE);
+    z.setup = sc.sinogram != nullptr || sc.full_indices != nullptr || sc.num_full_indices != 0;
+    z.flt_tiles = 0;
+    if (z.setup) {
+        if (!sc.sinogram || !sc.full_indices || sc.num_full_indices <= 0 || sc.num_full_indices > z.npix)
+            return MBX_ERR_INVALID_ARG;
+        if (g.kind == MBX_GEOM_TRANSLATION) return MBX_ERR_UNSUPPORTED;  // no direct recon
+        // the initial forward projection reads voxels by pixel index, which shares a word with the bin
+        if (z.npix > (1 << 24) || z.nrecon >= (1LL << 31)) return MBX_ERR_UNSUPPORTED;
+        if (filter_smem_bytes(g.num_det_channels) > 200 * 1024) return MBX_ERR_UNSUPPORTED;
+        z.ibp = plan_bp_fast(g, sc.num_full_indices, g.num_views);
+        z.hbp = plan_bp_fast(g, z.npix, g.num_views);
+        if (!z.ibp.ok || !z.hbp.ok) return MBX_ERR_UNSUPPORTED;
+        z.flt_tiles = (int)(((long long)g.num_views * g.num_det_rows + FILT_ROWS - 1) / FILT_ROWS);
+    }
     return MBX_OK;
 }
 
+// Tiles of scan s in a projection work list, the list's per-scan dimension (gx or channel blocks) and the cost
+// of one of its tiles (to order the list: most expensive tiles first).
+static void list_dims(int which, const mbx_scan &sc, const ScanSizes &z, int &tiles, int &dim, double &cost) {
+    const mbx_geom &g = sc.geom;
+    auto bp_cost = [&](const BpfPlan &b) {
+        return (double)g.num_views * std::min(g.num_recon_slices, b.ts * b.nsl) * 32.0 * b.npg;
+    };
+    auto fp_cost = [&](long long npix) {
+        return (double)npix * (2.0 + (double)(z.fpp.nb + 2) * z.fpp.rpad / g.num_det_channels);
+    };
+    switch (which) {
+        case PL_BP: tiles = z.bpp.gx * z.bpp.gy; dim = z.bpp.gx; cost = bp_cost(z.bpp); break;
+        case PL_FP: tiles = g.num_views * z.fpp.cblocks; dim = z.fpp.cblocks; cost = fp_cost(sc.subset_size); break;
+        case PL_INIT_BP: tiles = z.setup ? z.ibp.gx * z.ibp.gy : 0; dim = z.ibp.gx; cost = bp_cost(z.ibp); break;
+        case PL_INIT_FP:
+            tiles = z.setup ? g.num_views * z.fpp.cblocks : 0;
+            dim = z.fpp.cblocks;
+            cost = fp_cost(sc.num_full_indices);
+            break;
+        default: tiles = z.setup ? z.hbp.gx * z.hbp.gy : 0; dim = z.hbp.gx; cost = bp_cost(z.hbp); break;
+    }
+}
+
 struct Layout {
-    size_t scans, bpargs, fpargs, offs, cblocks, gx, scan_of, counters, sched, p_prior, p_fwd, p_l1, p_iter, alpha,
-        bufs, total;
-    int bp_total, fp_total, el_total, sn_total, rc_total;
-    std::vector<size_t> buf_off;  // per scan: bp, delta, dsino
-    std::vector<size_t> box_off;  // per scan: chunk bounding boxes of its subsets, [K][chunks]
+    size_t scans, fm, qp, bpargs, fpargs, ibp, ifp, hbp, filt, pl_off, pl_dim, pl_order, offs, box_first, counters,
+        sched, p_prior, p_fwd, p_l1, p_iter, p_init, alpha, alpha_init, arange, total;
+    int pl_total[PL_COUNT];
+    int el_total, sn_total, rc_total, flt_total, box_total, ksum, max_npix;
+    bool setup;
+    std::vector<size_t> buf_off;   // per scan: bp, delta, dsino
+    std::vector<size_t> box_off;   // per scan: chunk boxes of its subsets, [K][chunks]
+    std::vector<size_t> fbox_off;  // per scan: chunk boxes of its region-of-reconstruction list
 };
 
 static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::vector<ScanSizes> &zs) {
     zs.resize(n);
-    L.bp_total = L.fp_total = L.el_total = L.sn_total = L.rc_total = 0;
-    int kind = -1, ksum = 0;
+    for (int w = 0; w < PL_COUNT; ++w) L.pl_total[w] = 0;
+    L.el_total = L.sn_total = L.rc_total = L.flt_total = L.box_total = L.ksum = L.max_npix = 0;
+    int kind = -1, nsetup = 0;
     for (int s = 0; s < n; ++s) {
         int rc = scan_sizes(scans[s], zs[s]);
         if (rc != MBX_OK) return rc;
         if (kind >= 0 && scans[s].geom.kind != kind) return MBX_ERR_UNSUPPORTED;  // one geometry kind per batch
         if (scans[s].num_subsets != scans[0].num_subsets) return MBX_ERR_UNSUPPORTED;  // argument table is [scan][K]
         kind = scans[s].geom.kind;
-        L.bp_total += zs[s].bp_tiles;
-        L.fp_total += zs[s].fp_tiles;
+        for (int w = 0; w < PL_COUNT; ++w) {
+            int tiles, dim;
+            double cost;
+            list_dims(w, scans[s], zs[s], tiles, dim, cost);
+            L.pl_total[w] += tiles;
+        }
         L.el_total += zs[s].el_tiles;
         L.sn_total += zs[s].sn_tiles;
         L.rc_total += zs[s].rc_tiles;
-        ksum += scans[s].num_subsets;
+        L.flt_total += zs[s].flt_tiles;
+        L.ksum += scans[s].num_subsets;
+        L.box_total += scans[s].num_subsets * (int)((scans[s].subset_size + CB_CHUNK - 1) / CB_CHUNK);
+        L.max_npix = std::max<int>(L.max_npix, (int)zs[s].npix);
+        nsetup += zs[s].setup ? 1 : 0;
     }
+    if (nsetup != 0 && nsetup != n) return MBX_ERR_INVALID_ARG;  // set-up inputs for every scan or for none
+    L.setup = nsetup == n;
     size_t off = 0;
     auto take = [&](size_t bytes) { size_t o = off; off += align256(bytes); return o; };
     L.scans = take(sizeof(VcdScan) * n);
-    L.bpargs = take(sizeof(BpArgs) * ksum);
-    L.fpargs = take(sizeof(FpArgs) * ksum);
-    L.offs = take(sizeof(int) * 5 * (n + 1));
-    L.cblocks = take(sizeof(int) * n);
-    L.gx = take(sizeof(int) * n);
-    L.scan_of = take(sizeof(int) * 2 * n);
-    L.counters = take(sizeof(int) * 2);
-    L.sched = take(sizeof(int) * (size_t)num_steps * n);
+    L.fm = take(sizeof(float) * n);
+    L.qp = take(sizeof(QParams) * n);
+    L.bpargs = take(sizeof(BpArgs) * L.ksum);
+    L.fpargs = take(sizeof(FpArgs) * L.ksum);
+    L.ibp = take(sizeof(BpArgs) * n);
+    L.ifp = take(sizeof(FpArgs) * n);
+    L.hbp = take(sizeof(BpArgs) * n);
+    L.filt = take(sizeof(FiltScan) * n);
+    L.pl_off = take(sizeof(int) * PL_COUNT * (n + 1));
+    L.pl_dim = take(sizeof(int) * PL_COUNT * n);
+    L.pl_order = take(sizeof(int) * PL_COUNT * n);
+    L.offs = take(sizeof(int) * 4 * (n + 1));
+    L.box_first = take(sizeof(int) * (L.ksum + 1));
+    L.counters = take(sizeof(int) * PL_COUNT);
+    L.sched = take(sizeof(int) * (size_t)num_steps * n);  // the host-built tables end here
     L.p_prior = take(sizeof(double) * 2 * (size_t)L.el_total);
     L.p_fwd = take(sizeof(double) * 2 * (size_t)L.sn_total);
     L.p_l1 = take(sizeof(double) * (size_t)L.el_total);
     L.p_iter = take(sizeof(double) * ((size_t)L.sn_total + L.rc_total));
+    L.p_init = take(sizeof(double) * 2 * (size_t)L.sn_total);
     L.alpha = take(sizeof(float) * n);
+    L.alpha_init = take(sizeof(float) * n);
+    L.arange = take(L.setup ? sizeof(int32_t) * (size_t)L.max_npix : 0);
     L.buf_off.resize(3 * (size_t)n);
     for (int s = 0; s < n; ++s) {
         L.buf_off[3 * s] = take(4 * (size_t)zs[s].ncyl);
@@ -403,16 +616,19 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
         L.buf_off[3 * s + 2] = take(4 * (size_t)zs[s].nsino);
     }
     L.box_off.resize(n);
-    for (int s = 0; s < n; ++s)
+    L.fbox_off.assign(n, 0);
+    for (int s = 0; s < n; ++s) {
         L.box_off[s] = take((size_t)scans[s].num_subsets * fp_chunk_box_bytes(scans[s].subset_size));
+        if (L.setup) L.fbox_off[s] = take(fp_chunk_box_bytes(scans[s].num_full_indices));
+    }
     L.total = off;
     return MBX_OK;
 }
 
 template <typename K>
-static int occupancy_grid(K kern, size_t smem, int total) {
+static int occupancy_grid(K kern, int threads, size_t smem, int total) {
     int per_sm = 0;
-    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, BT_THREADS, smem) != cudaSuccess || per_sm < 1) {
+    if (cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem) != cudaSuccess || per_sm < 1) {
         cudaGetLastError();
         per_sm = 1;
     }
@@ -420,19 +636,70 @@ static int occupancy_grid(K kern, size_t smem, int total) {
     return (int)std::max(1LL, std::min<long long>(g, total));
 }
 
-}  // namespace mbx
-
-using namespace mbx;
-
-extern "C" size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps) {
-    if (!scans || num_scans <= 0 || num_steps <= 0) return 0;
-    Layout L;
-    std::vector<ScanSizes> zs;
-    if (layout(scans, num_scans, num_steps, L, zs) != MBX_OK) return 0;
-    return L.total;
+static int bp_grid(int kind, size_t smem, int total) {
+    return kind == MBX_GEOM_PARALLEL ? occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, BPF_THREADS, smem, total)
+                                     : occupancy_grid(b_bp<MBX_GEOM_CONE>, BPF_THREADS, smem, total);
 }
 
-static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStream_t st);
+static int fp_grid(int kind, int minb, size_t smem, int total) {
+    if (kind == MBX_GEOM_PARALLEL)
+        return minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 3>, CB_THREADS, smem, total)
+                         : occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, CB_THREADS, smem, total);
+    return minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, CB_THREADS, smem, total)
+                     : occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, CB_THREADS, smem, total);
+}
+
+// One launch of a back-projection work list over tiles [first, total) (resets the list's counter first).
+static cudaError_t launch_bp_list(const BatchedPlanHost &P, int which, int step, int first, int total, int grid,
+                                  size_t smem, cudaStream_t st) {
+    ProjList L = proj_list(P.t, which, P.num_scans);
+    L.stride = which == PL_BP ? P.ksum / P.num_scans : 1;
+    cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    int *err = device_error_ptr();
+    if (P.kind == MBX_GEOM_PARALLEL)
+        b_bp<MBX_GEOM_PARALLEL><<<grid, BPF_THREADS, smem, st>>>(L, P.num_scans, step, first, total, err);
+    else
+        b_bp<MBX_GEOM_CONE><<<grid, BPF_THREADS, smem, st>>>(L, P.num_scans, step, first, total, err);
+    note_launch();
+    return cudaGetLastError();
+}
+
+// One launch of a forward-projection work list (kernel variant for minb resident CTAs per SM).
+static cudaError_t launch_fp_list(const BatchedPlanHost &P, int which, int minb, int step, int first, int total,
+                                  int grid, size_t smem, cudaStream_t st) {
+    ProjList L = proj_list(P.t, which, P.num_scans);
+    L.stride = which == PL_FP ? P.ksum / P.num_scans : 1;
+    cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
+    if (e != cudaSuccess) return e;
+    int *err = device_error_ptr();
+    const int n = P.num_scans;
+    if (P.kind == MBX_GEOM_PARALLEL) {
+        if (minb >= 3)
+            b_fp<MBX_GEOM_PARALLEL, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+        else
+            b_fp<MBX_GEOM_PARALLEL, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+    } else {
+        if (minb >= 3)
+            b_fp<MBX_GEOM_CONE, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+        else
+            b_fp<MBX_GEOM_CONE, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+    }
+    note_launch();
+    return cudaGetLastError();
+}
+
+// Key of a batch shape for the autotune cache (every scan's sizes, subsets and pixels per subset).
+static std::vector<long long> batch_key(long long tag, const BatchedPlanHost &P, const mbx_scan *scans, bool weights) {
+    std::vector<long long> key = {tag, P.kind, P.num_scans, P.fp_minb, -1};
+    for (int s = 0; s < P.num_scans; ++s) {
+        const mbx_geom &g = scans[s].geom;
+        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
+                               g.num_recon_slices, scans[s].num_subsets, scans[s].subset_size});
+        if (weights) key.push_back(scans[s].weights ? 1 : 0);
+    }
+    return key;
+}
 
 // Autotuning of the forward-projection stage: the plans of every scan with the kernel variant compiled for 2
 // resident CTAs per SM (the tables as built) against the same channel blocks with smaller passes and the variant
@@ -440,10 +707,9 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
 // zeroed first); the faster one's argument table stays on the device, and the choice is remembered for the
 // batch shape, so later plans of the same batch do not time again.
 static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vector<ScanSizes> &zs,
-                           const mbx_scan *scans, int num_scans, const FpArgs *hf2, cudaStream_t st) {
-    int ksum = 0;
-    for (int s = 0; s < num_scans; ++s) ksum += scans[s].num_subsets;
-    std::vector<FpArgs> f3(hf2, hf2 + ksum);
+                           const mbx_scan *scans, const FpArgs *hf2, cudaStream_t st) {
+    const int num_scans = P.num_scans;
+    std::vector<FpArgs> f3(hf2, hf2 + L.ksum);
     size_t smem3 = 0;
     int ki = 0;
     for (int s = 0; s < num_scans; ++s) {
@@ -453,21 +719,15 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
         for (int k = 0; k < scans[s].num_subsets; ++k, ++ki) f3[ki].plan = c3;
     }
     char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
-    // the choice is cached per batch shape (every scan's sizes, subsets and pixels per subset)
-    std::vector<long long> key = {2, P.kind, num_scans};
-    for (int s = 0; s < num_scans; ++s) {
-        const mbx_geom &g = scans[s].geom;
-        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
-                               g.num_recon_slices, scans[s].num_subsets, scans[s].subset_size});
-    }
+    const std::vector<long long> key = batch_key(2, P, scans, false);
     auto use3 = [&]() -> int {
-        cudaError_t e3 = cudaMemcpyAsync(base + L.fpargs, f3.data(), sizeof(FpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        cudaError_t e3 = cudaMemcpyAsync(base + L.fpargs, f3.data(), sizeof(FpArgs) * L.ksum, cudaMemcpyHostToDevice,
+                                         st);
         if (e3 == cudaSuccess) e3 = cudaStreamSynchronize(st);
         if (e3 != cudaSuccess) return set_cuda_error(e3);
         P.fp_minb = 3;
-        P.fp_smem = smem3;
-        P.fp_grid = (P.kind == MBX_GEOM_PARALLEL) ? occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 3>, smem3, P.fp_total)
-                                                  : occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, smem3, P.fp_total);
+        P.pl_smem[PL_FP] = smem3;
+        P.pl_grid[PL_FP] = fp_grid(P.kind, 3, smem3, P.pl_total[PL_FP]);
         return MBX_OK;
     };
     const int cached = autotune_forced() >= 0 ? (autotune_forced() >= 1 ? 3 : 2)
@@ -479,25 +739,21 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
     for (int s = 0; s < num_scans && e == cudaSuccess; ++s)
         e = cudaMemsetAsync(base + L.buf_off[3 * s + 1], 0, 4 * (size_t)zs[s].ncyl, st);
     if (e != cudaSuccess) return set_cuda_error(e);
-    int rc = MBX_OK;
     auto run = [&]() {
-        rc = launch_stage(&P, 0, 2, st);
-        return rc == MBX_OK ? cudaSuccess : cudaErrorLaunchFailure;
+        return launch_fp_list(P, PL_FP, P.fp_minb, 0, 0, P.pl_total[PL_FP], P.pl_grid[PL_FP], P.pl_smem[PL_FP], st);
     };
     float t2 = 0.0f, t3 = 0.0f;
     e = time_on_stream(run, st, t2);
-    if (rc != MBX_OK) return rc;
     if (e != cudaSuccess) return set_cuda_error(e);
     const BatchedPlanHost keep = P;
-    rc = use3();
+    int rc = use3();
     if (rc != MBX_OK) return rc;
     e = time_on_stream(run, st, t3);
-    if (rc != MBX_OK) return rc;
     if (e != cudaSuccess) return set_cuda_error(e);
     autotune_store(key.data(), (int)key.size(), t2 <= t3 ? 2 : 3);
     if (t2 <= t3) {  // back to the tables as built
         P = keep;
-        e = cudaMemcpyAsync(base + L.fpargs, hf2, sizeof(FpArgs) * ksum, cudaMemcpyHostToDevice, st);
+        e = cudaMemcpyAsync(base + L.fpargs, hf2, sizeof(FpArgs) * L.ksum, cudaMemcpyHostToDevice, st);
         if (e == cudaSuccess) e = cudaStreamSynchronize(st);
         if (e != cudaSuccess) return set_cuda_error(e);
     }
@@ -507,10 +763,11 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
 // Per-scan lane layout of the forward-projection stage, after the kernel variant is chosen: each scan is timed
 // alone on step 0 with its plan and with the best layout that has another number of sub-groups per warp (same
 // channel blocks, so the same tiles), and keeps the faster.  Cached per batch shape.
-static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, int num_scans,
-                                   const int *o_fp, const int *scan_of, cudaStream_t st) {
+static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, const int *o_fp,
+                                   const int *order_fp, cudaStream_t st) {
+    const int num_scans = P.num_scans;
     const int K = scans[0].num_subsets;  // every scan of a batch has the same number of subsets
-    const int ksum = K * num_scans;
+    const int ksum = L.ksum;
     char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
     std::vector<FpArgs> cur(ksum);
     cudaError_t e = cudaMemcpyAsync(cur.data(), base + L.fpargs, sizeof(FpArgs) * ksum, cudaMemcpyDeviceToHost, st);
@@ -528,12 +785,7 @@ static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mb
         for (int j = 0; j < K; ++j) alt[sc * K + j].plan = q;
         smem_alt = std::max(smem_alt, q.smem);
     }
-    std::vector<long long> key = {5, P.kind, num_scans, P.fp_minb, -1};
-    for (int sc = 0; sc < num_scans; ++sc) {
-        const mbx_geom &g = scans[sc].geom;
-        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
-                               g.num_recon_slices, scans[sc].num_subsets, scans[sc].subset_size});
-    }
+    std::vector<long long> key = batch_key(5, P, scans, false);
     auto use = [&](int sc, int c) {
         for (int j = 0; j < K; ++j) cur[sc * K + j] = c ? alt[sc * K + j] : orig[sc * K + j];
     };
@@ -544,13 +796,8 @@ static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mb
     auto apply_smem = [&]() {
         size_t sm = 0;
         for (int k = 0; k < ksum; ++k) sm = std::max(sm, cur[k].plan.smem);
-        P.fp_smem = sm;
-        if (P.kind == MBX_GEOM_PARALLEL)
-            P.fp_grid = P.fp_minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 3>, sm, P.fp_total)
-                                       : occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, sm, P.fp_total);
-        else
-            P.fp_grid = P.fp_minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, sm, P.fp_total)
-                                       : occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, sm, P.fp_total);
+        P.pl_smem[PL_FP] = sm;
+        P.pl_grid[PL_FP] = fp_grid(P.kind, P.fp_minb, sm, P.pl_total[PL_FP]);
     };
     bool all_cached = true;
     std::vector<int> choice(num_scans, 0);
@@ -572,29 +819,14 @@ static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mb
         apply_smem();
         return MBX_OK;
     }
-    P.fp_smem = std::max(P.fp_smem, smem_alt);  // tuning launches fit either plan
-    int *err = device_error_ptr();
+    P.pl_smem[PL_FP] = std::max(P.pl_smem[PL_FP], smem_alt);  // tuning launches fit either plan
     for (int k = 0; k < num_scans; ++k) {
-        const int sc = scan_of[num_scans + k];
+        const int sc = order_fp[k];
         if (!can[sc]) continue;
         const int first = o_fp[k], last = o_fp[k + 1];
-        const int grid = std::min(P.fp_grid, last - first);
-        auto run = [&]() -> cudaError_t {
-            cudaError_t e2 = cudaMemsetAsync(P.t.counters + 1, 0, sizeof(int), st);
-            if (e2 != cudaSuccess) return e2;
-            if (P.kind == MBX_GEOM_PARALLEL) {
-                if (P.fp_minb >= 3)
-                    b_fp<MBX_GEOM_PARALLEL, 3><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
-                else
-                    b_fp<MBX_GEOM_PARALLEL, 2><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
-            } else {
-                if (P.fp_minb >= 3)
-                    b_fp<MBX_GEOM_CONE, 3><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
-                else
-                    b_fp<MBX_GEOM_CONE, 2><<<grid, CB_THREADS, P.fp_smem, st>>>(P.t, num_scans, 0, first, last, err);
-            }
-            note_launch();
-            return cudaGetLastError();
+        const int grid = std::min(P.pl_grid[PL_FP], last - first);
+        auto run = [&]() {
+            return launch_fp_list(P, PL_FP, P.fp_minb, 0, first, last, grid, P.pl_smem[PL_FP], st);
         };
         float t[2] = {0.0f, 0.0f};
         for (int c = 0; c < 2; ++c) {
@@ -619,10 +851,11 @@ static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mb
 // launch walks only that scan's tiles; the stage only writes the scans' back-projection scratch), so that every
 // scan keeps the plan that suits its shape, as the plain path's per-call tuner would choose.  The choices are
 // cached per batch shape.
-static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, int num_scans,
-                           const BpArgs *hb1, const int *o_bp, const int *scan_of, cudaStream_t st) {
+static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *scans, const BpArgs *hb1,
+                           const int *o_bp, const int *order_bp, cudaStream_t st) {
+    const int num_scans = P.num_scans;
     const int K = scans[0].num_subsets;  // every scan of a batch has the same number of subsets
-    const int ksum = K * num_scans;
+    const int ksum = L.ksum;
     std::vector<BpArgs> cur(hb1, hb1 + ksum), alt(hb1, hb1 + ksum);
     std::vector<char> can(num_scans, 1);
     size_t smem_alt = 0;
@@ -636,13 +869,8 @@ static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *
         smem_alt = std::max(smem_alt, q.smem);
     }
     char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
-    std::vector<long long> key = {4, P.kind, num_scans, -1};
-    for (int s = 0; s < num_scans; ++s) {
-        const mbx_geom &g = scans[s].geom;
-        key.insert(key.end(), {g.num_views, g.num_det_rows, g.num_det_channels, g.num_recon_rows, g.num_recon_cols,
-                               g.num_recon_slices, scans[s].num_subsets, scans[s].subset_size,
-                               scans[s].weights ? 1 : 0});
-    }
+    std::vector<long long> key = batch_key(4, P, scans, true);
+    key[3] = -1;
     auto upload = [&]() -> cudaError_t {
         cudaError_t e = cudaMemcpyAsync(base + L.bpargs, cur.data(), sizeof(BpArgs) * ksum, cudaMemcpyHostToDevice, st);
         return e == cudaSuccess ? cudaStreamSynchronize(st) : e;
@@ -650,9 +878,8 @@ static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *
     auto apply_smem = [&]() {
         size_t sm = 0;
         for (int k = 0; k < ksum; ++k) sm = std::max(sm, cur[k].plan.smem);
-        P.bp_smem = sm;
-        P.bp_grid = (P.kind == MBX_GEOM_PARALLEL) ? occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, sm, P.bp_total)
-                                                  : occupancy_grid(b_bp<MBX_GEOM_CONE>, sm, P.bp_total);
+        P.pl_smem[PL_BP] = sm;
+        P.pl_grid[PL_BP] = bp_grid(P.kind, sm, P.pl_total[PL_BP]);
     };
     auto use = [&](int s, int c) {
         for (int j = 0; j < K; ++j) cur[s * K + j] = c ? alt[s * K + j] : hb1[s * K + j];
@@ -664,7 +891,7 @@ static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *
         if (autotune_forced() >= 0) {
             choice[s] = autotune_forced() >= 1 ? 1 : 0;
         } else {
-            key[3] = s;
+            key[4] = s;
             const int c = autotune_lookup(key.data(), (int)key.size());
             if (c < 0) all_cached = false;
             choice[s] = c == 1 ? 1 : 0;
@@ -677,23 +904,13 @@ static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *
         apply_smem();
         return MBX_OK;
     }
-    P.bp_smem = std::max(P.bp_smem, smem_alt);  // tuning launches fit either plan
-    int *err = device_error_ptr();
+    P.pl_smem[PL_BP] = std::max(P.pl_smem[PL_BP], smem_alt);  // tuning launches fit either plan
     for (int k = 0; k < num_scans; ++k) {
-        const int s = scan_of[k];
+        const int s = order_bp[k];
         if (!can[s]) continue;
         const int first = o_bp[k], last = o_bp[k + 1];
-        const int grid = std::min(P.bp_grid, last - first);
-        auto run = [&]() -> cudaError_t {
-            cudaError_t e = cudaMemsetAsync(P.t.counters, 0, sizeof(int), st);
-            if (e != cudaSuccess) return e;
-            if (P.kind == MBX_GEOM_PARALLEL)
-                b_bp<MBX_GEOM_PARALLEL><<<grid, BPF_THREADS, P.bp_smem, st>>>(P.t, num_scans, 0, first, last, err);
-            else
-                b_bp<MBX_GEOM_CONE><<<grid, BPF_THREADS, P.bp_smem, st>>>(P.t, num_scans, 0, first, last, err);
-            note_launch();
-            return cudaGetLastError();
-        };
+        const int grid = std::min(P.pl_grid[PL_BP], last - first);
+        auto run = [&]() { return launch_bp_list(P, PL_BP, 0, first, last, grid, P.pl_smem[PL_BP], st); };
         float t[2] = {0.0f, 0.0f};
         for (int c = 0; c < 2; ++c) {
             use(s, c);
@@ -703,13 +920,48 @@ static int tune_batched_bp(BatchedPlanHost &P, const Layout &L, const mbx_scan *
         }
         choice[s] = t[1] < t[0] ? 1 : 0;
         use(s, choice[s]);
-        key[3] = s;
+        key[4] = s;
         autotune_store(key.data(), (int)key.size(), choice[s]);
     }
     cudaError_t e = upload();
     if (e != cudaSuccess) return set_cuda_error(e);
     apply_smem();
     return MBX_OK;
+}
+
+// Per-call parameter tables: fm constants and qGGMRF parameters.
+static void fill_params(const mbx_scan *scans, int n, float *fm, QParams *qp) {
+    for (int s = 0; s < n; ++s) {
+        fm[s] = scans[s].fm_constant;
+        qp[s] = make_qparams(scans[s].qp);
+    }
+}
+
+static int check_schedule(const mbx_scan *scans, int n, const int32_t *schedule, int num_steps) {
+    for (int st = 0; st < num_steps; ++st)
+        for (int s = 0; s < n; ++s) {
+            const int v = schedule[(size_t)st * n + s];
+            if (v < 0 || v >= scans[s].num_subsets) return MBX_ERR_INVALID_ARG;
+        }
+    return MBX_OK;
+}
+
+}  // namespace mbx
+
+using namespace mbx;
+
+extern "C" size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps) {
+    if (!scans || num_scans <= 0 || num_steps <= 0) return 0;
+    Layout L;
+    std::vector<ScanSizes> zs;
+    if (layout(scans, num_scans, num_steps, L, zs) != MBX_OK) return 0;
+    return L.total;
+}
+
+static const BatchedPlanHost *plan_of(const mbx_batched_plan *p) {
+    if (!p) return nullptr;
+    const BatchedPlanHost *P = reinterpret_cast<const BatchedPlanHost *>(p);
+    return P->magic == BT_MAGIC ? P : nullptr;
 }
 
 extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans, const int32_t *schedule,
@@ -724,201 +976,267 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     int rc = layout(scans, num_scans, num_steps, L, zs);
     if (rc != MBX_OK) return rc;
     if (!workspace || workspace_bytes < L.total) return MBX_ERR_WORKSPACE;
-    for (int st = 0; st < num_steps; ++st)
-        for (int s = 0; s < num_scans; ++s) {
-            const int v = schedule[(size_t)st * num_scans + s];
-            if (v < 0 || v >= scans[s].num_subsets) return MBX_ERR_INVALID_ARG;
-        }
+    rc = check_schedule(scans, num_scans, schedule, num_steps);
+    if (rc != MBX_OK) return rc;
+    const int n = num_scans, n1 = num_scans + 1;
     char *base = static_cast<char *>(workspace);
-    std::vector<char> host(L.sched + sizeof(int) * (size_t)num_steps * num_scans, 0);
-    int *hscan_of = reinterpret_cast<int *>(host.data() + L.scan_of);
+    std::vector<char> host(L.sched + sizeof(int) * (size_t)num_steps * n, 0);
     VcdScan *hs = reinterpret_cast<VcdScan *>(host.data() + L.scans);
     BpArgs *hb = reinterpret_cast<BpArgs *>(host.data() + L.bpargs);
     FpArgs *hf = reinterpret_cast<FpArgs *>(host.data() + L.fpargs);
+    BpArgs *hib = reinterpret_cast<BpArgs *>(host.data() + L.ibp);
+    FpArgs *hif = reinterpret_cast<FpArgs *>(host.data() + L.ifp);
+    BpArgs *hhb = reinterpret_cast<BpArgs *>(host.data() + L.hbp);
+    FiltScan *hfl = reinterpret_cast<FiltScan *>(host.data() + L.filt);
+    int *hpl_off = reinterpret_cast<int *>(host.data() + L.pl_off);
+    int *hpl_dim = reinterpret_cast<int *>(host.data() + L.pl_dim);
+    int *hpl_order = reinterpret_cast<int *>(host.data() + L.pl_order);
     int *hoff = reinterpret_cast<int *>(host.data() + L.offs);
-    int *hcb = reinterpret_cast<int *>(host.data() + L.cblocks);
-    int *hgx = reinterpret_cast<int *>(host.data() + L.gx);
-    int *hsched = reinterpret_cast<int *>(host.data() + L.sched);
-    const int n1 = num_scans + 1;
-    int *o_bp = hoff, *o_fp = hoff + n1, *o_el = hoff + 2 * n1, *o_sn = hoff + 3 * n1, *o_rc = hoff + 4 * n1;
-    o_bp[0] = o_fp[0] = o_el[0] = o_sn[0] = o_rc[0] = 0;
-    size_t smem_bp = 0, smem_fp = 0;
+    int *hbox_first = reinterpret_cast<int *>(host.data() + L.box_first);
+    int *o_el = hoff, *o_sn = hoff + n1, *o_rc = hoff + 2 * n1, *o_flt = hoff + 3 * n1;
+    fill_params(scans, n, reinterpret_cast<float *>(host.data() + L.fm), reinterpret_cast<QParams *>(host.data() + L.qp));
+    o_el[0] = o_sn[0] = o_rc[0] = o_flt[0] = 0;
+    hbox_first[0] = 0;
+    auto bp_args = [](const mbx_geom &g, const float *sino, const float *wts, const int32_t *pix, long long npix,
+                      int cp, float *out, int by_index, const BpfPlan &plan) {
+        BpArgs a;
+        std::memset(&a, 0, sizeof(a));
+        a.g = g;
+        a.sino = sino;
+        a.wts = wts;
+        a.pix = pix;
+        a.num_pixels = npix;
+        a.order = nullptr;
+        a.views = nullptr;
+        a.num_views_sel = g.num_views;
+        a.views_per_split = g.num_views;
+        a.coeff_power = cp;
+        a.scale = 1.0f;
+        a.out = out;
+        a.split_stride = 0;
+        a.out_by_index = by_index;
+        a.plan = plan;
+        return a;
+    };
     int ki = 0;
-    for (int s = 0; s < num_scans; ++s) {
+    for (int s = 0; s < n; ++s) {
         const mbx_scan &sc = scans[s];
         const ScanSizes &z = zs[s];
+        const mbx_geom &g = sc.geom;
         VcdScan &v = hs[s];
         v.recon = sc.flat_recon;
         v.err = sc.error_sinogram;
         v.wts = sc.weights;
-        v.hess = sc.fm_hessian;
+        v.hess = const_cast<float *>(sc.fm_hessian);
         v.partition = sc.partition;
         v.bp = reinterpret_cast<float *>(base + L.buf_off[3 * s]);
         v.delta = reinterpret_cast<float *>(base + L.buf_off[3 * s + 1]);
         v.dsino = reinterpret_cast<float *>(base + L.buf_off[3 * s + 2]);
+        v.y = sc.sinogram;
         v.nsino = z.nsino;
         v.nrecon = z.nrecon;
         v.K = sc.num_subsets;
         v.M = sc.subset_size;
-        v.nr = sc.geom.num_recon_rows;
-        v.nc = sc.geom.num_recon_cols;
-        v.ns = sc.geom.num_recon_slices;
-        v.fm_constant = sc.fm_constant;
-        v.q = make_qparams(sc.qp);
+        v.nr = g.num_recon_rows;
+        v.nc = g.num_recon_cols;
+        v.ns = g.num_recon_slices;
         for (int k = 0; k < sc.num_subsets; ++k, ++ki) {
-            BpArgs &a = hb[ki];
-            a.g = sc.geom;
-            a.sino = sc.error_sinogram;
-            a.wts = sc.weights;
-            a.pix = sc.partition + (size_t)k * sc.subset_size;
-            a.num_pixels = sc.subset_size;
-            a.order = sc.partition_order ? sc.partition_order + (size_t)k * sc.subset_size : nullptr;
-            a.views = nullptr;
-            a.num_views_sel = sc.geom.num_views;
-            a.views_per_split = sc.geom.num_views;
-            a.coeff_power = 1;
-            a.scale = 1.0f;
-            a.out = v.bp;
-            a.split_stride = 0;
-            a.out_by_index = 0;
-            a.plan = z.bpp;
+            const int32_t *pix = sc.partition + (size_t)k * sc.subset_size;
+            hb[ki] = bp_args(g, sc.error_sinogram, sc.weights, pix, sc.subset_size, 1, v.bp, 0, z.bpp);
+            if (sc.partition_order) hb[ki].order = sc.partition_order + (size_t)k * sc.subset_size;
             FpArgs &f = hf[ki];
-            f.g = sc.geom;
+            std::memset(&f, 0, sizeof(f));
+            f.g = g;
             f.vox = v.delta;
-            f.pix = a.pix;
+            f.pix = pix;
             f.num_pixels = sc.subset_size;
             f.views = nullptr;
-            f.num_views_sel = sc.geom.num_views;
+            f.num_views_sel = g.num_views;
             f.out = v.dsino;
             f.vox_by_index = 0;
             f.plan = z.fpp;
             f.chunk_box = reinterpret_cast<const int4 *>(base + L.box_off[s] + (size_t)k * fp_chunk_box_bytes(sc.subset_size));
+            hbox_first[ki + 1] = hbox_first[ki] + (int)((sc.subset_size + CB_CHUNK - 1) / CB_CHUNK);
         }
-        // bp_fast smem without view splits
-        smem_bp = std::max(smem_bp, z.bpp.smem);
-        smem_fp = std::max(smem_fp, z.fpp.smem);
-        hcb[s] = z.fpp.cblocks;
-        hgx[s] = z.bp_gx;
+        if (L.setup) {
+            // x0: back projection of the filtered sinogram (held in the error sinogram) into the recon, by index
+            hib[s] = bp_args(g, sc.error_sinogram, nullptr, sc.full_indices, sc.num_full_indices, 1, sc.flat_recon, 1,
+                             z.ibp);
+            FpArgs &f = hif[s];
+            std::memset(&f, 0, sizeof(f));
+            f.g = g;
+            f.vox = sc.flat_recon;
+            f.pix = sc.full_indices;
+            f.num_pixels = sc.num_full_indices;
+            f.num_views_sel = g.num_views;
+            f.out = v.dsino;
+            f.vox_by_index = 1;
+            f.plan = z.fpp;
+            f.chunk_box = reinterpret_cast<const int4 *>(base + L.fbox_off[s]);
+            // Hessian: the weights (or ones: no sinogram) with squared coefficients over every pixel
+            hhb[s] = bp_args(g, sc.weights, nullptr, reinterpret_cast<const int32_t *>(base + L.arange), z.npix, 2,
+                             const_cast<float *>(sc.fm_hessian), 0, z.hbp);
+            FiltScan &fl = hfl[s];
+            fl.in = sc.sinogram;
+            fl.out = sc.error_sinogram;
+            fl.rows = (long long)g.num_views * g.num_det_rows;
+            fl.R = g.num_det_rows;
+            fl.C = g.num_det_channels;
+            direct_filter_scales(g, fl.filter_scale, fl.out_scale, fl.fdk);
+            fl.D = g.source_detector_dist;
+            fl.ddc = g.delta_det_channel;
+            fl.ddr = g.delta_det_row;
+            fl.dco = g.det_channel_offset;
+            fl.dro = g.det_row_offset;
+        }
         o_el[s + 1] = o_el[s] + z.el_tiles;
         o_sn[s + 1] = o_sn[s] + z.sn_tiles;
         o_rc[s + 1] = o_rc[s] + z.rc_tiles;
+        o_flt[s + 1] = o_flt[s] + z.flt_tiles;
     }
-    // bp / fp work lists: scans in decreasing order of per-tile cost, so that the dynamically scheduled tail of
+    // projection work lists: scans in decreasing order of per-tile cost, so that the dynamically scheduled tail of
     // a launch is made of the cheapest tiles
-    {
-        std::vector<int> ord(num_scans);
-        std::vector<double> cost(num_scans);
-        for (int s = 0; s < num_scans; ++s) {
-            const mbx_geom &g = scans[s].geom;
-            cost[s] = (double)g.num_views * std::min(g.num_recon_slices, zs[s].bpp.ts * zs[s].bpp.nsl) * 32.0 * zs[s].bpp.npg;
+    size_t pl_smem[PL_COUNT] = {0, 0, 0, 0, 0};
+    for (int w = 0; w < PL_COUNT; ++w) {
+        std::vector<int> ord(n), tiles(n), dim(n);
+        std::vector<double> cost(n);
+        for (int s = 0; s < n; ++s) {
+            list_dims(w, scans[s], zs[s], tiles[s], dim[s], cost[s]);
             ord[s] = s;
+            const ScanSizes &z = zs[s];
+            const size_t sm = w == PL_BP ? z.bpp.smem : (w == PL_FP || w == PL_INIT_FP) ? z.fpp.smem
+                              : w == PL_INIT_BP ? (z.setup ? z.ibp.smem : 0) : (z.setup ? z.hbp.smem : 0);
+            pl_smem[w] = std::max(pl_smem[w], sm);
         }
         std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-        for (int k = 0; k < num_scans; ++k) {
-            hscan_of[k] = ord[k];
-            o_bp[k + 1] = o_bp[k] + zs[ord[k]].bp_tiles;
+        int *off = hpl_off + w * n1;
+        off[0] = 0;
+        for (int k = 0; k < n; ++k) {
+            hpl_order[w * n + k] = ord[k];
+            off[k + 1] = off[k] + tiles[ord[k]];
         }
-        for (int s = 0; s < num_scans; ++s) {
-            const mbx_geom &g = scans[s].geom;
-            cost[s] = (double)scans[s].subset_size *
-                      (2.0 + (double)(zs[s].fpp.nb + 2) * zs[s].fpp.rpad / g.num_det_channels);
-            ord[s] = s;
-        }
-        std::stable_sort(ord.begin(), ord.end(), [&](int a, int b) { return cost[a] > cost[b]; });
-        for (int k = 0; k < num_scans; ++k) {
-            hscan_of[num_scans + k] = ord[k];
-            o_fp[k + 1] = o_fp[k] + zs[ord[k]].fp_tiles;
-        }
+        for (int s = 0; s < n; ++s) hpl_dim[w * n + s] = dim[s];
     }
-    std::memcpy(hsched, schedule, sizeof(int) * (size_t)num_steps * num_scans);
+    std::memcpy(host.data() + L.sched, schedule, sizeof(int) * (size_t)num_steps * n);
     cudaStream_t st = static_cast<cudaStream_t>(stream);
     cudaError_t e = cudaMemcpyAsync(base, host.data(), host.size(), cudaMemcpyHostToDevice, st);
-    // chunk bounding boxes of every subset (the forward projection skips chunks that miss its channel block)
-    for (int s = 0; s < num_scans && e == cudaSuccess; ++s) {
-        const mbx_scan &sc = scans[s];
-        const unsigned nch = (unsigned)((sc.subset_size + CB_CHUNK - 1) / CB_CHUNK);
-        for (int k = 0; k < sc.num_subsets && e == cudaSuccess; ++k) {
-            int4 *box = reinterpret_cast<int4 *>(base + L.box_off[s] + (size_t)k * fp_chunk_box_bytes(sc.subset_size));
-            fp_chunk_bounds_kernel<<<nch, CB_CHUNK, 0, st>>>(sc.partition + (size_t)k * sc.subset_size, sc.subset_size,
-                                                             sc.geom.num_recon_rows, sc.geom.num_recon_cols, box);
-            note_launch();
-            e = cudaGetLastError();
-        }
+    if (e == cudaSuccess && L.setup) {
+        std::vector<int32_t> ar((size_t)L.max_npix);
+        for (int i = 0; i < L.max_npix; ++i) ar[i] = i;
+        e = cudaMemcpyAsync(base + L.arange, ar.data(), sizeof(int32_t) * ar.size(), cudaMemcpyHostToDevice, st);
+        if (e == cudaSuccess) e = cudaStreamSynchronize(st);  // ar is released at scope end
     }
-    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error(e);
 
     BatchedPlanHost P;
     std::memset(&P, 0, sizeof(P));
     P.t.scans = reinterpret_cast<VcdScan *>(base + L.scans);
+    P.t.fm = reinterpret_cast<float *>(base + L.fm);
+    P.t.qp = reinterpret_cast<QParams *>(base + L.qp);
     P.t.bpargs = reinterpret_cast<BpArgs *>(base + L.bpargs);
     P.t.fpargs = reinterpret_cast<FpArgs *>(base + L.fpargs);
+    P.t.init_bp = reinterpret_cast<BpArgs *>(base + L.ibp);
+    P.t.init_fp = reinterpret_cast<FpArgs *>(base + L.ifp);
+    P.t.hess_bp = reinterpret_cast<BpArgs *>(base + L.hbp);
+    P.t.filt = reinterpret_cast<FiltScan *>(base + L.filt);
+    P.t.pl_off = reinterpret_cast<int *>(base + L.pl_off);
+    P.t.pl_dim = reinterpret_cast<int *>(base + L.pl_dim);
+    P.t.pl_order = reinterpret_cast<int *>(base + L.pl_order);
     int *doff = reinterpret_cast<int *>(base + L.offs);
-    P.t.bp_off = doff;
-    P.t.fp_off = doff + n1;
-    P.t.el_off = doff + 2 * n1;
-    P.t.sn_off = doff + 3 * n1;
-    P.t.rc_off = doff + 4 * n1;
-    P.t.fp_cblocks = reinterpret_cast<int *>(base + L.cblocks);
-    P.t.bp_gx = reinterpret_cast<int *>(base + L.gx);
-    P.t.bp_scan = reinterpret_cast<int *>(base + L.scan_of);
-    P.t.fp_scan = P.t.bp_scan + num_scans;
+    P.t.el_off = doff;
+    P.t.sn_off = doff + n1;
+    P.t.rc_off = doff + 2 * n1;
+    P.t.flt_off = doff + 3 * n1;
+    P.t.box_first = reinterpret_cast<int *>(base + L.box_first);
     P.t.counters = reinterpret_cast<int *>(base + L.counters);
     P.t.schedule = reinterpret_cast<int *>(base + L.sched);
     P.t.p_prior = reinterpret_cast<double *>(base + L.p_prior);
     P.t.p_fwd = reinterpret_cast<double *>(base + L.p_fwd);
     P.t.p_l1 = reinterpret_cast<double *>(base + L.p_l1);
     P.t.p_iter = reinterpret_cast<double *>(base + L.p_iter);
+    P.t.p_init = reinterpret_cast<double *>(base + L.p_init);
     P.t.alpha = reinterpret_cast<float *>(base + L.alpha);
+    P.t.alpha_init = reinterpret_cast<float *>(base + L.alpha_init);
     P.t.step_stats = step_stats;
     P.t.iter_stats = iter_stats;
-    P.num_scans = num_scans;
+    P.num_scans = n;
     P.kind = scans[0].geom.kind;
     P.num_steps = num_steps;
     P.num_iterations = num_iterations;
-    P.bp_total = L.bp_total;
-    P.fp_total = L.fp_total;
+    P.ksum = L.ksum;
+    P.has_setup = L.setup ? 1 : 0;
+    for (int w = 0; w < PL_COUNT; ++w) {
+        P.pl_total[w] = L.pl_total[w];
+        P.pl_smem[w] = pl_smem[w];
+    }
     P.el_total = L.el_total;
     P.sn_total = L.sn_total;
     P.rc_total = L.rc_total;
-    P.bp_smem = smem_bp;
-    P.fp_smem = smem_fp;
+    P.flt_total = L.flt_total;
+    P.box_total = L.box_total;
     P.fp_minb = 2;
+    size_t flt_smem = 0;
+    for (int s = 0; s < n; ++s)
+        if (zs[s].setup) flt_smem = std::max(flt_smem, filter_smem_bytes(scans[s].geom.num_det_channels));
+    P.flt_smem = flt_smem;
     // kernel attributes and resident-CTA grids
-    if (P.kind == MBX_GEOM_PARALLEL) {
-        set_max_dynamic_smem(reinterpret_cast<const void *>(b_bp<MBX_GEOM_PARALLEL>), 100 * 1024);
-        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 2>), 200 * 1024);
-        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>), 200 * 1024);
-        P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, smem_bp, L.bp_total);
-        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, smem_fp, L.fp_total);
-    } else {
-        set_max_dynamic_smem(reinterpret_cast<const void *>(b_bp<MBX_GEOM_CONE>), 100 * 1024);
-        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 2>), 200 * 1024);
-        set_max_dynamic_smem(reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>), 200 * 1024);
-        P.bp_grid = occupancy_grid(b_bp<MBX_GEOM_CONE>, smem_bp, L.bp_total);
-        P.fp_grid = occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, smem_fp, L.fp_total);
-    }
+    const bool par = P.kind == MBX_GEOM_PARALLEL;
+    const void *kbp = par ? reinterpret_cast<const void *>(b_bp<MBX_GEOM_PARALLEL>)
+                          : reinterpret_cast<const void *>(b_bp<MBX_GEOM_CONE>);
+    const void *kfp2 = par ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 2>)
+                           : reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 2>);
+    const void *kfp3 = par ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>)
+                           : reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>);
+    e = set_max_dynamic_smem(kbp, 100 * 1024);
+    if (e == cudaSuccess) e = set_max_dynamic_smem(kfp2, 200 * 1024);
+    if (e == cudaSuccess) e = set_max_dynamic_smem(kfp3, 200 * 1024);
+    if (e == cudaSuccess) e = set_max_dynamic_smem(reinterpret_cast<const void *>(b_filter), 200 * 1024);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    P.pl_grid[PL_BP] = bp_grid(P.kind, P.pl_smem[PL_BP], P.pl_total[PL_BP]);
+    P.pl_grid[PL_FP] = fp_grid(P.kind, 2, P.pl_smem[PL_FP], P.pl_total[PL_FP]);
+    P.pl_grid[PL_INIT_BP] = bp_grid(P.kind, P.pl_smem[PL_INIT_BP], std::max(1, P.pl_total[PL_INIT_BP]));
+    P.pl_grid[PL_INIT_FP] = fp_grid(P.kind, 2, P.pl_smem[PL_INIT_FP], std::max(1, P.pl_total[PL_INIT_FP]));
+    P.pl_grid[PL_HESS] = bp_grid(P.kind, P.pl_smem[PL_HESS], std::max(1, P.pl_total[PL_HESS]));
     {   // load every stage kernel now (lazy module loading must not happen inside a stream capture)
         cudaFuncAttributes fa;
-        cudaFuncGetAttributes(&fa, b_delta);
-        cudaFuncGetAttributes(&fa, b_linquad);
-        cudaFuncGetAttributes(&fa, b_alpha);
-        cudaFuncGetAttributes(&fa, b_apply);
-        cudaFuncGetAttributes(&fa, b_error);
-        cudaFuncGetAttributes(&fa, b_l1);
-        cudaFuncGetAttributes(&fa, b_iter_partials);
-        cudaFuncGetAttributes(&fa, b_iter_final);
+        const void *ks[] = {reinterpret_cast<const void *>(b_delta), reinterpret_cast<const void *>(b_linquad),
+                            reinterpret_cast<const void *>(b_alpha), reinterpret_cast<const void *>(b_apply),
+                            reinterpret_cast<const void *>(b_error), reinterpret_cast<const void *>(b_l1),
+                            reinterpret_cast<const void *>(b_iter_partials),
+                            reinterpret_cast<const void *>(b_iter_final),
+                            reinterpret_cast<const void *>(b_zero_recon), reinterpret_cast<const void *>(b_filter),
+                            reinterpret_cast<const void *>(b_init_partials),
+                            reinterpret_cast<const void *>(b_init_alpha),
+                            reinterpret_cast<const void *>(b_init_apply),
+                            reinterpret_cast<const void *>(b_chunk_bounds)};
+        for (const void *k : ks) cudaFuncGetAttributes(&fa, k);
         device_error_ptr();
     }
-    P.el_grid = occupancy_grid(b_delta, 0, L.el_total);
-    P.sn_grid = occupancy_grid(b_linquad, 0, L.sn_total);
-    P.rc_grid = occupancy_grid(b_iter_partials, 0, L.sn_total + L.rc_total);
+    P.el_grid = occupancy_grid(b_delta, BT_THREADS, 0, L.el_total);
+    P.sn_grid = occupancy_grid(b_linquad, BT_THREADS, 0, L.sn_total);
+    P.rc_grid = occupancy_grid(b_iter_partials, BT_THREADS, 0, L.sn_total + L.rc_total);
+    P.flt_grid = occupancy_grid(b_filter, FILT_THREADS, std::max<size_t>(flt_smem, 1), std::max(1, L.flt_total));
+    P.box_grid = occupancy_grid(b_chunk_bounds, CB_CHUNK, 0, std::max(1, L.box_total));
     e = cudaGetLastError();
     if (e != cudaSuccess) return set_cuda_error(e);
+    // chunk bounding boxes of every subset, and of every region-of-reconstruction list
+    b_chunk_bounds<<<P.box_grid, CB_CHUNK, 0, st>>>(P.t, P.ksum, P.box_total);
+    note_launch();
+    for (int s = 0; s < n && L.setup; ++s) {
+        const unsigned nch = (unsigned)((scans[s].num_full_indices + CB_CHUNK - 1) / CB_CHUNK);
+        fp_chunk_bounds_kernel<<<nch, CB_CHUNK, 0, st>>>(scans[s].full_indices, scans[s].num_full_indices,
+                                                         scans[s].geom.num_recon_rows, scans[s].geom.num_recon_cols,
+                                                         reinterpret_cast<int4 *>(base + L.fbox_off[s]));
+        note_launch();
+    }
+    e = cudaGetLastError();
+    if (e == cudaSuccess) e = cudaStreamSynchronize(st);
+    if (e != cudaSuccess) return set_cuda_error(e);
     if (autotune_enabled()) {  // (also in forced mode: the tune functions then apply the forced choice)
-        int rc2 = tune_batched_fp(P, L, zs, scans, num_scans, hf, st);
-        if (rc2 == MBX_OK) rc2 = tune_batched_fp_layouts(P, L, scans, num_scans, o_fp, hscan_of, st);
-        if (rc2 == MBX_OK) rc2 = tune_batched_bp(P, L, scans, num_scans, hb, o_bp, hscan_of, st);
+        const int *o_bp = hpl_off + PL_BP * n1, *o_fp = hpl_off + PL_FP * n1;
+        int rc2 = tune_batched_fp(P, L, zs, scans, hf, st);
+        if (rc2 == MBX_OK) rc2 = tune_batched_fp_layouts(P, L, scans, o_fp, hpl_order + PL_FP * n, st);
+        if (rc2 == MBX_OK) rc2 = tune_batched_bp(P, L, scans, hb, o_bp, hpl_order + PL_BP * n, st);
         if (rc2 != MBX_OK) return rc2;
     }
     P.magic = BT_MAGIC;
@@ -927,46 +1245,21 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     return MBX_OK;
 }
 
-static const BatchedPlanHost *plan_of(const mbx_batched_plan *p) {
-    if (!p) return nullptr;
-    const BatchedPlanHost *P = reinterpret_cast<const BatchedPlanHost *>(p);
-    return P->magic == BT_MAGIC ? P : nullptr;
-}
-
 static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStream_t st) {
-    int *err = device_error_ptr();
     const BatchedTables &T = P->t;
     const int n = P->num_scans;
     const int warp_blocks = (n + 7) / 8;
+    int *err = device_error_ptr();
+    cudaError_t e = cudaSuccess;
     switch (stage) {
         case 0:
-            {
-                const cudaError_t me = cudaMemsetAsync(T.counters, 0, sizeof(int), st);
-                if (me != cudaSuccess) return set_cuda_error(me);
-            }
-            if (P->kind == MBX_GEOM_PARALLEL)
-                b_bp<MBX_GEOM_PARALLEL><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, 0, P->bp_total, err);
-            else
-                b_bp<MBX_GEOM_CONE><<<P->bp_grid, BPF_THREADS, P->bp_smem, st>>>(T, n, step, 0, P->bp_total, err);
-            break;
+            e = launch_bp_list(*P, PL_BP, step, 0, P->pl_total[PL_BP], P->pl_grid[PL_BP], P->pl_smem[PL_BP], st);
+            return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
         case 1: b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err); break;
         case 2:
-            {
-                const cudaError_t me = cudaMemsetAsync(T.counters + 1, 0, sizeof(int), st);
-                if (me != cudaSuccess) return set_cuda_error(me);
-            }
-            if (P->kind == MBX_GEOM_PARALLEL) {
-                if (P->fp_minb >= 3)
-                    b_fp<MBX_GEOM_PARALLEL, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
-                else
-                    b_fp<MBX_GEOM_PARALLEL, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
-            } else {
-                if (P->fp_minb >= 3)
-                    b_fp<MBX_GEOM_CONE, 3><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
-                else
-                    b_fp<MBX_GEOM_CONE, 2><<<P->fp_grid, CB_THREADS, P->fp_smem, st>>>(T, n, step, 0, P->fp_total, err);
-            }
-            break;
+            e = launch_fp_list(*P, PL_FP, P->fp_minb, step, 0, P->pl_total[PL_FP], P->pl_grid[PL_FP],
+                               P->pl_smem[PL_FP], st);
+            return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
         case 3: b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;
         case 4: b_alpha<<<warp_blocks, 256, 0, st>>>(T, n, step); break;
         case 5: b_apply<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total); break;
@@ -975,7 +1268,7 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
         default: return MBX_ERR_INVALID_ARG;
     }
     note_launch();
-    cudaError_t e = cudaGetLastError();
+    e = cudaGetLastError();
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
 }
 
@@ -1003,6 +1296,73 @@ extern "C" int mbx_vcd_batched_iteration_stats(const mbx_batched_plan *plan, int
     b_iter_partials<<<P->rc_grid, BT_THREADS, 0, st>>>(P->t, n, P->sn_total, P->rc_total);
     note_launch();
     b_iter_final<<<(n + 7) / 8, 256, 0, st>>>(P->t, n, iteration, P->sn_total);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+}
+
+extern "C" int mbx_vcd_batched_setup(const mbx_batched_plan *plan, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P) return MBX_ERR_INVALID_ARG;
+    if (!P->has_setup) return MBX_ERR_UNSUPPORTED;
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    const BatchedTables &T = P->t;
+    const int n = P->num_scans;
+    b_zero_recon<<<P->rc_grid, BT_THREADS, 0, st>>>(T, n, P->rc_total);
+    note_launch();
+    b_filter<<<P->flt_grid, FILT_THREADS, P->flt_smem, st>>>(T, n, P->flt_total);
+    note_launch();
+    cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = launch_bp_list(*P, PL_INIT_BP, 0, 0, P->pl_total[PL_INIT_BP], P->pl_grid[PL_INIT_BP],
+                           P->pl_smem[PL_INIT_BP], st);
+    if (e == cudaSuccess)
+        e = launch_fp_list(*P, PL_INIT_FP, 2, 0, 0, P->pl_total[PL_INIT_FP], P->pl_grid[PL_INIT_FP],
+                           P->pl_smem[PL_INIT_FP], st);
+    if (e != cudaSuccess) return set_cuda_error(e);
+    b_init_partials<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
+    note_launch();
+    b_init_alpha<<<(n + 7) / 8, 256, 0, st>>>(T, n);
+    note_launch();
+    b_init_apply<<<P->rc_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total, P->rc_total);
+    note_launch();
+    e = cudaGetLastError();
+    if (e == cudaSuccess)
+        e = launch_bp_list(*P, PL_HESS, 0, 0, P->pl_total[PL_HESS], P->pl_grid[PL_HESS], P->pl_smem[PL_HESS], st);
+    return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+}
+
+extern "C" int mbx_vcd_batched_update(const mbx_batched_plan *plan, const mbx_scan *scans, int32_t num_scans,
+                                      const int32_t *schedule, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P || !scans || !schedule || num_scans != P->num_scans) return MBX_ERR_INVALID_ARG;
+    int ksum = 0;
+    for (int s = 0; s < num_scans; ++s) {
+        if (!(scans[s].qp.sigma_x > 0.0f) || !(scans[s].qp.T > 0.0f) || !(scans[s].qp.p > 0.0f))
+            return MBX_ERR_INVALID_ARG;
+        ksum += scans[s].num_subsets;
+    }
+    if (ksum != P->ksum) return MBX_ERR_INVALID_ARG;
+    int rc = check_schedule(scans, num_scans, schedule, P->num_steps);
+    if (rc != MBX_OK) return rc;
+    std::vector<float> fm(num_scans);
+    std::vector<QParams> qp(num_scans);
+    fill_params(scans, num_scans, fm.data(), qp.data());
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    // from pageable host memory: each copy is staged before the call returns, so the vectors may go
+    cudaError_t e = cudaMemcpyAsync(P->t.fm, fm.data(), sizeof(float) * num_scans, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(P->t.qp, qp.data(), sizeof(QParams) * num_scans, cudaMemcpyHostToDevice, st);
+    if (e == cudaSuccess)
+        e = cudaMemcpyAsync(P->t.schedule, schedule, sizeof(int32_t) * (size_t)P->num_steps * num_scans,
+                            cudaMemcpyHostToDevice, st);
+    return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+}
+
+extern "C" int mbx_vcd_batched_refresh(const mbx_batched_plan *plan, void *stream) {
+    const BatchedPlanHost *P = plan_of(plan);
+    if (!P) return MBX_ERR_INVALID_ARG;
+    b_chunk_bounds<<<P->box_grid, CB_CHUNK, 0, static_cast<cudaStream_t>(stream)>>>(P->t, P->ksum, P->box_total);
     note_launch();
     cudaError_t e = cudaGetLastError();
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
