@@ -13,12 +13,13 @@ and kept in a small cache, so later calls of the same shape only copy their sino
 run the host part (auto-regularisation statistics and the reference's partition and subset-order draws) while the
 set-up runs on the device, upload the new parameters and partitions, and replay the iteration graph.
 
-Restrictions of the batched path: all scans share one geometry kind (parallel or cone beam; translation
-geometry runs through ``TomographyModel.recon`` only), have psf radius 1, and use a single partition with the
-same number of subsets (``granularity=[K]``, ``partition_sequence=[0]``).
+Restrictions of the batched path: all scans share one geometry kind (parallel, cone or translation), have psf
+radius 1, and use a single partition with the same number of subsets (``granularity=[K]``,
+``partition_sequence=[0]``).  Translation scans start from zeros, as ``TranslationModel.recon`` does (the reference
+has no direct recon for that geometry).
 """
 import collections
-import ctypes
+import warnings
 
 import numpy as np
 import torch
@@ -42,7 +43,7 @@ def release_batched_sessions():
 class BatchedVCD:
     """recon() of many models at once.
 
-    models: list of ParallelBeamModel or ConeBeamModel (one kind), sinograms / weights: per-scan arrays or
+    models: list of ParallelBeamModel, ConeBeamModel or TranslationModel (one kind), sinograms / weights: per-scan arrays or
     tensors (weights entries may be None), seeds: per-scan np.random seeds applied before each scan's partition
     draw (None: use the global stream as is, scan after scan), init_recons: per-scan init (None: direct recon).
     """
@@ -84,7 +85,14 @@ class BatchedVCD:
                 num_subsets = part.shape[0]
             elif part.shape[0] != num_subsets:
                 raise ValueError('all scans of a batch need the same number of subsets')
-            for _ in range(2):
+            # the set-up's region-of-reconstruction draws: direct recon's back projection (none for translation
+            # geometry, whose direct recon is zeros) and the initial forward projection
+            if model._kind() == _capi.MBX_GEOM_TRANSLATION:
+                warnings.warn('direct_recon not implemented for TomographyModel.')
+                draws = 1
+            else:
+                draws = 2
+            for _ in range(draws):
                 gen_full_indices(recon_shape, use_ror_mask=model.use_ror_mask)
             schedules.append(np.stack([np.random.permutation(num_subsets) for _ in range(max_iterations)]))
             parts.append(morton_sorted_partition(part, recon_shape[1]))  # spatially coherent processing order
@@ -214,7 +222,10 @@ class _Session:
             g = _capi.MbxGeom.from_buffer_copy(g0)
             view_params = np.asarray(model.get_params(model.get_params('view_params_name')), dtype=np.float32)
             ang = torch.as_tensor(view_params, device=dev).contiguous()
-            g.angles = ang.data_ptr()
+            if g.kind == _capi.MBX_GEOM_TRANSLATION:
+                g.translations = ang.data_ptr()
+            else:
+                g.angles = ang.data_ptr()
             self.geoms.append(g)
             self.angles.append(ang)
             V, R, C = (int(v) for v in model.get_params('sinogram_shape'))

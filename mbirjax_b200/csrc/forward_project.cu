@@ -4,8 +4,8 @@
 // ParallelBeamModel.forward_project_pixel_batch_to_one_view (parallel_beam.py:138-178),
 // ConeBeamModel.forward_project_pixel_batch_to_one_view (cone_beam.py:189-377) and
 // TranslationModel.forward_project_pixel_batch_to_one_view (translation_model.py:190-378).
-// Parallel and cone beam run the channel-block kernel of fp_cb.cuh when its plan fits; translation geometry and
-// the other cases run the general kernel below.
+// Radius-1 geometries run the channel-block kernel of fp_cb.cuh when its plan fits (translation geometry when the
+// caller gives a magnification bound); the other cases run the general kernel below.
 //
 // One CTA owns an output tile (one view x a band of detector rows x all channels) held in shared memory,
 // walks every pixel of its pixel range in chunks of FP_PB, and scatters into the tile with shared-memory
@@ -244,10 +244,16 @@ static cudaError_t launch_fp_cb_v(const FpArgs &A, cudaStream_t st) {
 }
 
 static cudaError_t launch_fp_cb(const FpArgs &A, cudaStream_t st) {
-    const bool par = A.g.kind == MBX_GEOM_PARALLEL;
-    if (A.plan.minb >= 3)
-        return par ? launch_fp_cb_v<MBX_GEOM_PARALLEL, 3>(A, st) : launch_fp_cb_v<MBX_GEOM_CONE, 3>(A, st);
-    return par ? launch_fp_cb_v<MBX_GEOM_PARALLEL, 2>(A, st) : launch_fp_cb_v<MBX_GEOM_CONE, 2>(A, st);
+    const bool three = A.plan.minb >= 3;
+    switch (A.g.kind) {
+        case MBX_GEOM_PARALLEL:
+            return three ? launch_fp_cb_v<MBX_GEOM_PARALLEL, 3>(A, st) : launch_fp_cb_v<MBX_GEOM_PARALLEL, 2>(A, st);
+        case MBX_GEOM_CONE:
+            return three ? launch_fp_cb_v<MBX_GEOM_CONE, 3>(A, st) : launch_fp_cb_v<MBX_GEOM_CONE, 2>(A, st);
+        default:
+            return three ? launch_fp_cb_v<MBX_GEOM_TRANSLATION, 3>(A, st)
+                         : launch_fp_cb_v<MBX_GEOM_TRANSLATION, 2>(A, st);
+    }
 }
 
 int forward_project(const mbx_geom &g, const float *vox, const int32_t *pix, long long num_pixels,

@@ -22,6 +22,9 @@
 //  4. Write: the copies of each tile element are summed in a fixed order and written, coalesced.
 // For cone beam each lane evaluates the detector-row-centric vertical fan of the reference
 // (cone_beam.py:347-372, including the 128-row batch anchor) for its rows, reading the cylinder directly.
+// Translation geometry (translation_model.py:190-378) is the cone's arithmetic with the view's translation in
+// place of the rotation, rows spaced by delta_recon_row, no delta_voxel factor in the channel coefficient, and the
+// slice heights shifted by -tz (a per-view constant of the tile).
 #pragma once
 
 #include <climits>
@@ -66,7 +69,7 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
     pl.o_rec = (int)o;
     o += 4 * (size_t)(pl.cap + CB_PAD);
     pl.o_rec2 = (int)o;
-    if (kind == MBX_GEOM_CONE) o += 4 * (size_t)pl.cap;
+    if (kind != MBX_GEOM_PARALLEL) o += 4 * (size_t)pl.cap;
     pl.o_sbin = (int)o;
     o += pl.cap + CB_PAD;
     pl.o_ubin = (int)o;
@@ -80,7 +83,7 @@ inline size_t cb_layout(CbPlan &pl, int kind, int R) {
     pl.o_wstart = (int)o;
     o += (size_t)CB_WARPS * pl.nbins;
     pl.o_cone = (int)o;
-    if (kind == MBX_GEOM_CONE) o += 3 * (size_t)R;
+    if (kind != MBX_GEOM_PARALLEL) o += 3 * (size_t)R;
     pl.o_hl = (int)o;
     o += CB_THREADS;
     pl.o_misc = (int)o;
@@ -96,7 +99,10 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
                          int nb_max = 128, int avoid_ppw = 0) {
     CbPlan pl = {};
     pl.minb = minb;
-    pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || (g.kind == MBX_GEOM_CONE && g.bp_psf_radius == 1));
+    // translation geometry: radius 1 in both fans, and a magnification bound from the host (which also says that
+    // no pixel reaches the source plane, so the channel's denominator has one sign over the recon)
+    pl.ok = g.psf_radius == 1 && (g.kind == MBX_GEOM_PARALLEL || (g.kind == MBX_GEOM_CONE && g.bp_psf_radius == 1) ||
+                                  (g.kind == MBX_GEOM_TRANSLATION && g.max_magnification > 0.0f));
     const int R = g.num_det_rows, C = g.num_det_channels;
     // lane layout: padded rows weighted by the cost of ppw diverging sub-groups, plus a small cost per pass
     static const int combos[12][2] = {{1, 1}, {1, 2}, {1, 3}, {1, 4}, {2, 1}, {2, 2},
@@ -178,6 +184,11 @@ __device__ __forceinline__ float cb_channel(const mbx_geom &g, float cs, float s
                                             float &mag) {
     const float inv_dc = 1.0f / g.delta_det_channel;
     const float det_center_channel = 0.5f * (float)(g.num_det_channels - 1);
+    if (KIND == MBX_GEOM_TRANSLATION) {  // (cs, sn) carry the view's (tx, ty): no rotation
+        const float xp = xt - cs, yp = yt - sn;
+        mag = 1.0f / (1.0f / g.magnification - yp * inv_d);
+        return (mag * xp + g.det_channel_offset) * inv_dc + det_center_channel;
+    }
     const float x_p = cs * xt - sn * yt;
     if (KIND == MBX_GEOM_PARALLEL) {
         mag = 1.0f;
@@ -193,7 +204,7 @@ __device__ __forceinline__ float cb_channel(const mbx_geom &g, float cs, float s
 template <int KIND>
 __device__ __forceinline__ void cb_footprint(const mbx_geom &g, float cs, float sn, float xt, float yt, int nc,
                                              float &a0, float &a1, float &a2, float &imd, float &wr, float &mdz,
-                                             float &mz0) {
+                                             float &mz0, float tz = 0.0f) {
     const float inv_dc = 1.0f / g.delta_det_channel;
     const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
     float mag;
@@ -204,6 +215,20 @@ __device__ __forceinline__ void cb_footprint(const mbx_geom &g, float cs, float 
         w = (g.delta_voxel * inv_dc) * cos_alpha;
         scale = g.delta_voxel / cos_alpha;
         imd = wr = mdz = mz0 = 0.0f;
+    } else if (KIND == MBX_GEOM_TRANSLATION) {
+        // coefficient L / cos(theta_p) with no delta_voxel factor (translation_model.py:244-284); the vertical fan
+        // is the cone's with slice heights delta_voxel k + z0, z0 = -tz - delta_voxel (S-1)/2
+        const float u = mag * (xt - cs);
+        const float t = u * inv_d;
+        const float cos_tp = rsqrtf(fmaf(t, t, 1.0f));
+        w = mag * (g.delta_voxel * inv_dc);
+        scale = 1.0f / cos_tp;
+        imd = 1.0f / (mag * g.delta_voxel);
+        wr = (mag * g.delta_voxel) / g.delta_det_row;
+        const float mdd = mag * inv_d;
+        const float z0 = -tz - g.delta_voxel * 0.5f * (float)(g.num_recon_slices - 1);
+        mdz = mdd * g.delta_voxel;
+        mz0 = mdd * z0;
     } else {
         const float u = mag * (cs * xt - sn * yt);
         const float t = u * inv_d;
@@ -309,6 +334,12 @@ static __global__ void __launch_bounds__(CB_CHUNK) fp_chunk_bounds_kernel(const 
     fp_chunk_bounds_block(pix, num_pixels, num_rows, num_cols, box, blockIdx.x);
 }
 
+// Pixel position relative to the recon centre (ALU); translation geometry spaces rows by delta_recon_row.
+template <int KIND>
+__device__ __forceinline__ void cb_pixel(const mbx_geom &g, int idx, float inv_cols, float &xt, float &yt) {
+    pixel_tilde_fast(g, idx, inv_cols, xt, yt, KIND == MBX_GEOM_TRANSLATION ? g.delta_recon_row : 0.0f);
+}
+
 // True when no pixel of the box can have a centre channel in [n0 - 1, n0 + nb] (one rounding step of slack
 // on each side).  The channel is a linear (parallel) or linear-fractional (cone, denominator of one sign) function
 // of the pixel position, so its extremes over the box are at the corners.
@@ -321,7 +352,8 @@ __device__ __forceinline__ bool cb_box_misses(const mbx_geom &g, int4 bx, float 
     for (int corner = 0; corner < 4; ++corner) {
         const int r = (corner & 1) ? bx.y : bx.x;
         const int c = (corner & 2) ? bx.w : bx.z;
-        const float yt = g.delta_voxel * ((float)r - 0.5f * (float)(g.num_recon_rows - 1));
+        const float dy = KIND == MBX_GEOM_TRANSLATION ? g.delta_recon_row : g.delta_voxel;
+        const float yt = dy * ((float)r - 0.5f * (float)(g.num_recon_rows - 1));
         const float xt = g.delta_voxel * ((float)c - 0.5f * (float)(g.num_recon_cols - 1));
         float mag;
         const float np = cb_channel<KIND>(g, cs, sn, xt, yt, inv_d, mag);
@@ -403,7 +435,7 @@ __device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, 
             trow[j] = P.tile + ((size_t)sub * pl.rpad + m[j]) * pl.pitch;
             rw[j].vm = rw[j].vb = 0.f;
             rw[j].b0 = 0;
-            if (KIND == MBX_GEOM_CONE) {
+            if (KIND != MBX_GEOM_PARALLEL) {
                 rw[j].vm = P.s_vm[mc];
                 rw[j].vb = P.s_vb[mc];
                 rw[j].b0 = P.s_b0[mc];
@@ -445,7 +477,7 @@ __device__ __forceinline__ void cb_accumulate(const FpArgs &A, const CbPass &P, 
                 rq[u] = P.rec[ii];
                 bq[u] = P.sbin[ii];
                 float4 cv = make_float4(0.f, 0.f, 0.f, 0.f);
-                if (KIND == MBX_GEOM_CONE) cv = P.rec2[ii];
+                if (KIND != MBX_GEOM_PARALLEL) cv = P.rec2[ii];
                 const int off = __float_as_int(rq[u].x);  // 32-bit element offset of the cylinder
 #pragma unroll
                 for (int j = 0; j < RPL; ++j)
@@ -645,9 +677,20 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     const int vi = A.views ? A.views[j] : j;
     const bool view_ok = vi >= 0 && vi < g.num_views;
     if (!view_ok && tid == 0 && cb == 0) flag_error(err, MBX_ERRFLAG_VIEW);
-    const float angle = view_ok ? g.angles[vi] : 0.0f;
-    const float cs = cosf(angle), sn = sinf(angle);
-    const float kconst = 0.5f * (float)(num_slices - 1) - g.recon_slice_offset / g.delta_voxel;
+    float cs, sn, tz = 0.0f;  // translation: (cs, sn, tz) = the view's (tx, ty, tz)
+    if (KIND == MBX_GEOM_TRANSLATION) {
+        cs = view_ok ? g.translations[3 * vi] : 0.0f;
+        sn = view_ok ? g.translations[3 * vi + 1] : 0.0f;
+        tz = view_ok ? g.translations[3 * vi + 2] : 0.0f;
+    } else {
+        const float angle = view_ok ? g.angles[vi] : 0.0f;
+        cs = cosf(angle);
+        sn = sinf(angle);
+    }
+    // slice coordinate of detector height 0: (S-1)/2 - recon_slice_offset / delta_voxel (the translation view's
+    // slice heights are shifted by -tz instead)
+    const float zoff = KIND == MBX_GEOM_TRANSLATION ? -tz : g.recon_slice_offset;
+    const float kconst = 0.5f * (float)(num_slices - 1) - zoff / g.delta_voxel;
     const float inv_cols = 1.0f / (float)g.num_recon_cols;
     const float inv_d = isinf(g.source_detector_dist) ? 0.0f : 1.0f / g.source_detector_dist;
 
@@ -655,7 +698,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
     const int tile_words = pl.ppw * pl.rpad * pl.pitch;
     for (int i = tid; i < tile_words; i += CB_THREADS) tile[i] = 0.0f;
     for (int i = tid; i < CB_WARPS * nbins; i += CB_THREADS) wcnt[i] = 0;
-    if (KIND == MBX_GEOM_CONE) {
+    if (KIND != MBX_GEOM_PARALLEL) {
         int rows_per_batch = g.entries_per_cylinder_batch;
         if (rows_per_batch > num_rows) rows_per_batch = num_rows;
         const float det_center_row = 0.5f * (float)(num_rows - 1);
@@ -729,7 +772,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
                     if (cb == 0 && j == 0) flag_error(err, MBX_ERRFLAG_PIXEL);
                 } else {
                     float xt, yt, mag;
-                    pixel_tilde_fast(g, idx, inv_cols, xt, yt);
+                    cb_pixel<KIND>(g, idx, inv_cols, xt, yt);
                     const int nc = (int)rintf(cb_channel<KIND>(g, cs, sn, xt, yt, inv_d, mag));
                     bin = nc - n0 + 1;
                     take = bin >= 0 && bin < nbins;
@@ -811,12 +854,12 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
                 const int key = (int)(ub & 0xFFFFFFu);
                 const int idx = A.vox_by_index ? key : __ldg(A.pix + key);  // checked in the scan
                 float xt, yt;
-                pixel_tilde_fast(g, idx, inv_cols, xt, yt);
+                cb_pixel<KIND>(g, idx, inv_cols, xt, yt);
                 float a0, a1, a2, imd, wr, mdz, mz0;
-                cb_footprint<KIND>(g, cs, sn, xt, yt, n0 + b - 1, a0, a1, a2, imd, wr, mdz, mz0);
+                cb_footprint<KIND>(g, cs, sn, xt, yt, n0 + b - 1, a0, a1, a2, imd, wr, mdz, mz0, tz);
                 // element offset of the pixel's cylinder (the host admits vox buffers of < 2^31 elements)
                 rec[pos] = make_float4(__int_as_float(key * num_slices), a0, a1, a2);
-                if (KIND == MBX_GEOM_CONE) rec2[pos] = make_float4(imd, wr, mdz, mz0);
+                if (KIND != MBX_GEOM_PARALLEL) rec2[pos] = make_float4(imd, wr, mdz, mz0);
                 sbin[pos] = b;
             }
             // the next chunk's counts go to wcnt (cleared above); its starts overwrite wstart only after the

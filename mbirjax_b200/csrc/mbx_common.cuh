@@ -40,9 +40,10 @@ __device__ __forceinline__ void pixel_tilde(const mbx_geom &g, int idx, float &x
 }
 
 // Same, with the row / column split of the flat index done by a float reciprocal (inv_cols = 1/num_recon_cols)
-// and an exact integer correction instead of an integer division.
+// and an exact integer correction instead of an integer division; row_pitch > 0 replaces delta_voxel as the row
+// spacing (translation geometry's delta_recon_row).
 __device__ __forceinline__ void pixel_tilde_fast(const mbx_geom &g, int idx, float inv_cols, float &x_tilde,
-                                                 float &y_tilde) {
+                                                 float &y_tilde, float row_pitch = 0.0f) {
     int row = __float2int_rz(__int2float_rz(idx) * inv_cols);
     int col = idx - row * g.num_recon_cols;
     if (col < 0) {
@@ -52,7 +53,7 @@ __device__ __forceinline__ void pixel_tilde_fast(const mbx_geom &g, int idx, flo
         ++row;
         col -= g.num_recon_cols;
     }
-    y_tilde = g.delta_voxel * ((float)row - 0.5f * (float)(g.num_recon_rows - 1));
+    y_tilde = (row_pitch > 0.0f ? row_pitch : g.delta_voxel) * ((float)row - 0.5f * (float)(g.num_recon_rows - 1));
     x_tilde = g.delta_voxel * ((float)col - 0.5f * (float)(g.num_recon_cols - 1));
 }
 

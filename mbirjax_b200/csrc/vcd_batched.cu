@@ -464,6 +464,18 @@ __global__ void __launch_bounds__(BT_THREADS) b_init_apply(BatchedTables T, int 
     }
 }
 
+// Translation geometry has no direct recon: x0 = 0, so A x0 = 0, alpha = 1 and e = y (the reference's base-class
+// direct_recon returns zeros, tomography_model.py:934-949).
+__global__ void __launch_bounds__(BT_THREADS) b_copy_sino(BatchedTables T, int num_scans, int total) {
+    for (int t = blockIdx.x; t < total; t += gridDim.x) {
+        const int s = find_scan(T.sn_off, num_scans, t);
+        const int local = t - __ldg(T.sn_off + s);
+        const VcdScan &sc = T.scans[s];
+        const long long e0 = (long long)local * BT_SINO_TILE, e1 = min(sc.nsino, e0 + BT_SINO_TILE);
+        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) sc.err[i] = sc.y[i];
+    }
+}
+
 // Chunk bounding boxes of every (scan, subset) record's pixel list (after new partitions are written).
 __global__ void __launch_bounds__(CB_CHUNK) b_chunk_bounds(BatchedTables T, int ksum, int total) {
     for (int t = blockIdx.x; t < total; t += gridDim.x) {
@@ -509,14 +521,18 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
     if (z.setup) {
         if (!sc.sinogram || !sc.full_indices || sc.num_full_indices <= 0 || sc.num_full_indices > z.npix)
             return MBX_ERR_INVALID_ARG;
-        if (g.kind == MBX_GEOM_TRANSLATION) return MBX_ERR_UNSUPPORTED;  // no direct recon
         // the initial forward projection reads voxels by pixel index, which shares a word with the bin
         if (z.npix > (1 << 24) || z.nrecon >= (1LL << 31)) return MBX_ERR_UNSUPPORTED;
-        if (filter_smem_bytes(g.num_det_channels) > 200 * 1024) return MBX_ERR_UNSUPPORTED;
-        z.ibp = plan_bp_fast(g, sc.num_full_indices, g.num_views);
         z.hbp = plan_bp_fast(g, z.npix, g.num_views);
-        if (!z.ibp.ok || !z.hbp.ok) return MBX_ERR_UNSUPPORTED;
-        z.flt_tiles = (int)(((long long)g.num_views * g.num_det_rows + FILT_ROWS - 1) / FILT_ROWS);
+        if (!z.hbp.ok) return MBX_ERR_UNSUPPORTED;
+        if (g.kind != MBX_GEOM_TRANSLATION) {  // translation geometry starts from zeros (no direct recon)
+            if (filter_smem_bytes(g.num_det_channels) > 200 * 1024) return MBX_ERR_UNSUPPORTED;
+            z.ibp = plan_bp_fast(g, sc.num_full_indices, g.num_views);
+            if (!z.ibp.ok) return MBX_ERR_UNSUPPORTED;
+            z.flt_tiles = (int)(((long long)g.num_views * g.num_det_rows + FILT_ROWS - 1) / FILT_ROWS);
+        } else {
+            z.ibp = z.hbp;  // unused
+        }
     }
     return MBX_OK;
 }
@@ -534,9 +550,13 @@ static void list_dims(int which, const mbx_scan &sc, const ScanSizes &z, int &ti
     switch (which) {
         case PL_BP: tiles = z.bpp.gx * z.bpp.gy; dim = z.bpp.gx; cost = bp_cost(z.bpp); break;
         case PL_FP: tiles = g.num_views * z.fpp.cblocks; dim = z.fpp.cblocks; cost = fp_cost(sc.subset_size); break;
-        case PL_INIT_BP: tiles = z.setup ? z.ibp.gx * z.ibp.gy : 0; dim = z.ibp.gx; cost = bp_cost(z.ibp); break;
+        case PL_INIT_BP:
+            tiles = (z.setup && g.kind != MBX_GEOM_TRANSLATION) ? z.ibp.gx * z.ibp.gy : 0;
+            dim = z.ibp.gx;
+            cost = bp_cost(z.ibp);
+            break;
         case PL_INIT_FP:
-            tiles = z.setup ? g.num_views * z.fpp.cblocks : 0;
+            tiles = (z.setup && g.kind != MBX_GEOM_TRANSLATION) ? g.num_views * z.fpp.cblocks : 0;
             dim = z.fpp.cblocks;
             cost = fp_cost(sc.num_full_indices);
             break;
@@ -636,17 +656,29 @@ static int occupancy_grid(K kern, int threads, size_t smem, int total) {
     return (int)std::max(1LL, std::min<long long>(g, total));
 }
 
+// The projection stage kernels of a geometry kind.
+static const void *bp_kernel_of(int kind) {
+    return kind == MBX_GEOM_PARALLEL ? reinterpret_cast<const void *>(b_bp<MBX_GEOM_PARALLEL>)
+           : kind == MBX_GEOM_CONE   ? reinterpret_cast<const void *>(b_bp<MBX_GEOM_CONE>)
+                                     : reinterpret_cast<const void *>(b_bp<MBX_GEOM_TRANSLATION>);
+}
+
+static const void *fp_kernel_of(int kind, int minb) {
+    if (minb >= 3)
+        return kind == MBX_GEOM_PARALLEL ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>)
+               : kind == MBX_GEOM_CONE   ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>)
+                                         : reinterpret_cast<const void *>(b_fp<MBX_GEOM_TRANSLATION, 3>);
+    return kind == MBX_GEOM_PARALLEL ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 2>)
+           : kind == MBX_GEOM_CONE   ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 2>)
+                                     : reinterpret_cast<const void *>(b_fp<MBX_GEOM_TRANSLATION, 2>);
+}
+
 static int bp_grid(int kind, size_t smem, int total) {
-    return kind == MBX_GEOM_PARALLEL ? occupancy_grid(b_bp<MBX_GEOM_PARALLEL>, BPF_THREADS, smem, total)
-                                     : occupancy_grid(b_bp<MBX_GEOM_CONE>, BPF_THREADS, smem, total);
+    return occupancy_grid(bp_kernel_of(kind), BPF_THREADS, smem, total);
 }
 
 static int fp_grid(int kind, int minb, size_t smem, int total) {
-    if (kind == MBX_GEOM_PARALLEL)
-        return minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 3>, CB_THREADS, smem, total)
-                         : occupancy_grid(b_fp<MBX_GEOM_PARALLEL, 2>, CB_THREADS, smem, total);
-    return minb >= 3 ? occupancy_grid(b_fp<MBX_GEOM_CONE, 3>, CB_THREADS, smem, total)
-                     : occupancy_grid(b_fp<MBX_GEOM_CONE, 2>, CB_THREADS, smem, total);
+    return occupancy_grid(fp_kernel_of(kind, minb), CB_THREADS, smem, total);
 }
 
 // One launch of a back-projection work list over tiles [first, total) (resets the list's counter first).
@@ -659,8 +691,10 @@ static cudaError_t launch_bp_list(const BatchedPlanHost &P, int which, int step,
     int *err = device_error_ptr();
     if (P.kind == MBX_GEOM_PARALLEL)
         b_bp<MBX_GEOM_PARALLEL><<<grid, BPF_THREADS, smem, st>>>(L, P.num_scans, step, first, total, err);
-    else
+    else if (P.kind == MBX_GEOM_CONE)
         b_bp<MBX_GEOM_CONE><<<grid, BPF_THREADS, smem, st>>>(L, P.num_scans, step, first, total, err);
+    else
+        b_bp<MBX_GEOM_TRANSLATION><<<grid, BPF_THREADS, smem, st>>>(L, P.num_scans, step, first, total, err);
     note_launch();
     return cudaGetLastError();
 }
@@ -679,11 +713,16 @@ static cudaError_t launch_fp_list(const BatchedPlanHost &P, int which, int minb,
             b_fp<MBX_GEOM_PARALLEL, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
         else
             b_fp<MBX_GEOM_PARALLEL, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
-    } else {
+    } else if (P.kind == MBX_GEOM_CONE) {
         if (minb >= 3)
             b_fp<MBX_GEOM_CONE, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
         else
             b_fp<MBX_GEOM_CONE, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+    } else {
+        if (minb >= 3)
+            b_fp<MBX_GEOM_TRANSLATION, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+        else
+            b_fp<MBX_GEOM_TRANSLATION, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
     }
     note_launch();
     return cudaGetLastError();
@@ -1180,13 +1219,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
         if (zs[s].setup) flt_smem = std::max(flt_smem, filter_smem_bytes(scans[s].geom.num_det_channels));
     P.flt_smem = flt_smem;
     // kernel attributes and resident-CTA grids
-    const bool par = P.kind == MBX_GEOM_PARALLEL;
-    const void *kbp = par ? reinterpret_cast<const void *>(b_bp<MBX_GEOM_PARALLEL>)
-                          : reinterpret_cast<const void *>(b_bp<MBX_GEOM_CONE>);
-    const void *kfp2 = par ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 2>)
-                           : reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 2>);
-    const void *kfp3 = par ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>)
-                           : reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>);
+    const void *kbp = bp_kernel_of(P.kind), *kfp2 = fp_kernel_of(P.kind, 2), *kfp3 = fp_kernel_of(P.kind, 3);
     e = set_max_dynamic_smem(kbp, 100 * 1024);
     if (e == cudaSuccess) e = set_max_dynamic_smem(kfp2, 200 * 1024);
     if (e == cudaSuccess) e = set_max_dynamic_smem(kfp3, 200 * 1024);
@@ -1208,6 +1241,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
                             reinterpret_cast<const void *>(b_init_partials),
                             reinterpret_cast<const void *>(b_init_alpha),
                             reinterpret_cast<const void *>(b_init_apply),
+                            reinterpret_cast<const void *>(b_copy_sino),
                             reinterpret_cast<const void *>(b_chunk_bounds)};
         for (const void *k : ks) cudaFuncGetAttributes(&fa, k);
         device_error_ptr();
@@ -1310,23 +1344,30 @@ extern "C" int mbx_vcd_batched_setup(const mbx_batched_plan *plan, void *stream)
     const int n = P->num_scans;
     b_zero_recon<<<P->rc_grid, BT_THREADS, 0, st>>>(T, n, P->rc_total);
     note_launch();
-    b_filter<<<P->flt_grid, FILT_THREADS, P->flt_smem, st>>>(T, n, P->flt_total);
-    note_launch();
     cudaError_t e = cudaGetLastError();
-    if (e == cudaSuccess)
-        e = launch_bp_list(*P, PL_INIT_BP, 0, 0, P->pl_total[PL_INIT_BP], P->pl_grid[PL_INIT_BP],
-                           P->pl_smem[PL_INIT_BP], st);
-    if (e == cudaSuccess)
-        e = launch_fp_list(*P, PL_INIT_FP, 2, 0, 0, P->pl_total[PL_INIT_FP], P->pl_grid[PL_INIT_FP],
-                           P->pl_smem[PL_INIT_FP], st);
-    if (e != cudaSuccess) return set_cuda_error(e);
-    b_init_partials<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
-    note_launch();
-    b_init_alpha<<<(n + 7) / 8, 256, 0, st>>>(T, n);
-    note_launch();
-    b_init_apply<<<P->rc_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total, P->rc_total);
-    note_launch();
-    e = cudaGetLastError();
+    if (P->kind == MBX_GEOM_TRANSLATION) {  // zero initial recon: e = y
+        b_copy_sino<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
+        note_launch();
+        e = cudaGetLastError();
+    } else {
+        b_filter<<<P->flt_grid, FILT_THREADS, P->flt_smem, st>>>(T, n, P->flt_total);
+        note_launch();
+        e = cudaGetLastError();
+        if (e == cudaSuccess)
+            e = launch_bp_list(*P, PL_INIT_BP, 0, 0, P->pl_total[PL_INIT_BP], P->pl_grid[PL_INIT_BP],
+                               P->pl_smem[PL_INIT_BP], st);
+        if (e == cudaSuccess)
+            e = launch_fp_list(*P, PL_INIT_FP, 2, 0, 0, P->pl_total[PL_INIT_FP], P->pl_grid[PL_INIT_FP],
+                               P->pl_smem[PL_INIT_FP], st);
+        if (e != cudaSuccess) return set_cuda_error(e);
+        b_init_partials<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total);
+        note_launch();
+        b_init_alpha<<<(n + 7) / 8, 256, 0, st>>>(T, n);
+        note_launch();
+        b_init_apply<<<P->rc_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total, P->rc_total);
+        note_launch();
+        e = cudaGetLastError();
+    }
     if (e == cudaSuccess)
         e = launch_bp_list(*P, PL_HESS, 0, 0, P->pl_total[PL_HESS], P->pl_grid[PL_HESS], P->pl_smem[PL_HESS], st);
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);

@@ -68,15 +68,28 @@ def test_batched_cone_with_weights(cuda):
         assert rel_l2(rec.cpu().numpy(), plain) <= 1e-5
 
 
-def test_batched_rejects_translation_geometry(cuda):
-    # the batched kernels cover parallel and cone beam; translation scans are refused before any launch
-    from cases import make_case
-    model, geom = make_case('translation', views=12, rows=6, channels=24)
-    model.set_params(sharpness=0.0, granularity=[4], partition_sequence=[0], verbose=0)
-    sino = np.random.default_rng(0).random(geom.sinogram_shape).astype(np.float32)
+def test_batched_translation_matches_plain(cuda):
+    """Translation scans in one batch: zero initialisation as TranslationModel.recon, the same partition and subset
+    draws, and the translation kernels of the batched stages give the plain path's reconstructions."""
+    from cases import translations_for
+    items = []
+    for views, rows, channels, seed in ((12, 6, 24, 2), (16, 8, 28, 3)):
+        model = mb.TranslationModel((views, rows, channels), translations_for(views, seed=seed),
+                                    source_detector_dist=4.0 * channels, source_iso_dist=4.0 * channels)
+        model.set_params(sharpness=0.0, granularity=[4], partition_sequence=[0], verbose=0)
+        shape = tuple(model.get_params('recon_shape'))
+        ph = gen_ellipsoid_phantom(shape, 4, seed).numpy()
+        sino = model.forward_project(torch.as_tensor(ph, device='cuda')).cpu().numpy()
+        items.append((model, sino, seed))
+    models, sinos, seeds = [it[0] for it in items], [it[1] for it in items], [it[2] for it in items]
     with pytest.warns(UserWarning):  # no direct recon for translation geometry: the init is zeros
-        with pytest.raises(mb.MbxError):
-            BatchedVCD([model], [sino], seeds=[0]).recon(max_iterations=1)
+        recons, _ = BatchedVCD(models, sinos, seeds=seeds).recon(max_iterations=3)
+    for (model, sino, sd), rec in zip(items, recons):
+        np.random.seed(sd)
+        with pytest.warns(UserWarning):
+            plain, _ = model.recon(sino, max_iterations=3, stop_threshold_change_pct=0, logfile_path=None,
+                                   print_logs=False)
+        assert rel_l2(rec.cpu().numpy(), plain.cpu().numpy()) <= 1e-5
 
 
 def test_morton_order_is_a_permutation():
