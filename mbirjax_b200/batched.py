@@ -34,6 +34,19 @@ _SESSIONS = collections.OrderedDict()  # batch key -> _Session, most recently us
 _MAX_SESSIONS = 2
 
 
+_POOL = None
+
+
+def _draw_pool():
+    """Host threads for the per-scan draws."""
+    global _POOL
+    if _POOL is None:
+        import concurrent.futures
+        import os
+        _POOL = concurrent.futures.ThreadPoolExecutor(max_workers=min(16, os.cpu_count() or 1))
+    return _POOL
+
+
 def release_batched_sessions():
     """Free the device state (buffers, plans, graphs) kept for the batch shapes reconstructed so far."""
     while _SESSIONS:
@@ -64,45 +77,56 @@ class BatchedVCD:
         return ([_view_subsample(sino) for sino in self.sinograms],
                 [None if w is None else _view_subsample(w) for w in self.weights])
 
+    def _scan_draws(self, i, max_iterations, small, small_w, rng):
+        """Host part of scan i, in the reference's np.random order on the stream rng (None: the global stream):
+        auto-regularisation (on the host subsamples), the partition, the region-of-reconstruction draws of the
+        set-up (direct recon's back projection and the initial forward projection) and the subset order of every
+        iteration.  Returns (regularisation dict, Morton-sorted partition, schedule (iterations, K), fm constant,
+        qGGMRF record, sigma_y)."""
+        model = self.models[i]
+        reg = model.auto_set_regularization_params(small[i], weights=small_w[i])
+        recon_shape, granularity = model.get_params(['recon_shape', 'granularity'])
+        seq = gen_partition_sequence(model.get_params('partition_sequence'), max_iterations)
+        if len(set(int(v) for v in seq)) != 1:
+            raise ValueError('the batched path needs one partition per scan (e.g. granularity=[K], '
+                             'partition_sequence=[0])')
+        part = gen_set_of_pixel_partitions(recon_shape, granularity, use_ror_mask=model.use_ror_mask,
+                                           rng=rng)[int(seq[0])]
+        # translation geometry has no direct recon (zeros, no draw); the others draw for its back projection
+        draws = 1 if model._kind() == _capi.MBX_GEOM_TRANSLATION else 2
+        for _ in range(draws):
+            gen_full_indices(recon_shape, use_ror_mask=model.use_ror_mask, rng=rng)
+        src = np.random if rng is None else rng
+        num_subsets = part.shape[0]
+        schedule = np.stack([src.permutation(num_subsets) for _ in range(max_iterations)])
+        part = morton_sorted_partition(part, recon_shape[1])  # spatially coherent processing order
+        sigma_y = float(model.get_params('sigma_y'))
+        b, sigma_x, p, q, T = model._qggmrf_params()
+        return reg, part, schedule, 1.0 / (sigma_y ** 2.0), _capi.qggmrf_params(b, sigma_x, p, q, T), sigma_y
+
     def _host_draws(self, max_iterations, small, small_w):
-        """Per scan, in the reference's np.random order: auto-regularisation (on the host subsamples), the
-        partition, the two region-of-reconstruction draws of the set-up (direct recon's back projection and the
-        initial forward projection), and the subset order of every iteration.  Returns (regularisation dicts,
-        Morton-sorted partitions, schedule (steps, scans), fm constants, qGGMRF records, sigma_y values)."""
-        regs, parts, schedules, fms, qps, sigmas = [], [], [], [], [], []
-        num_subsets = None
-        for i, model in enumerate(self.models):
-            if self.seeds is not None:
-                np.random.seed(int(self.seeds[i]))
-            regs.append(model.auto_set_regularization_params(small[i], weights=small_w[i]))
-            recon_shape, granularity = model.get_params(['recon_shape', 'granularity'])
-            seq = gen_partition_sequence(model.get_params('partition_sequence'), max_iterations)
-            if len(set(int(v) for v in seq)) != 1:
-                raise ValueError('the batched path needs one partition per scan (e.g. granularity=[K], '
-                                 'partition_sequence=[0])')
-            part = gen_set_of_pixel_partitions(recon_shape, granularity, use_ror_mask=model.use_ror_mask)[int(seq[0])]
-            if num_subsets is None:
-                num_subsets = part.shape[0]
-            elif part.shape[0] != num_subsets:
-                raise ValueError('all scans of a batch need the same number of subsets')
-            # the set-up's region-of-reconstruction draws: direct recon's back projection (none for translation
-            # geometry, whose direct recon is zeros) and the initial forward projection
+        """The host part of every scan (see _scan_draws).  With per-scan seeds each scan draws from its own
+        RandomState, which is the stream np.random.seed(seed) gives, so the scans run on a pool of host threads
+        (NumPy releases the GIL in the draws and sorts) and the global stream is left where the plain path leaves it,
+        after the last scan's draws.  Without seeds the scans draw from the global stream one after another.
+        Returns (regularisation dicts, partitions, schedule (steps, scans), fm constants, qGGMRF records, sigmas)."""
+        n = len(self.models)
+        for model in self.models:
             if model._kind() == _capi.MBX_GEOM_TRANSLATION:
                 warnings.warn('direct_recon not implemented for TomographyModel.')
-                draws = 1
-            else:
-                draws = 2
-            for _ in range(draws):
-                gen_full_indices(recon_shape, use_ror_mask=model.use_ror_mask)
-            schedules.append(np.stack([np.random.permutation(num_subsets) for _ in range(max_iterations)]))
-            parts.append(morton_sorted_partition(part, recon_shape[1]))  # spatially coherent processing order
-            sigma_y = float(model.get_params('sigma_y'))
-            b, sigma_x, p, q, T = model._qggmrf_params()
-            sigmas.append(sigma_y)
-            fms.append(1.0 / (sigma_y ** 2.0))
-            qps.append(_capi.qggmrf_params(b, sigma_x, p, q, T))
+        if self.seeds is None:
+            out = [self._scan_draws(i, max_iterations, small, small_w, None) for i in range(n)]
+        else:
+            rngs = [np.random.RandomState(int(sd)) for sd in self.seeds]
+            out = list(_draw_pool().map(
+                lambda i: self._scan_draws(i, max_iterations, small, small_w, rngs[i]), range(n)))
+            np.random.set_state(rngs[-1].get_state())
+        regs, parts, schedules, fms, qps, sigmas = (list(v) for v in zip(*out))
+        num_subsets = parts[0].shape[0]
+        if any(p.shape[0] != num_subsets for p in parts):
+            raise ValueError('all scans of a batch need the same number of subsets')
         # schedule[step, scan] with step = iteration * K + j
-        sched = np.stack(schedules, axis=-1).reshape(max_iterations * num_subsets, len(self.models))
+        sched = np.stack(schedules, axis=-1).reshape(max_iterations * num_subsets, n)
         return regs, parts, sched.astype(np.int32), fms, qps, sigmas
 
     # ---------------------------------------------------------------- reconstruction

@@ -23,8 +23,12 @@ def get_2d_ror_mask(recon_shape, *, crop_radius_pixels=0, crop_radius_fraction=0
     return cols[None, :] ** 2 + rows[:, None] ** 2 <= radius ** 2
 
 
-def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True):
-    """(num_subsets, ceil(N/num_subsets)) int32 array of sorted flat pixel indices (vcd_utils.py:176-223)."""
+def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True, rng=None):
+    """(num_subsets, ceil(N/num_subsets)) int32 array of sorted flat pixel indices (vcd_utils.py:176-223).
+
+    rng: a legacy np.random.RandomState to draw from instead of the global stream (np.random.seed(s) followed by
+    the global draws is the same stream as RandomState(s))."""
+    rng = np.random if rng is None else rng
     num_rows, num_cols = recon_shape[:2]
     indices = np.arange(num_rows * num_cols, dtype=np.int32)
     if use_ror_mask:
@@ -35,16 +39,16 @@ def gen_pixel_partition(recon_shape, num_subsets, use_ror_mask=True):
                       'reconstruction.  \nReducing the number of subsets to equal the number of indices.')
     per_subset = int(np.ceil(len(indices) / num_subsets))
     num_extra = num_subsets * per_subset - len(indices)
-    indices = np.random.permutation(indices)
+    indices = rng.permutation(indices)
     num_non_final = (num_subsets - 1) * per_subset
-    extra = np.random.choice(indices[:num_non_final], size=num_extra, replace=False)
+    extra = rng.choice(indices[:num_non_final], size=num_extra, replace=False)
     indices = np.concatenate((indices, extra)).reshape(num_subsets, -1)
     return np.sort(indices, axis=1).astype(np.int32)
 
 
-def gen_set_of_pixel_partitions(recon_shape, granularity, output_device=None, use_ror_mask=True):
+def gen_set_of_pixel_partitions(recon_shape, granularity, output_device=None, use_ror_mask=True, rng=None):
     """One partition per entry of granularity (vcd_utils.py:105-124); output_device is accepted and ignored."""
-    return [gen_pixel_partition(recon_shape, k, use_ror_mask=use_ror_mask) for k in granularity]
+    return [gen_pixel_partition(recon_shape, k, use_ror_mask=use_ror_mask, rng=rng) for k in granularity]
 
 
 def gen_partition_sequence(partition_sequence, max_iterations):
@@ -66,21 +70,26 @@ def _cache_put(cache, key, value):
     return value
 
 
-def gen_full_indices(recon_shape, use_ror_mask=True):
+def gen_full_indices(recon_shape, use_ror_mask=True, rng=None):
     """All pixels of the region of reconstruction, sorted (vcd_utils.py:310-318).
 
     The reference draws them as a one-subset partition: a permutation of the N pixels (and an empty choice) from
     the global np.random stream, then a sort, so the result is always the same sorted set while the stream
     advances by one permutation of N.  After the first call for a grid, this returns a copy of the kept set and
-    advances the stream by shuffling N scratch entries, which draws exactly what that permutation draws."""
+    advances the stream by shuffling N scratch entries, which draws exactly what that permutation draws.
+    rng: a legacy RandomState to draw from instead of the global stream (it shuffles scratch of its own, so calls
+    from several threads with their own streams share nothing but the read-only kept set)."""
     key = (int(recon_shape[0]), int(recon_shape[1]), bool(use_ror_mask))
     hit = _FULL_INDICES.get(key)
     if hit is None:
-        idx = gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask)[0]
+        idx = gen_pixel_partition(recon_shape, num_subsets=1, use_ror_mask=use_ror_mask, rng=rng)[0]
         _cache_put(_FULL_INDICES, key, (idx, np.empty(len(idx), dtype=np.int32)))
         return idx.copy()
     idx, scratch = hit
-    np.random.shuffle(scratch)
+    if rng is None:
+        np.random.shuffle(scratch)
+    else:
+        rng.shuffle(np.empty(len(idx), dtype=np.int32))
     return idx.copy()
 
 

@@ -346,3 +346,55 @@ def test_geometry_validation_as_the_reference():
     model = mb.ParallelBeamModel((8, 4, 16), np.zeros(8))
     with pytest.raises(ValueError, match='slices'):
         model.set_params(recon_shape=(16, 16, 5))
+
+
+def test_partition_draws_from_a_random_state_are_the_global_stream():
+    """np.random.seed(s) followed by the global draws is the stream RandomState(s): partitions and region-of-
+    reconstruction draws from an explicit RandomState equal the seeded global ones, and leave it in the same
+    state."""
+    shape = (37, 41, 3)
+    for seed in (0, 5):
+        np.random.seed(seed)
+        want = mb.gen_pixel_partition(shape, 4)
+        mb.gen_full_indices(shape)
+        mb.gen_full_indices(shape)
+        want_state = np.random.get_state()[1]
+        rs = np.random.RandomState(seed)
+        got = mb.gen_pixel_partition(shape, 4, rng=rs)
+        mb.gen_full_indices(shape, rng=rs)
+        mb.gen_full_indices(shape, rng=rs)
+        np.testing.assert_array_equal(got, want)
+        np.testing.assert_array_equal(rs.get_state()[1], want_state)
+
+
+def test_batched_host_draws_on_threads_match_the_sequential_stream():
+    """The batched path's host part with per-scan seeds (threads, one RandomState each) gives what the plain path
+    draws scan after scan from the seeded global stream, and leaves the global stream where the plain path does."""
+    from mbirjax_b200.batched import BatchedVCD, _view_subsample
+    from mbirjax_b200.vcd_utils import morton_sorted_partition
+    shapes = [(30, 6, 40), (24, 9, 36), (40, 4, 52)]
+    models, sinos = [], []
+    rng = np.random.default_rng(0)
+    for v, r, c in shapes:
+        m = mb.ParallelBeamModel((v, r, c), np.linspace(0, np.pi, v, endpoint=False).astype(np.float32))
+        m.set_params(sharpness=0.0, granularity=[4], partition_sequence=[0], verbose=0)
+        models.append(m)
+        sinos.append(rng.random((v, r, c)).astype(np.float32))
+    seeds = [3, 8, 5]
+    b = BatchedVCD(models, sinos, seeds=seeds)
+    small, small_w = b._host_subsamples()
+    regs, parts, sched, fms, qps, sigmas = b._host_draws(4, small, small_w)
+    end_state = np.random.get_state()[1].copy()
+    for i, (m, sd) in enumerate(zip(models, seeds)):
+        np.random.seed(sd)
+        reg = m.auto_set_regularization_params(_view_subsample(sinos[i]))
+        shape = m.get_params('recon_shape')
+        part = mb.gen_set_of_pixel_partitions(shape, [4])[0]
+        mb.gen_full_indices(shape)
+        mb.gen_full_indices(shape)
+        order = np.stack([np.random.permutation(4) for _ in range(4)])
+        assert reg == regs[i]
+        np.testing.assert_array_equal(parts[i], morton_sorted_partition(part, shape[1]))
+        np.testing.assert_array_equal(sched.reshape(4, 4, len(models))[:, :, i], order)
+        assert fms[i] == pytest.approx(1.0 / reg['sigma_y'] ** 2)
+    np.testing.assert_array_equal(np.random.get_state()[1], end_state)
