@@ -265,6 +265,17 @@ typedef struct mbx_batched_plan {
 /* Workspace for a batch with num_steps subset steps in its schedule (0 if the batch is not supported). */
 MBX_API size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps);
 
+/* Option of mbx_vcd_batched_prepare2: plan the subset forward projections.  Each subset is projected once per
+ * iteration, always onto the same (view, channel block) tiles; with this option mbx_vcd_batched_refresh scans and
+ * sorts every tile's pixels once per reconstruction and stores the sorted record passes in the workspace (about
+ * 17 bytes per pixel and view, 33 for cone and translation geometry), and every forward-projection stage replays
+ * them instead of scanning and sorting again.  Same results as without it. */
+#define MBX_BATCHED_PLAN_FORWARD 1
+
+/* mbx_vcd_batched_workspace_bytes / mbx_vcd_batched_prepare with options (MBX_BATCHED_PLAN_FORWARD). */
+MBX_API size_t mbx_vcd_batched_workspace_bytes2(const mbx_scan *scans, int32_t num_scans, int32_t num_steps,
+                                                int32_t flags);
+
 /* Validates the batch, lays out the workspace and uploads the per-scan argument records, the tile work lists
  * and the subset schedule (schedule[step * num_scans + scan] = subset index that scan updates at that step;
  * the reference draws it with np.random.permutation per iteration, tomography_model.py:1281).  step_stats
@@ -277,6 +288,10 @@ MBX_API int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans, co
                                     int32_t num_steps, int32_t num_iterations, double *step_stats,
                                     double *iter_stats, void *workspace, size_t workspace_bytes,
                                     mbx_batched_plan *plan_out, void *stream);
+MBX_API int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans, const int32_t *schedule,
+                                     int32_t num_steps, int32_t num_iterations, double *step_stats,
+                                     double *iter_stats, void *workspace, size_t workspace_bytes, int32_t flags,
+                                     mbx_batched_plan *plan_out, void *stream);
 
 /* One subset update for every scan of the batch: eight persistent launches, each walking the packed work list
  * of all scans (no host synchronisation; capturable in a CUDA graph).  Replaces one vcd_subset_updater call
@@ -315,7 +330,8 @@ MBX_API int mbx_vcd_batched_update(const mbx_batched_plan *plan, const mbx_scan 
                                    const int32_t *schedule, void *stream);
 
 /* Recomputes the chunk bounding boxes of every scan's subsets from the partition buffers, after the caller has
- * written new partitions into them (one launch; capturable). */
+ * written new partitions into them, and for a batch prepared with MBX_BATCHED_PLAN_FORWARD builds the planned
+ * forward projections of those subsets (no host synchronisation; capturable). */
 MBX_API int mbx_vcd_batched_refresh(const mbx_batched_plan *plan, void *stream);
 
 /* ---- FBP / FDK filtering ---------------------------------------------------------------------- */

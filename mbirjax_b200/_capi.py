@@ -89,6 +89,10 @@ _SIGNATURES = {
                                                c_size_t, c_void_p]),
     'mbx_median_filter3d': (ctypes.c_int, [c_void_p, c_int32, c_int32, c_int32, c_void_p, c_void_p]),
     'mbx_vcd_batched_workspace_bytes': (c_size_t, [ctypes.POINTER(MbxScan), c_int32, c_int32]),
+    'mbx_vcd_batched_workspace_bytes2': (c_size_t, [ctypes.POINTER(MbxScan), c_int32, c_int32, c_int32]),
+    'mbx_vcd_batched_prepare2': (ctypes.c_int, [ctypes.POINTER(MbxScan), c_int32, c_void_p, c_int32, c_int32,
+                                                c_void_p, c_void_p, c_void_p, c_size_t, c_int32,
+                                                ctypes.POINTER(MbxBatchedPlan), c_void_p]),
     'mbx_vcd_batched_prepare': (ctypes.c_int, [ctypes.POINTER(MbxScan), c_int32, c_void_p, c_int32, c_int32,
                                                c_void_p, c_void_p, c_void_p, c_size_t,
                                                ctypes.POINTER(MbxBatchedPlan), c_void_p]),
@@ -339,23 +343,33 @@ def direct_filter(geom, sinogram, out=None):
     return out
 
 
-def vcd_batched_prepare(scans, schedule, num_iterations, step_stats, iter_stats, device):
-    """scans: list of MbxScan; schedule: int32 numpy (num_steps, num_scans).  Returns (plan, workspace)."""
+MBX_BATCHED_PLAN_FORWARD = 1
+
+
+def vcd_batched_workspace_bytes(scans, num_steps, flags=0):
+    n = len(scans)
+    arr = (MbxScan * n)(*scans)
+    return int(load_library().mbx_vcd_batched_workspace_bytes2(arr, n, int(num_steps), int(flags)))
+
+
+def vcd_batched_prepare(scans, schedule, num_iterations, step_stats, iter_stats, device, flags=0):
+    """scans: list of MbxScan; schedule: int32 numpy (num_steps, num_scans); flags: MBX_BATCHED_PLAN_FORWARD or 0.
+    Returns (plan, workspace)."""
     import numpy as np
     lib = load_library()
     n = len(scans)
     arr = (MbxScan * n)(*scans)
     sched = np.ascontiguousarray(schedule, dtype=np.int32)
     num_steps = int(sched.shape[0])
-    nbytes = lib.mbx_vcd_batched_workspace_bytes(arr, n, num_steps)
+    nbytes = lib.mbx_vcd_batched_workspace_bytes2(arr, n, num_steps, int(flags))
     if nbytes == 0:
         raise MbxError('mbx_vcd_batched_workspace_bytes: batch not supported (mixed geometry kinds, psf radius '
                        'other than 1, or invalid scans)')
     ws = torch.empty(int(nbytes), dtype=torch.uint8, device=device)
     plan = MbxBatchedPlan()
-    rc = lib.mbx_vcd_batched_prepare(arr, n, sched.ctypes.data_as(c_void_p), num_steps, int(num_iterations),
-                                     _ptr(step_stats), _ptr(iter_stats), _ptr(ws), int(nbytes), ctypes.byref(plan),
-                                     _stream())
+    rc = lib.mbx_vcd_batched_prepare2(arr, n, sched.ctypes.data_as(c_void_p), num_steps, int(num_iterations),
+                                      _ptr(step_stats), _ptr(iter_stats), _ptr(ws), int(nbytes), int(flags),
+                                      ctypes.byref(plan), _stream())
     _check(rc, 'mbx_vcd_batched_prepare')
     return plan, ws
 

@@ -32,6 +32,8 @@ __all__ = ['BatchedVCD', 'release_batched_sessions', 'morton_order']
 
 _SESSIONS = collections.OrderedDict()  # batch key -> _Session, most recently used last
 _MAX_SESSIONS = 2
+PLAN_FORWARD = True               # plan the subset forward projections of a batch when it fits (see _Session)
+PLAN_FORWARD_MAX_FRACTION = 0.5   # of the free device memory the plan's workspace may take
 
 
 _POOL = None
@@ -273,8 +275,17 @@ class _Session:
         self.iter_stats = torch.zeros((max_iterations, n, 4), dtype=torch.float64, device=dev)
         # pinned staging of the per-call partitions
         self.part_host = [torch.empty(tuple(p.shape), dtype=torch.int32).pin_memory() for p in self.part]
+        # planned forward projections (each subset's sorted record passes, built once per reconstruction and
+        # replayed by every iteration) when their storage leaves most of the device free
+        flags = _capi.MBX_BATCHED_PLAN_FORWARD if PLAN_FORWARD else 0
+        if flags:
+            need = _capi.vcd_batched_workspace_bytes(scans, sched.shape[0], flags)
+            free = torch.cuda.mem_get_info(dev)[0]
+            if need == 0 or need > PLAN_FORWARD_MAX_FRACTION * free:
+                flags = 0
+        self.planned_forward = bool(flags)
         self.plan, self.workspace = _capi.vcd_batched_prepare(scans, sched, max_iterations, self.step_stats,
-                                                              self.iter_stats, dev)
+                                                              self.iter_stats, dev, flags)
         self.setup_graph = None
         self.iter_graph = None
 

@@ -648,8 +648,35 @@ __device__ __forceinline__ void cb_accumulate_par(const FpArgs &A, const CbPass 
     }
 }
 
-template <int KIND, int MINB>
-__device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) {
+// Modes of a channel-block tile: scan, sort and walk its pixels (the forward projection); build, which scans and
+// sorts them and stores the sorted record passes in a CbPlanned list instead of walking them; replay, which walks
+// the stored passes (no scan, no sort).  A planned list is built once for a pixel list and replayed as often as
+// the same list is projected again with new voxel values (every iteration of a VCD reconstruction).
+enum { CB_WALK = 0, CB_BUILD = 1, CB_REPLAY = 2 };
+constexpr int CB_MAX_PASSES = 64;  // passes of one tile a planned list can hold (more: the tile is not planned)
+
+// Stored sorted record passes of every tile of one pixel list (device storage carved by the caller).  Records and
+// pass slots are taken from bump cursors (reset before a build), so their placement depends on scheduling, but
+// each tile replays its own passes in order: the result is deterministic.  A tile whose passes did not fit has
+// tile_npass = -1 and must be projected by the walk instead.
+struct CbPlanned {
+    float4 *rec;                      // [rec_cap] sorted records of every pass
+    float4 *rec2;                     // [rec_cap] second record word (cone / translation) or NULL
+    uint8_t *sbin;                    // [rec_cap] bin of each record
+    unsigned long long *rec_cursor;   // next free record
+    int *pass_cursor;                 // next free pass slot
+    long long *pass_rec;              // [pass_cap] first record of each pass
+    int *pass_count;                  // [pass_cap] records of each pass
+    int *pass_bstart;                 // [pass_cap][nbins + 1] bin starts of each pass
+    int *tile_npass;                  // [tiles] passes of each tile (-1: not planned)
+    int *tile_pass;                   // [tiles][CB_MAX_PASSES] pass slots of each tile
+    long long rec_cap;
+    int pass_cap;
+};
+
+template <int KIND, int MINB, int MODE = CB_WALK>
+__device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, const CbPlanned *PL = nullptr,
+                           long long ptile = 0) {
     const mbx_geom &g = A.g;
     const CbPlan &pl = A.plan;
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
@@ -710,13 +737,117 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
         }
     }
 
+    // phase 3 of a pass whose sorted records (rec, rec2, sbin) and bin starts (bstart) are in shared memory
+    auto walk = [&]() {
+        // ---- 3. warp ranges of bins with about equal record counts, at least two bins each:
+        //         B_v = 2v + max_{u<=v}(lb_u - 2u), then B_v <= nbins - 2(8 - v); lb_v = first bin starting at or
+        //         after v/8 of the records
+        CbPass P;
+        {
+            const int tot = bstart[nbins];
+            int lb = 0;
+            if (lane <= CB_WARPS) {
+                const int target = (int)(((long long)lane * tot) / CB_WARPS);
+                int lo = 0, hi = nbins;
+                while (lo < hi) {
+                    const int mid = (lo + hi) >> 1;
+                    if (bstart[mid] >= target)
+                        hi = mid;
+                    else
+                        lo = mid + 1;
+                }
+                lb = lo;
+            }
+            int t = (lane <= CB_WARPS) ? lb - 2 * lane : INT_MIN / 2;
+    #pragma unroll
+            for (int off = 1; off < 32; off <<= 1) {
+                const int u = __shfl_up_sync(0xffffffffu, t, off);
+                if (lane >= off) t = max(t, u);
+            }
+            int bv = min(2 * lane + t, nbins - 2 * (CB_WARPS - lane));
+            if (lane == CB_WARPS) bv = nbins;
+            P.b_lo = __shfl_sync(0xffffffffu, bv, warp);
+            P.b_hi = __shfl_sync(0xffffffffu, bv, warp + 1);
+        }
+        P.rec = rec;
+        P.rec2 = rec2;
+        P.sbin = sbin;
+        P.bstart = bstart;
+        P.tile = tile;
+        P.s_vm = s_vm;
+        P.s_vb = s_vb;
+        P.s_b0 = s_b0;
+        if (KIND == MBX_GEOM_PARALLEL) {
+            switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
+                case 9: cb_accumulate_par<1, 1, MINB>(A, P, warp, lane); break;
+                case 10: cb_accumulate_par<1, 2, MINB>(A, P, warp, lane); break;
+                case 11: cb_accumulate_par<1, 3, MINB>(A, P, warp, lane); break;
+                case 12: cb_accumulate_par<1, 4, MINB>(A, P, warp, lane); break;
+                case 17: cb_accumulate_par<2, 1, MINB>(A, P, warp, lane); break;
+                case 18: cb_accumulate_par<2, 2, MINB>(A, P, warp, lane); break;
+                case 19: cb_accumulate_par<2, 3, MINB>(A, P, warp, lane); break;
+                case 20: cb_accumulate_par<2, 4, MINB>(A, P, warp, lane); break;
+                case 33: cb_accumulate_par<4, 1, MINB>(A, P, warp, lane); break;
+                case 34: cb_accumulate_par<4, 2, MINB>(A, P, warp, lane); break;
+                case 35: cb_accumulate_par<4, 3, MINB>(A, P, warp, lane); break;
+                default: cb_accumulate_par<4, 4, MINB>(A, P, warp, lane); break;
+            }
+        } else switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
+            case 9: cb_accumulate<KIND, 1, 1>(A, P, warp, lane, kconst); break;
+            case 10: cb_accumulate<KIND, 1, 2>(A, P, warp, lane, kconst); break;
+            case 11: cb_accumulate<KIND, 1, 3>(A, P, warp, lane, kconst); break;
+            case 12: cb_accumulate<KIND, 1, 4>(A, P, warp, lane, kconst); break;
+            case 17: cb_accumulate<KIND, 2, 1>(A, P, warp, lane, kconst); break;
+            case 18: cb_accumulate<KIND, 2, 2>(A, P, warp, lane, kconst); break;
+            case 19: cb_accumulate<KIND, 2, 3>(A, P, warp, lane, kconst); break;
+            case 20: cb_accumulate<KIND, 2, 4>(A, P, warp, lane, kconst); break;
+            case 33: cb_accumulate<KIND, 4, 1>(A, P, warp, lane, kconst); break;
+            case 34: cb_accumulate<KIND, 4, 2>(A, P, warp, lane, kconst); break;
+            case 35: cb_accumulate<KIND, 4, 3>(A, P, warp, lane, kconst); break;
+            default: cb_accumulate<KIND, 4, 4>(A, P, warp, lane, kconst); break;
+        }
+    };
+
+    if (MODE == CB_REPLAY) {  // the stored passes of this tile, walked in order
+        const int npass = min(PL->tile_npass[ptile], CB_MAX_PASSES);
+        for (int q = 0; q < npass; ++q) {
+            // every value below is read by all threads from one address, so the skips are uniform
+            const int ps = PL->tile_pass[ptile * CB_MAX_PASSES + q];
+            if (ps < 0 || ps >= PL->pass_cap) {  // never written by a build: skip, and say so
+                if (tid == 0) flag_error(err, MBX_ERRFLAG_CACHE);
+                continue;
+            }
+            const int count = PL->pass_count[ps];
+            const long long rs = PL->pass_rec[ps];
+            if (count < 0 || count > pl.cap || rs < 0 || rs + count > PL->rec_cap) {
+                if (tid == 0) flag_error(err, MBX_ERRFLAG_CACHE);
+                continue;
+            }
+            __syncthreads();  // the previous pass is done with every list
+            for (int b = tid; b <= nbins; b += CB_THREADS) bstart[b] = PL->pass_bstart[(long long)ps * (nbins + 1) + b];
+            for (int i = tid; i < count; i += CB_THREADS) {
+                rec[i] = PL->rec[rs + i];
+                if (KIND != MBX_GEOM_PARALLEL) rec2[i] = PL->rec2[rs + i];
+                sbin[i] = PL->sbin[rs + i];
+            }
+            if (tid < CB_PAD) {  // padding read (never used) by the walk past the last record
+                rec[count + tid] = make_float4(0.f, 0.f, 0.f, 0.f);
+                sbin[count + tid] = nbins - 1;
+            }
+            __syncthreads();
+            walk();
+        }
+    }
+    bool build_ok = true;  // build: every pass so far found room in the planned list
+    int build_np = 0;      // build: passes stored so far
+
     const int npix_grid = g.num_recon_rows * g.num_recon_cols;
     const long long num_pixels = view_ok ? A.num_pixels : 0;
     const long long nchunks = (num_pixels + CB_CHUNK - 1) / CB_CHUNK;
     long long seg = 0;    // first chunk of the next segment of CB_THREADS chunks to test
     int nh = 0, hp = 0;   // chunks of the current segment that can reach the block (in hl), next one to scan
     int idx_next = -1;    // prefetched pixel index of entry tid of chunk hl[hp]
-    bool more = num_pixels > 0;
+    bool more = MODE != CB_REPLAY && num_pixels > 0;
 
     while (more) {
         __syncthreads();  // the previous pass is done with every list
@@ -870,73 +1001,45 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err) 
             sbin[count + tid] = nbins - 1;
         }
         __syncthreads();
-        // ---- 3. warp ranges of bins with about equal record counts, at least two bins each:
-        //         B_v = 2v + max_{u<=v}(lb_u - 2u), then B_v <= nbins - 2(8 - v); lb_v = first bin starting at or
-        //         after v/8 of the records
-        CbPass P;
-        {
-            const int tot = bstart[nbins];
-            int lb = 0;
-            if (lane <= CB_WARPS) {
-                const int target = (int)(((long long)lane * tot) / CB_WARPS);
-                int lo = 0, hi = nbins;
-                while (lo < hi) {
-                    const int mid = (lo + hi) >> 1;
-                    if (bstart[mid] >= target)
-                        hi = mid;
-                    else
-                        lo = mid + 1;
+        if (MODE == CB_BUILD) {  // store the pass instead of walking it
+            __shared__ long long s_rs;
+            __shared__ int s_ps;
+            if (tid == 0) {
+                long long rsv = -1;
+                int psv = -1;
+                if (build_ok && build_np < CB_MAX_PASSES) {
+                    rsv = (long long)atomicAdd(PL->rec_cursor, (unsigned long long)count);
+                    psv = atomicAdd(PL->pass_cursor, 1);
+                    if (rsv + count > PL->rec_cap || psv >= PL->pass_cap) rsv = -1;
                 }
-                lb = lo;
+                s_rs = rsv;
+                s_ps = psv;
             }
-            int t = (lane <= CB_WARPS) ? lb - 2 * lane : INT_MIN / 2;
-#pragma unroll
-            for (int off = 1; off < 32; off <<= 1) {
-                const int u = __shfl_up_sync(0xffffffffu, t, off);
-                if (lane >= off) t = max(t, u);
+            __syncthreads();
+            const long long rsv = s_rs;
+            const int psv = s_ps;
+            if (rsv < 0) build_ok = false;
+            if (build_ok) {
+                for (int i = tid; i < count; i += CB_THREADS) {
+                    PL->rec[rsv + i] = rec[i];
+                    if (KIND != MBX_GEOM_PARALLEL) PL->rec2[rsv + i] = rec2[i];
+                    PL->sbin[rsv + i] = (uint8_t)sbin[i];
+                }
+                for (int b = tid; b <= nbins; b += CB_THREADS) PL->pass_bstart[(long long)psv * (nbins + 1) + b] = bstart[b];
+                if (tid == 0) {
+                    PL->pass_rec[psv] = rsv;
+                    PL->pass_count[psv] = count;
+                    PL->tile_pass[ptile * CB_MAX_PASSES + build_np] = psv;
+                }
             }
-            int bv = min(2 * lane + t, nbins - 2 * (CB_WARPS - lane));
-            if (lane == CB_WARPS) bv = nbins;
-            P.b_lo = __shfl_sync(0xffffffffu, bv, warp);
-            P.b_hi = __shfl_sync(0xffffffffu, bv, warp + 1);
+            ++build_np;
+        } else {
+            walk();
         }
-        P.rec = rec;
-        P.rec2 = rec2;
-        P.sbin = sbin;
-        P.bstart = bstart;
-        P.tile = tile;
-        P.s_vm = s_vm;
-        P.s_vb = s_vb;
-        P.s_b0 = s_b0;
-        if (KIND == MBX_GEOM_PARALLEL) {
-            switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
-                case 9: cb_accumulate_par<1, 1, MINB>(A, P, warp, lane); break;
-                case 10: cb_accumulate_par<1, 2, MINB>(A, P, warp, lane); break;
-                case 11: cb_accumulate_par<1, 3, MINB>(A, P, warp, lane); break;
-                case 12: cb_accumulate_par<1, 4, MINB>(A, P, warp, lane); break;
-                case 17: cb_accumulate_par<2, 1, MINB>(A, P, warp, lane); break;
-                case 18: cb_accumulate_par<2, 2, MINB>(A, P, warp, lane); break;
-                case 19: cb_accumulate_par<2, 3, MINB>(A, P, warp, lane); break;
-                case 20: cb_accumulate_par<2, 4, MINB>(A, P, warp, lane); break;
-                case 33: cb_accumulate_par<4, 1, MINB>(A, P, warp, lane); break;
-                case 34: cb_accumulate_par<4, 2, MINB>(A, P, warp, lane); break;
-                case 35: cb_accumulate_par<4, 3, MINB>(A, P, warp, lane); break;
-                default: cb_accumulate_par<4, 4, MINB>(A, P, warp, lane); break;
-            }
-        } else switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
-            case 9: cb_accumulate<KIND, 1, 1>(A, P, warp, lane, kconst); break;
-            case 10: cb_accumulate<KIND, 1, 2>(A, P, warp, lane, kconst); break;
-            case 11: cb_accumulate<KIND, 1, 3>(A, P, warp, lane, kconst); break;
-            case 12: cb_accumulate<KIND, 1, 4>(A, P, warp, lane, kconst); break;
-            case 17: cb_accumulate<KIND, 2, 1>(A, P, warp, lane, kconst); break;
-            case 18: cb_accumulate<KIND, 2, 2>(A, P, warp, lane, kconst); break;
-            case 19: cb_accumulate<KIND, 2, 3>(A, P, warp, lane, kconst); break;
-            case 20: cb_accumulate<KIND, 2, 4>(A, P, warp, lane, kconst); break;
-            case 33: cb_accumulate<KIND, 4, 1>(A, P, warp, lane, kconst); break;
-            case 34: cb_accumulate<KIND, 4, 2>(A, P, warp, lane, kconst); break;
-            case 35: cb_accumulate<KIND, 4, 3>(A, P, warp, lane, kconst); break;
-            default: cb_accumulate<KIND, 4, 4>(A, P, warp, lane, kconst); break;
-        }
+    }
+    if (MODE == CB_BUILD) {
+        if (tid == 0) PL->tile_npass[ptile] = build_ok ? build_np : -1;
+        return;
     }
     __syncthreads();
     // ---- 4. fixed-order sum of the sub-group copies, coalesced write

@@ -75,10 +75,12 @@ struct ProjList {
     const int *schedule;   // [num_steps][num_scans] record of each scan at each step, or NULL (record 0)
     int stride;            // records per scan
     int *counter;          // next tile (reset by a memset before each launch)
+    const CbPlanned *planned;  // forward lists: stored record passes of each record, or NULL (walk every tile)
 };
 
-// Projection work lists of a batch.
-enum { PL_BP = 0, PL_FP, PL_INIT_BP, PL_INIT_FP, PL_HESS, PL_COUNT };
+// Projection work lists of a batch.  PL_BUILD covers every (scan, subset, view, channel block) tile: the builds
+// of the planned forward projections.
+enum { PL_BP = 0, PL_FP, PL_INIT_BP, PL_INIT_FP, PL_HESS, PL_BUILD, PL_COUNT };
 
 struct BatchedTables {
     VcdScan *scans;
@@ -90,6 +92,7 @@ struct BatchedTables {
     FpArgs *init_fp;    // [scan]: recon -> dsino over the region of reconstruction
     BpArgs *hess_bp;    // [scan]: weights (or ones) -> Hessian over every pixel, squared coefficients
     FiltScan *filt;     // [scan]
+    CbPlanned *planned; // [scan][subset] stored record passes of the subset forward projections (planned batches)
     int *pl_off;        // [PL_COUNT][num_scans + 1]
     int *pl_dim;        // [PL_COUNT][num_scans]
     int *pl_order;      // [PL_COUNT][num_scans]
@@ -107,6 +110,10 @@ struct BatchedTables {
 struct BatchedPlanHost {
     BatchedTables t;
     int num_scans, kind, num_steps, num_iterations, ksum, has_setup;
+    int planned_fp;                 // subset forward projections replay stored record passes
+    int pl_grid_replay, pl_grid_build;  // grids of the replay and build kernels (variant fp_minb)
+    void *plan_cursors;             // [ksum] bump cursors of the planned lists (one memset resets them)
+    size_t plan_cursor_bytes;
     int pl_total[PL_COUNT], pl_grid[PL_COUNT];
     size_t pl_smem[PL_COUNT];
     int el_total, sn_total, rc_total, flt_total, box_total;
@@ -129,6 +136,7 @@ static ProjList proj_list(const BatchedTables &T, int which, int num_scans) {
     L.schedule = subsets ? T.schedule : nullptr;
     L.stride = 0;  // set by the caller (the number of subsets for the subset lists)
     L.counter = T.counters + which;
+    L.planned = nullptr;
     return L;
 }
 
@@ -205,6 +213,45 @@ __global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(ProjList L, int num_sca
         const int local = t - __ldg(L.off + k);
         const int cbs = __ldg(L.dim + s);
         fp_cb_tile<KIND, MINB>(list_record(L.fp, L, num_scans, step, s), local / cbs, local % cbs, smf2, err);
+    }
+}
+
+// Subset forward projection from stored record passes: the tile's passes are walked as stored (no scan, no
+// sort); a tile the build could not store is projected by the walk.
+template <int KIND, int MINB>
+__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp_replay(ProjList L, int num_scans, int step, int first, int total, int *err) {
+    extern __shared__ __align__(16) float smf3[];
+    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
+        const int k = find_scan(L.off, num_scans, t);
+        const int s = __ldg(L.order + k);
+        const int local = t - __ldg(L.off + k);
+        const int cbs = __ldg(L.dim + s);
+        const int r = L.schedule ? __ldg(L.schedule + step * num_scans + s) : 0;
+        const FpArgs &A = L.fp[s * L.stride + r];
+        const CbPlanned &pc = L.planned[s * L.stride + r];
+        const int view = local / cbs, cb = local % cbs;
+        const long long ptile = local;  // view * cbs + cb
+        if (pc.tile_npass[ptile] >= 0)
+            fp_cb_tile<KIND, MINB, CB_REPLAY>(A, view, cb, smf3, err, &pc, ptile);
+        else
+            fp_cb_tile<KIND, MINB, CB_WALK>(A, view, cb, smf3, err);
+    }
+}
+
+// Builds of the planned forward projections: every (scan, subset, view, channel block) tile scans and sorts its
+// pixels and stores the sorted passes.
+template <int KIND, int MINB>
+__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp_build(ProjList L, int num_scans, int first, int total, int *err) {
+    extern __shared__ __align__(16) float smf4[];
+    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
+        const int k = find_scan(L.off, num_scans, t);
+        const int s = __ldg(L.order + k);
+        const int local = t - __ldg(L.off + k);
+        const int cbs = __ldg(L.dim + s);
+        const int per_subset = L.fp[s * L.stride].num_views_sel * cbs;
+        const int sub = local / per_subset, r = local - sub * per_subset;
+        fp_cb_tile<KIND, MINB, CB_BUILD>(L.fp[s * L.stride + sub], r / cbs, r % cbs, smf4, err,
+                                         L.planned + s * L.stride + sub, r);
     }
 }
 
@@ -539,7 +586,8 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
 
 // Tiles of scan s in a projection work list, the list's per-scan dimension (gx or channel blocks) and the cost
 // of one of its tiles (to order the list: most expensive tiles first).
-static void list_dims(int which, const mbx_scan &sc, const ScanSizes &z, int &tiles, int &dim, double &cost) {
+static void list_dims(int which, const mbx_scan &sc, const ScanSizes &z, int &tiles, int &dim, double &cost,
+                      bool planned = false) {
     const mbx_geom &g = sc.geom;
     auto bp_cost = [&](const BpfPlan &b) {
         return (double)g.num_views * std::min(g.num_recon_slices, b.ts * b.nsl) * 32.0 * b.npg;
@@ -560,13 +608,51 @@ static void list_dims(int which, const mbx_scan &sc, const ScanSizes &z, int &ti
             dim = z.fpp.cblocks;
             cost = fp_cost(sc.num_full_indices);
             break;
+        case PL_BUILD:
+            tiles = planned ? sc.num_subsets * g.num_views * z.fpp.cblocks : 0;
+            dim = z.fpp.cblocks;
+            cost = fp_cost(sc.subset_size);
+            break;
         default: tiles = z.setup ? z.hbp.gx * z.hbp.gy : 0; dim = z.hbp.gx; cost = bp_cost(z.hbp); break;
     }
 }
 
+// Storage of the planned forward projection of one (scan, subset) pixel list: records for about every pixel in
+// every view plus the pixels shared by neighbouring channel blocks (a tile whose passes find no room is walked
+// instead), pass slots for the most passes the records can need (every pass but a tile's last holds more than
+// 256 records), and per-tile pass tables.
+struct PlannedSizes {
+    long long rec_cap;
+    int pass_cap, tiles, nbins;
+    size_t rec, rec2, sbin, pass_rec, pass_count, pass_bstart, tile_npass, tile_pass, total;
+};
+
+static PlannedSizes planned_sizes(const mbx_scan &sc, const ScanSizes &z) {
+    PlannedSizes q;
+    const mbx_geom &g = sc.geom;
+    q.tiles = g.num_views * z.fpp.cblocks;
+    q.nbins = z.fpp.nbins;
+    q.rec_cap = (long long)std::ceil(1.06 * g.num_views * (double)sc.subset_size) + 16LL * q.tiles;
+    q.pass_cap = (int)(q.rec_cap / 257 + q.tiles + 1);
+    size_t off = 0;
+    auto take = [&](size_t bytes) { size_t o = off; off += align256(bytes); return o; };
+    q.rec = take(sizeof(float4) * (size_t)q.rec_cap);
+    q.rec2 = take(g.kind != MBX_GEOM_PARALLEL ? sizeof(float4) * (size_t)q.rec_cap : 0);
+    q.sbin = take((size_t)q.rec_cap);
+    q.pass_rec = take(sizeof(long long) * (size_t)q.pass_cap);
+    q.pass_count = take(sizeof(int) * (size_t)q.pass_cap);
+    q.pass_bstart = take(sizeof(int) * (size_t)q.pass_cap * (q.nbins + 1));
+    q.tile_npass = take(sizeof(int) * (size_t)q.tiles);
+    q.tile_pass = take(sizeof(int) * (size_t)q.tiles * CB_MAX_PASSES);
+    q.total = off;
+    return q;
+}
+
 struct Layout {
-    size_t scans, fm, qp, bpargs, fpargs, ibp, ifp, hbp, filt, pl_off, pl_dim, pl_order, offs, box_first, counters,
-        sched, p_prior, p_fwd, p_l1, p_iter, p_init, alpha, alpha_init, arange, total;
+    size_t scans, fm, qp, bpargs, fpargs, ibp, ifp, hbp, filt, planned, pl_off, pl_dim, pl_order, offs, box_first,
+        counters, sched, p_prior, p_fwd, p_l1, p_iter, p_init, alpha, alpha_init, arange, cursors, total;
+    bool plan_fp;
+    std::vector<size_t> plan_off;  // per scan: its subsets' planned storage, [K][PlannedSizes::total]
     int pl_total[PL_COUNT];
     int el_total, sn_total, rc_total, flt_total, box_total, ksum, max_npix;
     bool setup;
@@ -575,7 +661,9 @@ struct Layout {
     std::vector<size_t> fbox_off;  // per scan: chunk boxes of its region-of-reconstruction list
 };
 
-static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::vector<ScanSizes> &zs) {
+static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::vector<ScanSizes> &zs,
+                  int flags = 0) {
+    L.plan_fp = (flags & MBX_BATCHED_PLAN_FORWARD) != 0;
     zs.resize(n);
     for (int w = 0; w < PL_COUNT; ++w) L.pl_total[w] = 0;
     L.el_total = L.sn_total = L.rc_total = L.flt_total = L.box_total = L.ksum = L.max_npix = 0;
@@ -589,7 +677,7 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
         for (int w = 0; w < PL_COUNT; ++w) {
             int tiles, dim;
             double cost;
-            list_dims(w, scans[s], zs[s], tiles, dim, cost);
+            list_dims(w, scans[s], zs[s], tiles, dim, cost, L.plan_fp);
             L.pl_total[w] += tiles;
         }
         L.el_total += zs[s].el_tiles;
@@ -614,6 +702,7 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
     L.ifp = take(sizeof(FpArgs) * n);
     L.hbp = take(sizeof(BpArgs) * n);
     L.filt = take(sizeof(FiltScan) * n);
+    L.planned = take(L.plan_fp ? sizeof(CbPlanned) * L.ksum : 0);
     L.pl_off = take(sizeof(int) * PL_COUNT * (n + 1));
     L.pl_dim = take(sizeof(int) * PL_COUNT * n);
     L.pl_order = take(sizeof(int) * PL_COUNT * n);
@@ -629,6 +718,7 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
     L.alpha = take(sizeof(float) * n);
     L.alpha_init = take(sizeof(float) * n);
     L.arange = take(L.setup ? sizeof(int32_t) * (size_t)L.max_npix : 0);
+    L.cursors = take(L.plan_fp ? 16 * (size_t)L.ksum : 0);  // {unsigned long long records, int passes, pad}
     L.buf_off.resize(3 * (size_t)n);
     for (int s = 0; s < n; ++s) {
         L.buf_off[3 * s] = take(4 * (size_t)zs[s].ncyl);
@@ -641,6 +731,9 @@ static int layout(const mbx_scan *scans, int n, int num_steps, Layout &L, std::v
         L.box_off[s] = take((size_t)scans[s].num_subsets * fp_chunk_box_bytes(scans[s].subset_size));
         if (L.setup) L.fbox_off[s] = take(fp_chunk_box_bytes(scans[s].num_full_indices));
     }
+    L.plan_off.assign(n, 0);
+    for (int s = 0; s < n && L.plan_fp; ++s)
+        L.plan_off[s] = take((size_t)scans[s].num_subsets * planned_sizes(scans[s], zs[s]).total);
     L.total = off;
     return MBX_OK;
 }
@@ -663,7 +756,21 @@ static const void *bp_kernel_of(int kind) {
                                      : reinterpret_cast<const void *>(b_bp<MBX_GEOM_TRANSLATION>);
 }
 
-static const void *fp_kernel_of(int kind, int minb) {
+// The forward stage kernels: mode CB_WALK (b_fp), CB_REPLAY (b_fp_replay) or CB_BUILD (b_fp_build).
+template <int KIND>
+static const void *fp_kernel_mode(int minb, int mode) {
+    if (mode == CB_REPLAY)
+        return minb >= 3 ? reinterpret_cast<const void *>(b_fp_replay<KIND, 3>)
+                         : reinterpret_cast<const void *>(b_fp_replay<KIND, 2>);
+    return minb >= 3 ? reinterpret_cast<const void *>(b_fp_build<KIND, 3>)
+                     : reinterpret_cast<const void *>(b_fp_build<KIND, 2>);
+}
+
+static const void *fp_kernel_of(int kind, int minb, int mode = CB_WALK) {
+    if (mode != CB_WALK)
+        return kind == MBX_GEOM_PARALLEL ? fp_kernel_mode<MBX_GEOM_PARALLEL>(minb, mode)
+               : kind == MBX_GEOM_CONE   ? fp_kernel_mode<MBX_GEOM_CONE>(minb, mode)
+                                         : fp_kernel_mode<MBX_GEOM_TRANSLATION>(minb, mode);
     if (minb >= 3)
         return kind == MBX_GEOM_PARALLEL ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>)
                : kind == MBX_GEOM_CONE   ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>)
@@ -677,8 +784,8 @@ static int bp_grid(int kind, size_t smem, int total) {
     return occupancy_grid(bp_kernel_of(kind), BPF_THREADS, smem, total);
 }
 
-static int fp_grid(int kind, int minb, size_t smem, int total) {
-    return occupancy_grid(fp_kernel_of(kind, minb), CB_THREADS, smem, total);
+static int fp_grid(int kind, int minb, size_t smem, int total, int mode = CB_WALK) {
+    return occupancy_grid(fp_kernel_of(kind, minb, mode), CB_THREADS, smem, total);
 }
 
 // One launch of a back-projection work list over tiles [first, total) (resets the list's counter first).
@@ -700,29 +807,42 @@ static cudaError_t launch_bp_list(const BatchedPlanHost &P, int which, int step,
 }
 
 // One launch of a forward-projection work list (kernel variant for minb resident CTAs per SM).
+template <int KIND, int MINB>
+static void launch_fp_kernel(int mode, int grid, size_t smem, cudaStream_t st, const ProjList &L, int n, int step,
+                             int first, int total, int *err) {
+    if (mode == CB_REPLAY)
+        b_fp_replay<KIND, MINB><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+    else if (mode == CB_BUILD)
+        b_fp_build<KIND, MINB><<<grid, CB_THREADS, smem, st>>>(L, n, first, total, err);
+    else
+        b_fp<KIND, MINB><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+}
+
+// One launch of a forward-projection work list (kernel variant for minb resident CTAs per SM): the walk
+// (mode CB_WALK), the replay of planned passes (CB_REPLAY, subset list) or their build (CB_BUILD, PL_BUILD).
 static cudaError_t launch_fp_list(const BatchedPlanHost &P, int which, int minb, int step, int first, int total,
-                                  int grid, size_t smem, cudaStream_t st) {
+                                  int grid, size_t smem, cudaStream_t st, int mode = CB_WALK) {
     ProjList L = proj_list(P.t, which, P.num_scans);
-    L.stride = which == PL_FP ? P.ksum / P.num_scans : 1;
+    const bool subsets = which == PL_FP || which == PL_BUILD;
+    L.stride = subsets ? P.ksum / P.num_scans : 1;
+    if (which == PL_BUILD) {
+        L.fp = P.t.fpargs;
+        L.schedule = nullptr;
+    }
+    if (mode != CB_WALK) L.planned = P.t.planned;
     cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     int *err = device_error_ptr();
     const int n = P.num_scans;
     if (P.kind == MBX_GEOM_PARALLEL) {
-        if (minb >= 3)
-            b_fp<MBX_GEOM_PARALLEL, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
-        else
-            b_fp<MBX_GEOM_PARALLEL, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+        if (minb >= 3) launch_fp_kernel<MBX_GEOM_PARALLEL, 3>(mode, grid, smem, st, L, n, step, first, total, err);
+        else launch_fp_kernel<MBX_GEOM_PARALLEL, 2>(mode, grid, smem, st, L, n, step, first, total, err);
     } else if (P.kind == MBX_GEOM_CONE) {
-        if (minb >= 3)
-            b_fp<MBX_GEOM_CONE, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
-        else
-            b_fp<MBX_GEOM_CONE, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+        if (minb >= 3) launch_fp_kernel<MBX_GEOM_CONE, 3>(mode, grid, smem, st, L, n, step, first, total, err);
+        else launch_fp_kernel<MBX_GEOM_CONE, 2>(mode, grid, smem, st, L, n, step, first, total, err);
     } else {
-        if (minb >= 3)
-            b_fp<MBX_GEOM_TRANSLATION, 3><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
-        else
-            b_fp<MBX_GEOM_TRANSLATION, 2><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
+        if (minb >= 3) launch_fp_kernel<MBX_GEOM_TRANSLATION, 3>(mode, grid, smem, st, L, n, step, first, total, err);
+        else launch_fp_kernel<MBX_GEOM_TRANSLATION, 2>(mode, grid, smem, st, L, n, step, first, total, err);
     }
     note_launch();
     return cudaGetLastError();
@@ -989,12 +1109,17 @@ static int check_schedule(const mbx_scan *scans, int n, const int32_t *schedule,
 
 using namespace mbx;
 
-extern "C" size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps) {
-    if (!scans || num_scans <= 0 || num_steps <= 0) return 0;
+extern "C" size_t mbx_vcd_batched_workspace_bytes2(const mbx_scan *scans, int32_t num_scans, int32_t num_steps,
+                                                   int32_t flags) {
+    if (!scans || num_scans <= 0 || num_steps <= 0 || (flags & ~MBX_BATCHED_PLAN_FORWARD)) return 0;
     Layout L;
     std::vector<ScanSizes> zs;
-    if (layout(scans, num_scans, num_steps, L, zs) != MBX_OK) return 0;
+    if (layout(scans, num_scans, num_steps, L, zs, flags) != MBX_OK) return 0;
     return L.total;
+}
+
+extern "C" size_t mbx_vcd_batched_workspace_bytes(const mbx_scan *scans, int32_t num_scans, int32_t num_steps) {
+    return mbx_vcd_batched_workspace_bytes2(scans, num_scans, num_steps, 0);
 }
 
 static const BatchedPlanHost *plan_of(const mbx_batched_plan *p) {
@@ -1007,12 +1132,20 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
                                        int32_t num_steps, int32_t num_iterations, double *step_stats,
                                        double *iter_stats, void *workspace, size_t workspace_bytes,
                                        mbx_batched_plan *plan_out, void *stream) {
+    return mbx_vcd_batched_prepare2(scans, num_scans, schedule, num_steps, num_iterations, step_stats, iter_stats,
+                                    workspace, workspace_bytes, 0, plan_out, stream);
+}
+
+extern "C" int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans, const int32_t *schedule,
+                                        int32_t num_steps, int32_t num_iterations, double *step_stats,
+                                        double *iter_stats, void *workspace, size_t workspace_bytes, int32_t flags,
+                                        mbx_batched_plan *plan_out, void *stream) {
     if (!scans || num_scans <= 0 || !schedule || num_steps <= 0 || num_iterations < 0 || !plan_out || !step_stats ||
-        (num_iterations > 0 && !iter_stats))
+        (num_iterations > 0 && !iter_stats) || (flags & ~MBX_BATCHED_PLAN_FORWARD))
         return MBX_ERR_INVALID_ARG;
     Layout L;
     std::vector<ScanSizes> zs;
-    int rc = layout(scans, num_scans, num_steps, L, zs);
+    int rc = layout(scans, num_scans, num_steps, L, zs, flags);
     if (rc != MBX_OK) return rc;
     if (!workspace || workspace_bytes < L.total) return MBX_ERR_WORKSPACE;
     rc = check_schedule(scans, num_scans, schedule, num_steps);
@@ -1027,6 +1160,7 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     FpArgs *hif = reinterpret_cast<FpArgs *>(host.data() + L.ifp);
     BpArgs *hhb = reinterpret_cast<BpArgs *>(host.data() + L.hbp);
     FiltScan *hfl = reinterpret_cast<FiltScan *>(host.data() + L.filt);
+    CbPlanned *hpn = reinterpret_cast<CbPlanned *>(host.data() + L.planned);
     int *hpl_off = reinterpret_cast<int *>(host.data() + L.pl_off);
     int *hpl_dim = reinterpret_cast<int *>(host.data() + L.pl_dim);
     int *hpl_order = reinterpret_cast<int *>(host.data() + L.pl_order);
@@ -1096,6 +1230,23 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
             f.plan = z.fpp;
             f.chunk_box = reinterpret_cast<const int4 *>(base + L.box_off[s] + (size_t)k * fp_chunk_box_bytes(sc.subset_size));
             hbox_first[ki + 1] = hbox_first[ki] + (int)((sc.subset_size + CB_CHUNK - 1) / CB_CHUNK);
+            if (L.plan_fp) {  // this subset's planned storage
+                const PlannedSizes q = planned_sizes(sc, z);
+                char *pb = base + L.plan_off[s] + (size_t)k * q.total;
+                CbPlanned &pn = hpn[ki];
+                pn.rec = reinterpret_cast<float4 *>(pb + q.rec);
+                pn.rec2 = g.kind != MBX_GEOM_PARALLEL ? reinterpret_cast<float4 *>(pb + q.rec2) : nullptr;
+                pn.sbin = reinterpret_cast<uint8_t *>(pb + q.sbin);
+                pn.rec_cursor = reinterpret_cast<unsigned long long *>(base + L.cursors + 16 * (size_t)ki);
+                pn.pass_cursor = reinterpret_cast<int *>(base + L.cursors + 16 * (size_t)ki + 8);
+                pn.pass_rec = reinterpret_cast<long long *>(pb + q.pass_rec);
+                pn.pass_count = reinterpret_cast<int *>(pb + q.pass_count);
+                pn.pass_bstart = reinterpret_cast<int *>(pb + q.pass_bstart);
+                pn.tile_npass = reinterpret_cast<int *>(pb + q.tile_npass);
+                pn.tile_pass = reinterpret_cast<int *>(pb + q.tile_pass);
+                pn.rec_cap = q.rec_cap;
+                pn.pass_cap = q.pass_cap;
+            }
         }
         if (L.setup) {
             // x0: back projection of the filtered sinogram (held in the error sinogram) into the recon, by index
@@ -1135,15 +1286,15 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     }
     // projection work lists: scans in decreasing order of per-tile cost, so that the dynamically scheduled tail of
     // a launch is made of the cheapest tiles
-    size_t pl_smem[PL_COUNT] = {0, 0, 0, 0, 0};
+    size_t pl_smem[PL_COUNT] = {0, 0, 0, 0, 0, 0};
     for (int w = 0; w < PL_COUNT; ++w) {
         std::vector<int> ord(n), tiles(n), dim(n);
         std::vector<double> cost(n);
         for (int s = 0; s < n; ++s) {
-            list_dims(w, scans[s], zs[s], tiles[s], dim[s], cost[s]);
+            list_dims(w, scans[s], zs[s], tiles[s], dim[s], cost[s], L.plan_fp);
             ord[s] = s;
             const ScanSizes &z = zs[s];
-            const size_t sm = w == PL_BP ? z.bpp.smem : (w == PL_FP || w == PL_INIT_FP) ? z.fpp.smem
+            const size_t sm = w == PL_BP ? z.bpp.smem : (w == PL_FP || w == PL_INIT_FP || w == PL_BUILD) ? z.fpp.smem
                               : w == PL_INIT_BP ? (z.setup ? z.ibp.smem : 0) : (z.setup ? z.hbp.smem : 0);
             pl_smem[w] = std::max(pl_smem[w], sm);
         }
@@ -1178,6 +1329,10 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     P.t.init_fp = reinterpret_cast<FpArgs *>(base + L.ifp);
     P.t.hess_bp = reinterpret_cast<BpArgs *>(base + L.hbp);
     P.t.filt = reinterpret_cast<FiltScan *>(base + L.filt);
+    P.t.planned = L.plan_fp ? reinterpret_cast<CbPlanned *>(base + L.planned) : nullptr;
+    P.planned_fp = L.plan_fp ? 1 : 0;
+    P.plan_cursors = L.plan_fp ? base + L.cursors : nullptr;
+    P.plan_cursor_bytes = L.plan_fp ? 16 * (size_t)L.ksum : 0;
     P.t.pl_off = reinterpret_cast<int *>(base + L.pl_off);
     P.t.pl_dim = reinterpret_cast<int *>(base + L.pl_dim);
     P.t.pl_order = reinterpret_cast<int *>(base + L.pl_order);
@@ -1223,6 +1378,10 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
     e = set_max_dynamic_smem(kbp, 100 * 1024);
     if (e == cudaSuccess) e = set_max_dynamic_smem(kfp2, 200 * 1024);
     if (e == cudaSuccess) e = set_max_dynamic_smem(kfp3, 200 * 1024);
+    for (int mb = 2; mb <= 3 && e == cudaSuccess && L.plan_fp; ++mb) {
+        e = set_max_dynamic_smem(fp_kernel_of(P.kind, mb, CB_REPLAY), 200 * 1024);
+        if (e == cudaSuccess) e = set_max_dynamic_smem(fp_kernel_of(P.kind, mb, CB_BUILD), 200 * 1024);
+    }
     if (e == cudaSuccess) e = set_max_dynamic_smem(reinterpret_cast<const void *>(b_filter), 200 * 1024);
     if (e != cudaSuccess) return set_cuda_error(e);
     P.pl_grid[PL_BP] = bp_grid(P.kind, P.pl_smem[PL_BP], P.pl_total[PL_BP]);
@@ -1263,7 +1422,14 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
                                                          reinterpret_cast<int4 *>(base + L.fbox_off[s]));
         note_launch();
     }
-    e = cudaGetLastError();
+    // no planned tile is replayed before a build stores it
+    for (int s2 = 0, k2 = 0; s2 < n && L.plan_fp; ++s2)
+        for (int k = 0; k < scans[s2].num_subsets && e == cudaSuccess; ++k, ++k2) {
+            const PlannedSizes q = planned_sizes(scans[s2], zs[s2]);
+            e = cudaMemsetAsync(base + L.plan_off[s2] + (size_t)k * q.total + q.tile_npass, 0xFF,
+                                sizeof(int) * (size_t)q.tiles, st);
+        }
+    if (e == cudaSuccess) e = cudaGetLastError();
     if (e == cudaSuccess) e = cudaStreamSynchronize(st);
     if (e != cudaSuccess) return set_cuda_error(e);
     if (autotune_enabled()) {  // (also in forced mode: the tune functions then apply the forced choice)
@@ -1272,6 +1438,10 @@ extern "C" int mbx_vcd_batched_prepare(const mbx_scan *scans, int32_t num_scans,
         if (rc2 == MBX_OK) rc2 = tune_batched_fp_layouts(P, L, scans, o_fp, hpl_order + PL_FP * n, st);
         if (rc2 == MBX_OK) rc2 = tune_batched_bp(P, L, scans, hb, o_bp, hpl_order + PL_BP * n, st);
         if (rc2 != MBX_OK) return rc2;
+    }
+    if (P.planned_fp) {  // the replay and build kernels of the forward variant the tuner kept
+        P.pl_grid_replay = fp_grid(P.kind, P.fp_minb, P.pl_smem[PL_FP], P.pl_total[PL_FP], CB_REPLAY);
+        P.pl_grid_build = fp_grid(P.kind, P.fp_minb, P.pl_smem[PL_FP], std::max(1, P.pl_total[PL_BUILD]), CB_BUILD);
     }
     P.magic = BT_MAGIC;
     std::memset(plan_out, 0, sizeof(*plan_out));
@@ -1291,8 +1461,9 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
             return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
         case 1: b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err); break;
         case 2:
-            e = launch_fp_list(*P, PL_FP, P->fp_minb, step, 0, P->pl_total[PL_FP], P->pl_grid[PL_FP],
-                               P->pl_smem[PL_FP], st);
+            e = launch_fp_list(*P, PL_FP, P->fp_minb, step, 0, P->pl_total[PL_FP],
+                               P->planned_fp ? P->pl_grid_replay : P->pl_grid[PL_FP], P->pl_smem[PL_FP], st,
+                               P->planned_fp ? CB_REPLAY : CB_WALK);
             return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
         case 3: b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;
         case 4: b_alpha<<<warp_blocks, 256, 0, st>>>(T, n, step); break;
@@ -1403,8 +1574,15 @@ extern "C" int mbx_vcd_batched_update(const mbx_batched_plan *plan, const mbx_sc
 extern "C" int mbx_vcd_batched_refresh(const mbx_batched_plan *plan, void *stream) {
     const BatchedPlanHost *P = plan_of(plan);
     if (!P) return MBX_ERR_INVALID_ARG;
-    b_chunk_bounds<<<P->box_grid, CB_CHUNK, 0, static_cast<cudaStream_t>(stream)>>>(P->t, P->ksum, P->box_total);
+    cudaStream_t st = static_cast<cudaStream_t>(stream);
+    b_chunk_bounds<<<P->box_grid, CB_CHUNK, 0, st>>>(P->t, P->ksum, P->box_total);
     note_launch();
     cudaError_t e = cudaGetLastError();
+    if (e == cudaSuccess && P->planned_fp) {  // store the sorted passes of every subset's tiles
+        e = cudaMemsetAsync(P->plan_cursors, 0, P->plan_cursor_bytes, st);
+        if (e == cudaSuccess)
+            e = launch_fp_list(*P, PL_BUILD, P->fp_minb, 0, 0, P->pl_total[PL_BUILD], P->pl_grid_build,
+                               P->pl_smem[PL_FP], st, CB_BUILD);
+    }
     return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
 }

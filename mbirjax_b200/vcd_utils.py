@@ -60,7 +60,7 @@ def gen_partition_sequence(partition_sequence, max_iterations):
 
 
 _FULL_INDICES = {}  # (rows, cols, use_ror_mask) -> sorted region of reconstruction
-_CACHE_GRIDS = 16    # grid sizes each host cache keeps (the oldest entry goes first)
+_CACHE_GRIDS = 64    # grid sizes each host cache keeps (the oldest entry goes first; a batch holds many)
 
 
 def _cache_put(cache, key, value):
