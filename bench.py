@@ -283,44 +283,51 @@ def plain_recon(models, sinos):
 
 
 def batched_roofline(models, sinos, peak_gbs, peak_kind):
-    """Average duration of the batched back- and forward-projection stages (CUDA events, 4 subset steps)."""
+    """Average duration of each batched stage of a subset step (CUDA events, the K steps of one iteration), on the
+    device state the benchmark's reconstructions use: after one recon() call of the batch, whose refresh built the
+    planned forward projections, the stages of steps 0..K-1 are launched one by one.  Also the duration of that
+    refresh (chunk boxes and the build of the planned forward projections, once per reconstruction)."""
     import torch
     from mbirjax_b200 import _capi
-    from mbirjax_b200.batched import BatchedVCD
-    b = BatchedVCD(models, sinos, seeds=list(range(len(models))))
-    scans, sched = b._setup(1)
-    dev = b.states[0]['device']
-    n = len(scans)
-    step_stats = torch.zeros((sched.shape[0], n, 4), dtype=torch.float64, device=dev)
-    iter_stats = torch.zeros((1, n, 4), dtype=torch.float64, device=dev)
-    plan, ws = _capi.vcd_batched_prepare(scans, sched, 1, step_stats, iter_stats, dev)
+    from mbirjax_b200 import batched as B
+    b = B.BatchedVCD(models, sinos, seeds=list(range(len(models))))
+    b.recon(max_iterations=BATCH['iterations'])
+    sess = B._SESSIONS[B._batch_key(models, b.weights, BATCH['iterations'])]
+    plan, K = sess.plan, sess.num_subsets
+
+    def timed(fn):
+        s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
+        s.record()
+        fn()
+        e.record()
+        torch.cuda.synchronize()
+        return s.elapsed_time(e)
+
+    build_ms = timed(lambda: _capi.vcd_batched_refresh(plan))
     times = {k: 0.0 for k in _capi.BATCHED_STAGES}
-    for step in range(sched.shape[0]):
+    for step in range(K):
         for stage, name in enumerate(_capi.BATCHED_STAGES):
-            s, e = torch.cuda.Event(enable_timing=True), torch.cuda.Event(enable_timing=True)
-            s.record()
-            _capi.vcd_batched_stage(plan, step, stage)
-            e.record()
-            torch.cuda.synchronize()
-            times[name] += s.elapsed_time(e)
-    steps = sched.shape[0]
+            times[name] += timed(lambda: _capi.vcd_batched_stage(plan, step, stage))
     alg = 0.0
-    for m, sc in zip(models, scans):
+    for m, part in zip(models, sess.part):
         V, R, C = m.get_params('sinogram_shape')
         S = m.get_params('recon_shape')[2]
-        alg += 4.0 * (V * sc.subset_size * S + V * R * C)
+        alg += 4.0 * (V * int(part.shape[1]) * S + V * R * C)
     res = {}
     for name in ('bp', 'fp'):
-        ms = times[name] / steps
+        ms = times[name] / K
         res[name] = {'ms': ms, 'gbs': alg / (ms * 1e-3) / 1e9}
     dom = max(res, key=lambda k: res[k]['ms'])
-    traffic = profile_traffic('b_' + dom)
+    kernel = {'bp': 'b_bp', 'fp': 'b_fp_replay' if sess.planned_forward else 'b_fp'}
+    traffic = profile_traffic(kernel[dom])
     share = {k: round(v / sum(times.values()), 4) for k, v in times.items()}
-    return {'kernel': 'b_' + dom, 'bound': 'hbm', 'achieved': round(res[dom]['gbs'], 1), 'peak': peak_gbs,
+    return {'kernel': kernel[dom], 'bound': 'hbm', 'achieved': round(res[dom]['gbs'], 1), 'peak': peak_gbs,
             'peak_kind': peak_kind, 'unit': 'GB/s', 'frac': round(res[dom]['gbs'] / peak_gbs, 4),
             'traffic': traffic, 'launch_ms': round(res[dom]['ms'], 4), 'alg_bytes_per_launch': alg,
-            'other': {'b_' + k: {'launch_ms': round(v['ms'], 4), 'achieved_gbs': round(v['gbs'], 1)}
+            'other': {kernel[k]: {'launch_ms': round(v['ms'], 4), 'achieved_gbs': round(v['gbs'], 1),
+                                  'frac': round(v['gbs'] / peak_gbs, 4)}
                       for k, v in res.items() if k != dom},
+            'planned_forward': bool(sess.planned_forward), 'plan_build_ms_per_recon': round(build_ms, 3),
             'stage_time_share': share}
 
 
@@ -684,9 +691,14 @@ def run_gpu(args):
     torch.cuda.synchronize()
     clocks = ClockSampler(local)
     clocks.start()
-    launches0 = lib.mbx_launch_count()
+    from mbirjax_b200 import batched as _batched
+
+    def kernel_launches():  # host-submitted launches plus the kernels of replayed batched graphs
+        return int(lib.mbx_launch_count()) + _batched.replayed_launches()
+
+    launches0 = kernel_launches()
     ms = timed_steps(step, args.steps, 0, world, flush)
-    launches = lib.mbx_launch_count() - launches0
+    launches = kernel_launches() - launches0
     clk = clocks.stop()
     ms = max_over_ranks(ms, world)
     value = world * units * args.steps / (ms * 1e-3)

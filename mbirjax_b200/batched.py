@@ -30,6 +30,15 @@ from .vcd_utils import (gen_full_indices, gen_partition_sequence, gen_set_of_pix
 
 __all__ = ['BatchedVCD', 'release_batched_sessions', 'morton_order']
 
+_REPLAYED = [0]  # kernel launches replayed from the batched CUDA graphs (mbx_launch_count counts host launches)
+
+
+def replayed_launches():
+    """Kernels of this library launched by replays of the batched CUDA graphs so far (each replay launches every
+    kernel node its capture recorded; mbx_launch_count counts only launches the host submits)."""
+    return _REPLAYED[0]
+
+
 _SESSIONS = collections.OrderedDict()  # batch key -> _Session, most recently used last
 _MAX_SESSIONS = 2
 PLAN_FORWARD = True               # plan the subset forward projections of a batch when it fits (see _Session)
@@ -216,8 +225,9 @@ class BatchedVCD:
 
         graph = None
         if use_graph:
-            graph = _capture(run_all)
+            graph, kernels = _capture_counted(run_all)
             graph.replay()
+            _REPLAYED[0] += kernels
         else:
             run_all()
         step = step_stats.cpu().numpy()  # synchronises
@@ -326,16 +336,18 @@ class _Session:
             self._setup_launches()
             return
         if self.setup_graph is None:
-            self.setup_graph = _capture(self._setup_launches)
+            self.setup_graph, self.setup_kernels = _capture_counted(self._setup_launches)
         self.setup_graph.replay()
+        _REPLAYED[0] += self.setup_kernels
 
     def run_iterations(self, use_graph):
         if not use_graph:
             self._iteration_launches()
             return
         if self.iter_graph is None:
-            self.iter_graph = _capture(self._iteration_launches)
+            self.iter_graph, self.iter_kernels = _capture_counted(self._iteration_launches)
         self.iter_graph.replay()
+        _REPLAYED[0] += self.iter_kernels
 
     def results(self, models, regs, sigmas):
         step = self.step_stats.cpu().numpy()  # synchronises
@@ -399,6 +411,14 @@ def _capture(launches):
             graph.capture_end()
     main.wait_stream(side)
     return graph
+
+
+def _capture_counted(launches):
+    """_capture, and the number of library kernels the graph holds (counted while capturing)."""
+    lib = _capi.load_library()
+    n0 = lib.mbx_launch_count()
+    graph = _capture(launches)
+    return graph, int(lib.mbx_launch_count() - n0)
 
 
 def _copy_in(dst, src):

@@ -137,3 +137,16 @@ def test_planned_forward_projections_match_the_walk(cuda):
         B.release_batched_sessions()
     for a, b in zip(out[False], out[True]):
         assert torch.equal(a, b)
+
+
+def test_graph_replays_count_their_kernels(cuda):
+    """Every replay of the batched graphs adds the kernels its capture recorded to batched.replayed_launches(), so
+    that a benchmark counting library launches sees the replayed ones too."""
+    from mbirjax_b200 import batched as B
+    items = [_scan('parallel', v, r, c, sd) for (v, r, c), sd in zip([(30, 6, 40), (26, 5, 44)], [1, 2])]
+    args = ([it[0] for it in items], [it[2] for it in items])
+    BatchedVCD(*args, seeds=[1, 2]).recon(max_iterations=2)  # builds the session and captures its graphs
+    n0 = B.replayed_launches()
+    BatchedVCD(*args, seeds=[1, 2]).recon(max_iterations=2)
+    sess = next(s for s in B._SESSIONS.values() if s.max_iterations == 2)
+    assert B.replayed_launches() - n0 == sess.setup_kernels + sess.iter_kernels > 2 * 8
