@@ -66,6 +66,11 @@ TRANS = dict(nx=7, nz=7, spacing=22.0, rows=128, channels=128, sdd=64.0, sid=64.
              iterations=15, sharpness=1.0)
 
 
+def sig(x, digits=4):
+    """x rounded to a number of significant digits (throughputs here span 1e-5 to 1e2 recons/s)."""
+    return float('%.*g' % (digits, x))
+
+
 def parse_args():
     ap = argparse.ArgumentParser()
     ap.add_argument('--gpus', type=int, default=1)
@@ -702,7 +707,7 @@ def run_gpu(args):
     clk = clocks.stop()
     ms = max_over_ranks(ms, world)
     value = world * units * args.steps / (ms * 1e-3)
-    line = {'metric': METRIC, 'value': round(value, 4), 'unit': 'recons/s', 'n_gpus': world, 'steps': args.steps,
+    line = {'metric': METRIC, 'value': sig(value), 'unit': 'recons/s', 'n_gpus': world, 'steps': args.steps,
             'warmup': args.warmup, 'ms_per_step': round(ms / args.steps, 3), 'higher_is_better': True,
             'scaling': 'weak', 'vs_baseline': None, 'dtype': 'f32', 'data': 'synthetic', 'config': config,
             'gpu_launches': int(launches), 'clocks': clk}
@@ -717,7 +722,7 @@ def run_gpu(args):
         rb = batched_recon(models, sinos)
         rp = plain_recon(models, sinos)
         diff = max(float(torch.linalg.norm(a - b) / torch.linalg.norm(b)) for a, b in zip(rb, rp))
-        line['plain_recons_per_s'] = round(plain_value, 4)
+        line['plain_recons_per_s'] = sig(plain_value)
         line['batched_over_plain'] = round(value / plain_value, 3)
         line['max_rel_l2_batched_vs_plain'] = diff
         del rb, rp
@@ -743,7 +748,7 @@ def run_gpu(args):
             h2d, d2h = int(host_sino.numel()) * 4, int(out_host.numel()) * 4
         e_ms = timed_steps(e2e_step, args.steps, 1, world, flush)
         e_ms = max_over_ranks(e_ms, world)
-        line['e2e'] = {'value': round(world * units * args.steps / (e_ms * 1e-3), 4), 'unit': 'recons/s',
+        line['e2e'] = {'value': sig(world * units * args.steps / (e_ms * 1e-3)), 'unit': 'recons/s',
                        'h2d_bytes_per_step': h2d, 'd2h_bytes_per_step': d2h}
 
     if args.workload == 'batched':
@@ -781,13 +786,13 @@ def run_gpu(args):
                 dt = cs.run()
             finally:
                 cs.close()
-            line['cpu_baseline'] = {'value': round(units / (dt * cs.scale), 6), 'unit': 'recons/s',
+            line['cpu_baseline'] = {'value': sig(units / (dt * cs.scale)), 'unit': 'recons/s',
                                     'cores': cs.workers, 'kind': 'port', 'sample': cs.describe(dt)}
         else:
             spec = single_scan_spec(args.workload)[0]
             dt, cores = cpu_reference_sample(workload=args.workload)
             scale = cpu_sample_scale(args.workload)
-            line['cpu_baseline'] = {'value': round(units / (dt * scale), 6), 'unit': 'recons/s', 'cores': cores,
+            line['cpu_baseline'] = {'value': sig(units / (dt * scale)), 'unit': 'recons/s', 'cores': cores,
                                     'kind': 'port',
                                     'sample': 'one VCD subset update of %s (oracle NumPy port, %d processes), %.2f s, '
                                               'scaled x%.1f to the whole reconstruction' % (

@@ -114,9 +114,9 @@ def qggmrf_loss(recon, qggmrf_params):
 
 
 def weighted_ls_qggmrf_loss(recon, model, sinogram, weights, qggmrf_params, view_chunk=None):
-    """0.5 * || W^(1/2) (A x - y) ||^2 + qGGMRF(x)."""
+    """0.5 * || W^(1/2) (A x - y) ||^2 + qGGMRF(x), summed in float64 (a float64 scalar)."""
     r = forward_project(recon, model, view_chunk) - sinogram
-    data = 0.5 * torch.sum(weights * r * r) if weights is not None else 0.5 * torch.sum(r * r)
+    data = 0.5 * torch.sum(weights * r * r if weights is not None else r * r, dtype=torch.float64)
     return data + qggmrf_loss(recon, qggmrf_params)
 
 

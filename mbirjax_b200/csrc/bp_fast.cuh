@@ -32,6 +32,9 @@ constexpr int BPF_CACHE_ROWS = 48;  // row-cache depth per thread (cone): ts * m
 #ifndef MBX_BPF_CHUNK_CONE
 #define MBX_BPF_CHUNK_CONE 512          // same, cone beam (its row cache takes most of the shared memory)
 #endif
+#ifndef MBX_BPF_PREFETCH
+#define MBX_BPF_PREFETCH 0              // parallel beam, staged footprints: views ahead whose rows are prefetched
+#endif                                  // into L1 while the current view is gathered (0: none)
 
 struct BpfPlan {
     int nsl;      // slice tiles per CTA (warps per pixel group)
@@ -394,6 +397,19 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
             if (!active) continue;
             for (int t = 0; t < nv; ++t) {
                 const int f = (t << lg_pcta) + pl;
+                if (MBX_BPF_PREFETCH > 0 && KIND == MBX_GEOM_PARALLEL && sino && t + MBX_BPF_PREFETCH < nv) {
+                    // the rows of a later view of the chunk: start their L2 -> L1 fills now, so that its gathers
+                    // hit L1 (a prefetch writes no register and faults on no address; the view and channel are
+                    // checked as for the gather)
+                    const int tn = t + MBX_BPF_PREFETCH;
+                    const int first_n = __float_as_int(s_fa[(tn << lg_pcta) + pl].x);
+                    const int voff_n = s_voff[tn];
+                    if (first_n >= 0 && voff_n >= 0) {
+                        const float *q = sino + (voff_n + s0c + first_n);
+                        for (int s = 0; s < ns; ++s, q += num_channels)
+                            asm volatile("prefetch.global.L1 [%0];" ::"l"(q));
+                    }
+                }
                 const float4 fa = s_fa[f];
                 if (__float_as_int(fa.x) < 0) continue;
                 gather(fa, KIND != MBX_GEOM_PARALLEL ? s_fb[f] : make_float4(0.f, 0.f, 0.f, 0.f), s_voff[t]);

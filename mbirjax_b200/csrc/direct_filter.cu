@@ -9,7 +9,9 @@
 // FILT_ROWS detector rows: it stages them transposed in shared memory ([channel][row], so one float4 pair
 // feeds FILT_ROWS accumulators), stages the scaled filter taps, and each thread produces channel outputs.
 // FDK: the pre-weight D / sqrt(D^2 + u^2 + v^2) (cone_beam.py:806-818, detector_mn_to_uv :709-738) is applied
-// while staging; both geometries apply the final pi / num_views.
+// while staging; both geometries apply the final pi / num_views.  Taps, pre-weight and sums are float64 (the
+// float32 sums of a direct convolution are off by a few 1e-6 of the row's scale, which the VCD iterations that
+// start from this recon can amplify).
 #include "direct_filter.cuh"
 #include "mbx_host.hpp"
 
@@ -17,8 +19,8 @@ namespace mbx {
 
 __global__ void __launch_bounds__(FILT_THREADS)
 direct_filter_kernel(const float *__restrict__ sino, float *__restrict__ out, long long num_rows_total, int R, int C,
-                     float filter_scale, float out_scale, int fdk, float D, float delta_det_channel,
-                     float delta_det_row, float det_channel_offset, float det_row_offset) {
+                     double filter_scale, double out_scale, int fdk, double D, double delta_det_channel,
+                     double delta_det_row, double det_channel_offset, double det_row_offset) {
     extern __shared__ __align__(16) float sm[];
     direct_filter_rows(sino, out, (long long)blockIdx.x * FILT_ROWS, num_rows_total, R, C, filter_scale, out_scale,
                        fdk, D, delta_det_channel, delta_det_row, det_channel_offset, det_row_offset, sm);
@@ -34,7 +36,7 @@ extern "C" int mbx_direct_filter(const mbx_geom *g, const float *sinogram, float
     // tomography_model.py:934-964)
     if (g->kind == MBX_GEOM_TRANSLATION) return MBX_ERR_UNSUPPORTED;
     const int C = g->num_det_channels, R = g->num_det_rows;
-    const size_t smem = mbx::filter_smem_bytes(C);
+    const size_t smem = mbx::filter_smem_bytes(C, g->kind != MBX_GEOM_PARALLEL);
     if (smem > 200 * 1024) return MBX_ERR_UNSUPPORTED;
     {
         cudaError_t e = mbx::set_max_dynamic_smem(reinterpret_cast<const void *>(mbx::direct_filter_kernel),
@@ -42,7 +44,7 @@ extern "C" int mbx_direct_filter(const mbx_geom *g, const float *sinogram, float
         if (e != cudaSuccess) return mbx::set_cuda_error(e);
     }
     const long long rows_total = (long long)g->num_views * R;
-    float filter_scale, out_scale;
+    double filter_scale, out_scale;
     int fdk;
     mbx::direct_filter_scales(*g, filter_scale, out_scale, fdk);
     const unsigned blocks = (unsigned)((rows_total + mbx::FILT_ROWS - 1) / mbx::FILT_ROWS);

@@ -61,7 +61,7 @@ struct FiltScan {
     float *out;
     long long rows;
     int R, C, fdk;
-    float filter_scale, out_scale, D, ddc, ddr, dco, dro;
+    double filter_scale, out_scale, D, ddc, ddr, dco, dro;
 };
 
 // A work list of projection tiles over the scans of a batch: per scan, its argument record(s) and tile count.
@@ -573,7 +573,8 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
         z.hbp = plan_bp_fast(g, z.npix, g.num_views);
         if (!z.hbp.ok) return MBX_ERR_UNSUPPORTED;
         if (g.kind != MBX_GEOM_TRANSLATION) {  // translation geometry starts from zeros (no direct recon)
-            if (filter_smem_bytes(g.num_det_channels) > 200 * 1024) return MBX_ERR_UNSUPPORTED;
+            if (filter_smem_bytes(g.num_det_channels, g.kind != MBX_GEOM_PARALLEL) > 200 * 1024)
+                return MBX_ERR_UNSUPPORTED;
             z.ibp = plan_bp_fast(g, sc.num_full_indices, g.num_views);
             if (!z.ibp.ok) return MBX_ERR_UNSUPPORTED;
             z.flt_tiles = (int)(((long long)g.num_views * g.num_det_rows + FILT_ROWS - 1) / FILT_ROWS);
@@ -1371,7 +1372,9 @@ extern "C" int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans
     P.fp_minb = 2;
     size_t flt_smem = 0;
     for (int s = 0; s < n; ++s)
-        if (zs[s].setup) flt_smem = std::max(flt_smem, filter_smem_bytes(scans[s].geom.num_det_channels));
+        if (zs[s].setup)
+            flt_smem = std::max(flt_smem, filter_smem_bytes(scans[s].geom.num_det_channels,
+                                                            scans[s].geom.kind != MBX_GEOM_PARALLEL));
     P.flt_smem = flt_smem;
     // kernel attributes and resident-CTA grids
     const void *kbp = bp_kernel_of(P.kind), *kfp2 = fp_kernel_of(P.kind, 2), *kfp3 = fp_kernel_of(P.kind, 3);
