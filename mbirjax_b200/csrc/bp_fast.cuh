@@ -33,8 +33,9 @@ constexpr int BPF_CACHE_ROWS = 48;  // row-cache depth per thread (cone): ts * m
 #define MBX_BPF_CHUNK_CONE 512          // same, cone beam (its row cache takes most of the shared memory)
 #endif
 #ifndef MBX_BPF_PREFETCH
-#define MBX_BPF_PREFETCH 0              // parallel beam, staged footprints: views ahead whose rows are prefetched
-#endif                                  // into L1 while the current view is gathered (0: none)
+#define MBX_BPF_PREFETCH 2              // parallel beam, staged footprints: views ahead whose rows are prefetched
+#endif                                  // into L1 while the current view is gathered (0: none; 1, 2 and 4 measure
+                                        // the same, 8.5% faster than none on the batched bench stage)
 
 struct BpfPlan {
     int nsl;      // slice tiles per CTA (warps per pixel group)
