@@ -88,6 +88,9 @@ def parse_args():
                          '(default 0)')
     ap.add_argument('--autotune', type=int, default=1, choices=[0, 1],
                     help='1: tune the projector plans (default); 0: default plans, no tuning launches (for profiling)')
+    ap.add_argument('--no-plan-forward', action='store_true',
+                    help='batched path: scan, sort and walk every forward projection instead of replaying stored '
+                         'record passes (for comparison and profiling)')
     args = ap.parse_args()
     if args.steps is None:
         args.steps = 1 if args.workload == 'large' else 5
@@ -651,6 +654,9 @@ def run_gpu(args):
     device = torch.device('cuda', local)
     lib = _capi.load_library()
     _capi.set_autotune(args.autotune)
+    if args.no_plan_forward:
+        from mbirjax_b200 import batched as B
+        B.PLAN_FORWARD = False
     peak_gbs, peak_kind = load_peaks()
     flush_buf = torch.empty(256 * 1024 * 1024 // 4, dtype=torch.float32, device=device)
 
