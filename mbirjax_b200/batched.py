@@ -118,8 +118,10 @@ class BatchedVCD:
     def _host_draws(self, max_iterations, small, small_w):
         """The host part of every scan (see _scan_draws).  With per-scan seeds each scan draws from its own
         RandomState, which is the stream np.random.seed(seed) gives, so the scans run on a pool of host threads
-        (NumPy releases the GIL in the draws and sorts) and the global stream is left where the plain path leaves it,
-        after the last scan's draws.  Without seeds the scans draw from the global stream one after another.
+        and the global stream is left where the plain path leaves it, after the last scan's draws.  (The legacy
+        shuffles, most of this time, hold the GIL, so the threads overlap only the sorts and array work; the
+        whole host part runs while the set-up graph runs on the device.)  Without seeds the scans draw from the
+        global stream one after another.
         Returns (regularisation dicts, partitions, schedule (steps, scans), fm constants, qGGMRF records, sigmas)."""
         n = len(self.models)
         for model in self.models:

@@ -24,7 +24,10 @@
 namespace mbx {
 
 constexpr int BPF_THREADS = 256;
-constexpr int BPF_ST = 16;          // most slices per thread
+#ifndef MBX_BPF_ST
+#define MBX_BPF_ST 16
+#endif
+constexpr int BPF_ST = MBX_BPF_ST;  // most slices per thread
 constexpr int BPF_CACHE_ROWS = 48;  // row-cache depth per thread (cone): ts * max|dm/dk| + 4 must fit
 #ifndef MBX_BPF_CHUNK_PARALLEL
 #define MBX_BPF_CHUNK_PARALLEL 1024     // footprints staged per view chunk, parallel beam
@@ -183,6 +186,13 @@ __device__ __forceinline__ void bpf_gather_rows(float (&acc)[BPF_ST], const floa
     }
 }
 
+// The same for a tile of TS slices when TS fits the accumulators (other TS never occur: ns <= ts <= BPF_ST).
+template <int TS>
+__device__ __forceinline__ void bpf_gather_ts(float (&acc)[BPF_ST], const float *__restrict__ sino, int o,
+                                              int num_channels, const float4 &fa) {
+    if constexpr (TS <= BPF_ST) bpf_gather_rows<TS>(acc, sino, o, num_channels, fa);
+}
+
 template <int KIND>
 __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf, int *err) {
     const mbx_geom &g = A.g;
@@ -270,21 +280,21 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 }
             } else {
                 switch (ns) {  // the same for every lane of the warp (a warp holds one slice tile)
-                    case 1: bpf_gather_rows<1>(acc, sino, o, num_channels, fa); break;
-                    case 2: bpf_gather_rows<2>(acc, sino, o, num_channels, fa); break;
-                    case 3: bpf_gather_rows<3>(acc, sino, o, num_channels, fa); break;
-                    case 4: bpf_gather_rows<4>(acc, sino, o, num_channels, fa); break;
-                    case 5: bpf_gather_rows<5>(acc, sino, o, num_channels, fa); break;
-                    case 6: bpf_gather_rows<6>(acc, sino, o, num_channels, fa); break;
-                    case 7: bpf_gather_rows<7>(acc, sino, o, num_channels, fa); break;
-                    case 8: bpf_gather_rows<8>(acc, sino, o, num_channels, fa); break;
-                    case 9: bpf_gather_rows<9>(acc, sino, o, num_channels, fa); break;
-                    case 10: bpf_gather_rows<10>(acc, sino, o, num_channels, fa); break;
-                    case 11: bpf_gather_rows<11>(acc, sino, o, num_channels, fa); break;
-                    case 12: bpf_gather_rows<12>(acc, sino, o, num_channels, fa); break;
-                    case 13: bpf_gather_rows<13>(acc, sino, o, num_channels, fa); break;
-                    case 14: bpf_gather_rows<14>(acc, sino, o, num_channels, fa); break;
-                    case 15: bpf_gather_rows<15>(acc, sino, o, num_channels, fa); break;
+                    case 1: bpf_gather_ts<1>(acc, sino, o, num_channels, fa); break;
+                    case 2: bpf_gather_ts<2>(acc, sino, o, num_channels, fa); break;
+                    case 3: bpf_gather_ts<3>(acc, sino, o, num_channels, fa); break;
+                    case 4: bpf_gather_ts<4>(acc, sino, o, num_channels, fa); break;
+                    case 5: bpf_gather_ts<5>(acc, sino, o, num_channels, fa); break;
+                    case 6: bpf_gather_ts<6>(acc, sino, o, num_channels, fa); break;
+                    case 7: bpf_gather_ts<7>(acc, sino, o, num_channels, fa); break;
+                    case 8: bpf_gather_ts<8>(acc, sino, o, num_channels, fa); break;
+                    case 9: bpf_gather_ts<9>(acc, sino, o, num_channels, fa); break;
+                    case 10: bpf_gather_ts<10>(acc, sino, o, num_channels, fa); break;
+                    case 11: bpf_gather_ts<11>(acc, sino, o, num_channels, fa); break;
+                    case 12: bpf_gather_ts<12>(acc, sino, o, num_channels, fa); break;
+                    case 13: bpf_gather_ts<13>(acc, sino, o, num_channels, fa); break;
+                    case 14: bpf_gather_ts<14>(acc, sino, o, num_channels, fa); break;
+                    case 15: bpf_gather_ts<15>(acc, sino, o, num_channels, fa); break;
                     default: bpf_gather_rows<BPF_ST>(acc, sino, o, num_channels, fa); break;
                 }
             }
