@@ -32,7 +32,7 @@ size_t bp_workspace_bytes(const mbx_geom &g, long long num_pixels, int num_views
 template <int KIND>
 static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const float *sino, const float *w,
                                   const int32_t *pix, long long n, const int32_t *views, int nv, int cp, float scale,
-                                  float *dst, long long ss, cudaStream_t st) {
+                                  float *dst, long long ss, cudaStream_t st, int out_slices = 0) {
     auto kern = bp_fast_kernel<KIND>;
     cudaError_t ea = set_max_dynamic_smem(reinterpret_cast<const void *>(kern), 100 * 1024);
     if (ea != cudaSuccess) return ea;
@@ -51,6 +51,7 @@ static cudaError_t launch_bp_fast(const mbx_geom &g, const BpfPlan &pl, const fl
     A.out = dst;
     A.split_stride = ss;
     A.out_by_index = 0;
+    A.out_slices = out_slices;
     A.plan = pl;
     dim3 grid(pl.gx, pl.gy, pl.splits);
     kern<<<grid, BPF_THREADS, pl.smem, st>>>(A, device_error_ptr());
@@ -62,6 +63,16 @@ int back_project(const mbx_geom &g, const float *sino, const float *w, const int
                  const int32_t *views, int num_views_sel, int coeff_power, float scale, float *out, void *ws,
                  size_t ws_bytes, cudaStream_t st) {
     if (num_pixels == 0) return MBX_OK;
+    if (bp_unit_broadcast(g, sino, w)) {  // unit-weight parallel Hessian: one slice, written to every slice
+        const mbx_geom g1 = one_slice_geometry(g);
+        const BpfPlan p1 = plan_bp_fast(g1, num_pixels, num_views_sel);
+        if (p1.ok && p1.splits == 1) {
+            const cudaError_t e = launch_bp_fast<MBX_GEOM_PARALLEL>(g1, p1, nullptr, nullptr, pix, num_pixels, views,
+                                                                   num_views_sel, coeff_power, scale, out, 0, st,
+                                                                   g.num_recon_slices);
+            return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
+        }
+    }
     const BpfPlan fpl = plan_bp_fast(g, num_pixels, num_views_sel);
     if (fpl.ok) {
         if (fpl.workspace > 0 && (ws == nullptr || ws_bytes < fpl.workspace)) return MBX_ERR_WORKSPACE;

@@ -170,8 +170,24 @@ struct BpArgs {
     float *out;                // (num_pixels, S) in list order, or a flat recon when out_by_index
     long long split_stride;    // 0: final output; else partial-sum workspace stride
     int out_by_index;
+    int out_slices;            // > 0: g has one slice and its value is written to all out_slices slices of the
+                               // output cylinder (the unit-weight Hessian of parallel beam, equal in every slice)
     BpfPlan plan;
 };
+
+// Parallel beam with neither sinogram nor weights (the unit-weight Hessian diagonal): every detector row holds the
+// same ones and every slice the same footprints, so all slices of a pixel receive the same sum of the same terms
+// in the same order.  The back projection is then planned on one slice (one_slice_geometry) and that value is
+// written to every slice.
+inline bool bp_unit_broadcast(const mbx_geom &g, const float *sino, const float *wts) {
+    return g.kind == MBX_GEOM_PARALLEL && !sino && !wts && g.num_recon_slices > 1;
+}
+
+inline mbx_geom one_slice_geometry(const mbx_geom &g) {
+    mbx_geom g1 = g;
+    g1.num_recon_slices = 1;
+    return g1;
+}
 
 // Parallel-beam gather of one view into the first TS accumulators: three taps at constant offsets from one
 // 32-bit element offset, one detector row per slice (TS = the tile's slice count, so no slot is predicated off).
@@ -411,7 +427,8 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
                 if (MBX_BPF_PREFETCH > 0 && KIND == MBX_GEOM_PARALLEL && sino && t + MBX_BPF_PREFETCH < nv) {
                     // the rows of a later view of the chunk: start their L2 -> L1 fills now, so that its gathers
                     // hit L1 (a prefetch writes no register and faults on no address; the view and channel are
-                    // checked as for the gather)
+                    // checked as for the gather).  (One prefetch per lane and view, of the warp's lowest and
+                    // highest tap line per row, was 7% slower on the batched stage than this one per slice.)
                     const int tn = t + MBX_BPF_PREFETCH;
                     const int first_n = __float_as_int(s_fa[(tn << lg_pcta) + pl].x);
                     const int voff_n = s_voff[tn];
@@ -433,8 +450,14 @@ __device__ void bp_fast_tile(const BpArgs &A, int bx, int by, int bz, float *smf
         if (!active) return;
         row_of_out = pix[p];
     }
-    float *out = A.out + (long long)split * A.split_stride + row_of_out * (long long)num_slices + s0;
     const float sc = (A.split_stride == 0) ? A.scale : 1.0f;
+    if (A.out_slices > 0) {  // the one slice's value in every slice of the cylinder
+        float *out = A.out + row_of_out * (long long)A.out_slices;
+        const float v = active ? sc * acc[0] : 0.0f;
+        for (int s = 0; s < A.out_slices; ++s) out[s] = v;
+        return;
+    }
+    float *out = A.out + (long long)split * A.split_stride + row_of_out * (long long)num_slices + s0;
 #pragma unroll
     for (int s = 0; s < BPF_ST; ++s)
         if (s < ns) out[s] = active ? sc * acc[s] : 0.0f;

@@ -238,7 +238,7 @@ static cudaError_t launch_fp_cb_v(const FpArgs &A, cudaStream_t st) {
     cudaError_t ea = set_max_dynamic_smem(reinterpret_cast<const void *>(fp_cb_kernel<KIND, MINB>), 200 * 1024);
     if (ea != cudaSuccess) return ea;
     dim3 grid(A.num_views_sel, A.plan.cblocks);
-    fp_cb_kernel<KIND, MINB><<<grid, CB_THREADS, A.plan.smem, st>>>(A, device_error_ptr());
+    fp_cb_kernel<KIND, MINB><<<grid, CB_THREADS, A.plan.walk.smem, st>>>(A, device_error_ptr());
     note_launch();
     return cudaGetLastError();
 }

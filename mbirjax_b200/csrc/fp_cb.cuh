@@ -27,8 +27,10 @@
 // slice heights shifted by -tz (a per-view constant of the tile).
 #pragma once
 
+#include <algorithm>
 #include <climits>
 #include <cmath>
+#include <type_traits>
 
 #include "mbx_common.cuh"
 #include "mbx_host.hpp"
@@ -43,6 +45,15 @@ constexpr int CB_THREADS = 256;
 constexpr int CB_WARPS = CB_THREADS / 32;
 constexpr int CB_LOADS = 8;  // loads in flight per lane in the accumulation walk
 constexpr int CB_PAD = 32;   // padding records after a pass's last record: the parallel walk reads U * PPW <= 32 ahead
+constexpr int CB_MAX_PASSES = 64;  // passes of one tile a planned list can hold (more: the tile is not planned)
+
+// Shared-memory layout of a channel-block tile for one pass size (offsets in 4-byte words).
+struct CbLayout {
+    int cap;   // records per pass
+    int fill;  // the scan stops adding pixels once a pass holds more than this many
+    int o_rec, o_rec2, o_sbin, o_ubin, o_bstart, o_run, o_wcnt, o_wstart, o_cone, o_hl, o_misc, o_win;
+    size_t smem;
+};
 
 struct CbPlan {
     int nb;          // channels per block
@@ -52,14 +63,13 @@ struct CbPlan {
     int row_passes;  // ceil(R / (rl * rpl))
     int rpad;        // row_passes * rl * rpl
     int pitch;       // tile row pitch (nb + 1)
-    int cap;         // records per pass
-    int fill;        // the scan stops adding pixels once a pass holds more than this many
     int nbins;       // nb + 2
     int cblocks;     // channel blocks per view
     int minb;        // resident CTAs per SM the kernel variant is compiled for (2 or 3)
-    // shared-memory layout (4-byte words)
-    int o_rec, o_rec2, o_sbin, o_ubin, o_bstart, o_run, o_wcnt, o_wstart, o_cone, o_hl, o_misc, o_win;
-    size_t smem;
+    CbLayout walk;   // scan, sort and walk passes of walk.cap records (also the build of stored passes)
+    CbLayout replay; // replay of stored passes (of walk.cap records): the tile, records, bins and bin starts only,
+                     // which leaves the rest of the SM's shared memory to the L1 cache that serves the row loads
+    CbLayout small;  // a walk that fits replay.smem: the tiles a build could not store, walked by the replay kernel
     bool ok;
 };
 
@@ -69,43 +79,89 @@ struct CbPlan {
 __host__ __device__ constexpr int cb_cone_records(int rpl) { return (CB_LOADS / rpl) > 0 ? (CB_LOADS / rpl) : 1; }
 __host__ __device__ constexpr int cb_cone_window(int ppw, int rpl) { return (3 * rpl * (32 / ppw)) / 2 + 4; }
 
-inline size_t cb_layout(CbPlan &pl, int kind, int R) {
+// Walk layout for passes of cap records: tile copies, sorted records (+ the cone's second words), bins, scan
+// order, bin starts, histogram, per-warp counts and starts, cone row tables, chunk hit list, warp counts, cone
+// slice windows.
+inline CbLayout cb_layout(const CbPlan &pl, int kind, int R, int cap) {
+    CbLayout lo = {};
+    lo.cap = cap;
+    lo.fill = cap - CB_THREADS;
     size_t o = (size_t)pl.ppw * pl.rpad * pl.pitch;
     o = (o + 3) & ~(size_t)3;
-    pl.o_rec = (int)o;
-    o += 4 * (size_t)(pl.cap + CB_PAD);
-    pl.o_rec2 = (int)o;
-    if (kind != MBX_GEOM_PARALLEL) o += 4 * (size_t)pl.cap;
-    pl.o_sbin = (int)o;
-    o += pl.cap + CB_PAD;
-    pl.o_ubin = (int)o;
-    o += pl.cap;
-    pl.o_bstart = (int)o;
+    lo.o_rec = (int)o;
+    o += 4 * (size_t)(cap + CB_PAD);
+    lo.o_rec2 = (int)o;
+    if (kind != MBX_GEOM_PARALLEL) o += 4 * (size_t)cap;
+    lo.o_sbin = (int)o;
+    o += cap + CB_PAD;
+    lo.o_ubin = (int)o;
+    o += cap;
+    lo.o_bstart = (int)o;
     o += pl.nbins + 1;
-    pl.o_run = (int)o;
+    lo.o_run = (int)o;
     o += pl.nbins;
-    pl.o_wcnt = (int)o;
+    lo.o_wcnt = (int)o;
     o += (size_t)CB_WARPS * pl.nbins;
-    pl.o_wstart = (int)o;
+    lo.o_wstart = (int)o;
     o += (size_t)CB_WARPS * pl.nbins;
-    pl.o_cone = (int)o;
+    lo.o_cone = (int)o;
     if (kind != MBX_GEOM_PARALLEL) o += 3 * (size_t)R;
-    pl.o_hl = (int)o;
+    lo.o_hl = (int)o;
     o += CB_THREADS;
-    pl.o_misc = (int)o;
+    lo.o_misc = (int)o;
     o += 3 * CB_WARPS;
-    pl.o_win = (int)o;
+    lo.o_win = (int)o;
     if (kind != MBX_GEOM_PARALLEL)
         o += (size_t)CB_WARPS * cb_cone_records(pl.rpl) * pl.ppw * cb_cone_window(pl.ppw, pl.rpl);
-    return o * 4;
+    lo.smem = o * 4;
+    return lo;
+}
+
+// Replay layout for stored passes of cap records: what the walk of a pass reads (tile copies, records, bins, bin
+// starts, cone row tables and slice windows), none of the scan and sort buffers.
+inline CbLayout cb_layout_replay(const CbPlan &pl, int kind, int R, int cap) {
+    CbLayout lo = {};
+    lo.cap = cap;
+    lo.fill = cap - CB_THREADS;
+    size_t o = (size_t)pl.ppw * pl.rpad * pl.pitch;
+    o = (o + 3) & ~(size_t)3;
+    lo.o_rec = (int)o;
+    o += 4 * (size_t)(cap + CB_PAD);
+    lo.o_rec2 = (int)o;
+    if (kind != MBX_GEOM_PARALLEL) o += 4 * (size_t)cap;
+    lo.o_sbin = (int)o;
+    o += cap + CB_PAD;
+    lo.o_bstart = (int)o;
+    o += pl.nbins + 1;
+    lo.o_cone = (int)o;
+    if (kind != MBX_GEOM_PARALLEL) o += 3 * (size_t)R;
+    lo.o_win = (int)o;
+    if (kind != MBX_GEOM_PARALLEL)
+        o += (size_t)CB_WARPS * cb_cone_records(pl.rpl) * pl.ppw * cb_cone_window(pl.ppw, pl.rpl);
+    lo.o_ubin = lo.o_run = lo.o_wcnt = lo.o_wstart = lo.o_hl = lo.o_misc = 0;  // scan and sort buffers: unused
+    lo.smem = o * 4;
+    return lo;
+}
+
+// The replay layout of a plan, and the walk that fits it (the largest pass size, down to 256 records; the replay
+// layout grows to the 256-record walk when even that does not fit).
+inline void cb_plan_replay(CbPlan &pl, int kind, int R) {
+    pl.replay = cb_layout_replay(pl, kind, R, pl.walk.cap);
+    for (int cap = pl.walk.cap / 2; cap >= CB_THREADS; cap >>= 1) {
+        pl.small = cb_layout(pl, kind, R, cap);
+        if (pl.small.smem <= pl.replay.smem) return;
+    }
+    pl.small = cb_layout(pl, kind, R, CB_THREADS);
+    pl.replay.smem = std::max(pl.replay.smem, pl.small.smem);
 }
 
 // num_views_sel: views per call (0 = all); min_blocks: CTAs wanted per call (a narrower channel block is
 // chosen to reach it); 0 = widest block.  minb: 2 (first shared-memory tier 112 KB) or 3 (74 KB, for the kernel
 // variant compiled for three resident CTAs per SM); nb_max: widest channel block allowed.
 // avoid_ppw: when nonzero, the best lane layout with a different number of sub-groups (an autotuner candidate).
+// max_cap: most records per pass.
 inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min_blocks = 0, int minb = 2,
-                         int nb_max = 128, int avoid_ppw = 0) {
+                         int nb_max = 128, int avoid_ppw = 0, int max_cap = 2048) {
     CbPlan pl = {};
     pl.minb = minb;
     // translation geometry: radius 1 in both fans, and a magnification bound from the host (which also says that
@@ -139,16 +195,14 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
         for (int nb = nb_max; nb >= 32 && !found; nb >>= 1) {
             const long long nv = num_views_sel > 0 ? num_views_sel : g.num_views;
             if (nb > 32 && min_blocks > 0 && (long long)ceil_div(C, nb) * nv < min_blocks) continue;
-            for (int cap = 2048; cap >= 512 && !found; cap >>= 1) {
+            for (int cap = max_cap; cap >= 512 && !found; cap >>= 1) {
                 CbPlan q = pl;
                 q.nb = nb;
                 q.pitch = nb + 1;
-                q.cap = cap;
                 q.nbins = nb + 2;
-                q.fill = cap - CB_THREADS;
                 q.cblocks = ceil_div(C, nb);
-                q.smem = cb_layout(q, g.kind, R);
-                if (q.smem <= tiers[t]) {
+                q.walk = cb_layout(q, g.kind, R, cap);
+                if (q.walk.smem <= tiers[t]) {
                     pl = q;
                     found = true;
                 }
@@ -156,6 +210,7 @@ inline CbPlan plan_fp_cb(const mbx_geom &g, int num_views_sel = 0, long long min
         }
     }
     if (!found) pl.ok = false;
+    if (found) cb_plan_replay(pl, g.kind, R);
     if ((long long)g.num_recon_rows * g.num_recon_cols > (1LL << 24)) pl.ok = false;  // bin and index share a word
     if (g.kind == MBX_GEOM_CONE) {
         const double half_r = 0.5 * (g.num_recon_rows - 1), half_c = 0.5 * (g.num_recon_cols - 1);
@@ -617,24 +672,35 @@ __device__ __forceinline__ void ldg_if(float &v, const float *p, int ok) {
         : "l"(p), "r"(ok));
 }
 
+#ifndef MBX_FPCB_LOADS2
+#define MBX_FPCB_LOADS2 16  // parallel walk: row loads in flight per lane, variant for 2 CTAs per SM
+#endif
+#ifndef MBX_FPCB_LOADS3
+#define MBX_FPCB_LOADS3 16  // the same, variant for 3 CTAs per SM (85 registers)
+#endif
+
 // Parallel-beam accumulation of one pass by one warp (same contract and record interleaving as cb_accumulate).
 // Slice m of a cylinder is detector row m, so a lane's rows are one base pointer plus fixed strides and each
-// record costs one address computation; rows past the last detector row are predicated off.  The records after
-// a warp's range (the next warp's, or the pass's padding) are read but contribute nothing, so the walk needs no
-// clamping.  Running sums: before bin bc completes, ca[] / cbb[] / cc[] hold channels bc-2, bc-1, bc;
-// completing bin bc finishes channel bc-2.  Only the first two channels finished in the walk can be shared with
-// the warp below (E0, E1), and only the last two of the final flush with the warp above (E2, E3).
-// (Measured alternatives that ran no faster: sub-groups walking whole bins of their own, which diverge at every
-// bin end; a walk split into edge, guard-free and tail loops.)
+// record costs one address computation; rows past the last detector row are predicated off.  Running sums:
+// before bin bc completes, ca[] / cbb[] / cc[] hold channels bc-2, bc-1, bc; completing bin bc finishes channel
+// bc-2.  Only the first two channels finished in the walk can be shared with the warp below (E0, E1), and only
+// the last two of the final flush with the warp above (E2, E3).
+// The walk is bound by the latency of the row loads.  Each loop iteration first issues the row loads of U records
+// (reading only the cylinder offset of each record), then, as the values arrive, reads each record's coefficients
+// and bin from shared memory again and accumulates, so only the loaded values stay in registers across the load
+// latency (4% faster on the batched replay stage than keeping the records live).  Full iterations run unguarded;
+// the last one of a sub-group clamps its record positions to the warp's range and skips the clamped ones.
+// Measured and dropped: more loads in flight (24 or 32 per lane: 30% and 70% slower; the SM's L1 left beside the
+// shared memory of two CTAs thrashes), the row loads without L1 allocation or cached in L2 only (37% and 4%
+// slower), one guarded loop instead of the unguarded loop and a tail (10% slower), sub-groups walking whole bins
+// of their own (they diverge at every bin end).
 template <int PPW, int RPL, int MINB>
 __device__ __forceinline__ void cb_accumulate_par(const FpArgs &A, const CbPass &P, int warp, int lane) {
     const mbx_geom &g = A.g;
     const CbPlan &pl = A.plan;
     constexpr int RL = 32 / PPW;
-    // records prefetched per lane: about 16 row loads in flight (the walk is latency-bound), at most 8 records;
-    // the variant for three CTAs per SM (85 registers) keeps CB_LOADS, which it holds without spilling
-    constexpr int LOADS = MINB >= 3 ? CB_LOADS : 16;
-    constexpr int U = (LOADS / RPL) < 1 ? 1 : ((LOADS / RPL) > 8 ? 8 : (LOADS / RPL));
+    constexpr int LOADS = MINB >= 3 ? MBX_FPCB_LOADS3 : MBX_FPCB_LOADS2;
+    constexpr int U = (LOADS / RPL) < 1 ? 1 : ((LOADS / RPL) > 32 ? 32 : (LOADS / RPL));
     const int sub = lane / RL, lr = lane % RL;
     const int num_rows = g.num_det_rows, nb = pl.nb, pitch = pl.pitch;
     const int w_lo = P.bstart[P.b_lo], w_hi = P.bstart[P.b_hi];
@@ -667,37 +733,40 @@ __device__ __forceinline__ void cb_accumulate_par(const FpArgs &A, const CbPass 
             }
             ++bc;
         };
-        const float4 *rp4 = P.rec + r_a;
-        const int *bp = P.sbin + r_a;
         float vq[U][RPL];
 #pragma unroll
         for (int u = 0; u < U; ++u)
 #pragma unroll
-            for (int j = 0; j < RPL; ++j) vq[u][j] = 0.0f;
-        for (int i = r_a; i < r_b; i += U * PPW, rp4 += U * PPW, bp += U * PPW) {
-            float4 rq[U];
-            int bq[U];
+            for (int j = 0; j < RPL; ++j) vq[u][j] = 0.0f;  // rows past R keep a finite value (never written out)
+        // one iteration: records i, i + PPW, ..., i + (U-1) PPW of the sub-group (CLAMP: the last, partial one)
+        auto iteration = [&](int i, auto clamp) {
+            constexpr bool CLAMP = decltype(clamp)::value;
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                rq[u] = rp4[u * PPW];
-                bq[u] = bp[u * PPW];
-                const float *cyl = base + __float_as_int(rq[u].x);  // 32-bit element offset of the cylinder
+                const int ii = CLAMP ? min(i + u * PPW, r_b - 1) : i + u * PPW;
+                const float *cyl = base + __float_as_int(P.rec[ii].x);  // 32-bit element offset of the cylinder
 #pragma unroll
                 for (int j = 0; j < RPL; ++j) ldg_if(vq[u][j], cyl + j * RL, ok[j]);
             }
 #pragma unroll
             for (int u = 0; u < U; ++u) {
-                if (i + u * PPW < r_b) {
-                    while (bc < bq[u]) finish();
+                const int ii = i + u * PPW;
+                if (!CLAMP || ii < r_b) {
+                    const float4 rq = P.rec[ii];
+                    const int bq = P.sbin[ii];
+                    while (bc < bq) finish();
 #pragma unroll
                     for (int j = 0; j < RPL; ++j) {
-                        ca[j] = fmaf(rq[u].y, vq[u][j], ca[j]);
-                        cbb[j] = fmaf(rq[u].z, vq[u][j], cbb[j]);
-                        cc[j] = fmaf(rq[u].w, vq[u][j], cc[j]);
+                        ca[j] = fmaf(rq.y, vq[u][j], ca[j]);
+                        cbb[j] = fmaf(rq.z, vq[u][j], cbb[j]);
+                        cc[j] = fmaf(rq.w, vq[u][j], cc[j]);
                     }
                 }
             }
-        }
+        };
+        int i = r_a;
+        for (; i + (U - 1) * PPW < r_b; i += U * PPW) iteration(i, std::false_type{});
+        if (i < r_b) iteration(i, std::true_type{});
         // final flush: channels bc-2, bc-1, bc; the ones above b_hi - 3 are shared with the warp above
         float e2[RPL], e3[RPL];
 #pragma unroll
@@ -744,8 +813,8 @@ __device__ __forceinline__ void cb_accumulate_par(const FpArgs &A, const CbPass 
 // sorts them and stores the sorted record passes in a CbPlanned list instead of walking them; replay, which walks
 // the stored passes (no scan, no sort).  A planned list is built once for a pixel list and replayed as often as
 // the same list is projected again with new voxel values (every iteration of a VCD reconstruction).
-enum { CB_WALK = 0, CB_BUILD = 1, CB_REPLAY = 2 };
-constexpr int CB_MAX_PASSES = 64;  // passes of one tile a planned list can hold (more: the tile is not planned)
+// CB_WALK_SMALL is the walk in the replay layout's shared memory (plan.small), for the tiles a build could not store.
+enum { CB_WALK = 0, CB_BUILD = 1, CB_REPLAY = 2, CB_WALK_SMALL = 3 };
 
 // Stored sorted record passes of every tile of one pixel list (device storage carved by the caller).  Records and
 // pass slots are taken from bump cursors (reset before a build), so their placement depends on scheduling, but
@@ -774,23 +843,24 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, 
     const int tid = threadIdx.x, lane = tid & 31, warp = tid >> 5;
     const int num_rows = g.num_det_rows, num_channels = g.num_det_channels, num_slices = g.num_recon_slices;
     const int nb = pl.nb, nbins = pl.nbins, n0 = cb * nb;
+    const CbLayout &Lo = MODE == CB_REPLAY ? pl.replay : (MODE == CB_WALK_SMALL ? pl.small : pl.walk);
 
     float *tile = sm;  // [ppw][rpad][pitch]
-    float4 *rec = reinterpret_cast<float4 *>(sm + pl.o_rec);    // sorted {cylinder offset (int bits), a0, a1, a2}
-    float4 *rec2 = reinterpret_cast<float4 *>(sm + pl.o_rec2);  // cone: sorted {imd, W_r, mdz, mz0}
-    int *sbin = reinterpret_cast<int *>(sm + pl.o_sbin);        // bin of each sorted record
-    int *ubin = reinterpret_cast<int *>(sm + pl.o_ubin);        // kept pixels, scan order: bin << 24 | key
+    float4 *rec = reinterpret_cast<float4 *>(sm + Lo.o_rec);    // sorted {cylinder offset (int bits), a0, a1, a2}
+    float4 *rec2 = reinterpret_cast<float4 *>(sm + Lo.o_rec2);  // cone: sorted {imd, W_r, mdz, mz0}
+    int *sbin = reinterpret_cast<int *>(sm + Lo.o_sbin);        // bin of each sorted record
+    int *ubin = reinterpret_cast<int *>(sm + Lo.o_ubin);        // kept pixels, scan order: bin << 24 | key
                                                                 // (key: pixel index when vox is indexed by pixel,
                                                                 // else list position; both < 2^24)
-    int *bstart = reinterpret_cast<int *>(sm + pl.o_bstart);    // [nbins + 1] padded start of each bin
-    int *run = reinterpret_cast<int *>(sm + pl.o_run);          // [nbins] histogram, then placement cursor
-    int *wcnt = reinterpret_cast<int *>(sm + pl.o_wcnt);        // [warps][nbins] per-warp counts of a chunk
-    int *wstart = reinterpret_cast<int *>(sm + pl.o_wstart);    // [warps][nbins] per-warp start positions
-    float *s_vm = sm + pl.o_cone;                               // cone: [R] detector height of each row centre
+    int *bstart = reinterpret_cast<int *>(sm + Lo.o_bstart);    // [nbins + 1] padded start of each bin
+    int *run = reinterpret_cast<int *>(sm + Lo.o_run);          // [nbins] histogram, then placement cursor
+    int *wcnt = reinterpret_cast<int *>(sm + Lo.o_wcnt);        // [warps][nbins] per-warp counts of a chunk
+    int *wstart = reinterpret_cast<int *>(sm + Lo.o_wstart);    // [warps][nbins] per-warp start positions
+    float *s_vm = sm + Lo.o_cone;                               // cone: [R] detector height of each row centre
     float *s_vb = s_vm + num_rows;                              // cone: [R] same at the row's 128-row batch start
     int *s_b0 = reinterpret_cast<int *>(s_vb + num_rows);       // cone: [R] batch start row
-    int *hl = reinterpret_cast<int *>(sm + pl.o_hl);            // chunks of the current segment that can hit
-    int *s_misc = reinterpret_cast<int *>(sm + pl.o_misc);      // [2][warps]: warp counts, double-buffered;
+    int *hl = reinterpret_cast<int *>(sm + Lo.o_hl);            // chunks of the current segment that can hit
+    int *s_misc = reinterpret_cast<int *>(sm + Lo.o_misc);      // [2][warps]: warp counts, double-buffered;
                                                                 // [2][warps]: hit counts of a segment
 
     const int vi = A.views ? A.views[j] : j;
@@ -816,7 +886,8 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, 
     __syncthreads();  // previous tile of this CTA (batched use) is finished with shared memory
     const int tile_words = pl.ppw * pl.rpad * pl.pitch;
     for (int i = tid; i < tile_words; i += CB_THREADS) tile[i] = 0.0f;
-    for (int i = tid; i < CB_WARPS * nbins; i += CB_THREADS) wcnt[i] = 0;
+    if (MODE != CB_REPLAY)
+        for (int i = tid; i < CB_WARPS * nbins; i += CB_THREADS) wcnt[i] = 0;
     if (KIND != MBX_GEOM_PARALLEL) {
         int rows_per_batch = g.entries_per_cylinder_batch;
         if (rows_per_batch > num_rows) rows_per_batch = num_rows;
@@ -869,7 +940,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, 
         P.s_vm = s_vm;
         P.s_vb = s_vb;
         P.s_b0 = s_b0;
-        P.win = sm + pl.o_win;
+        P.win = sm + Lo.o_win;
         if (KIND == MBX_GEOM_PARALLEL) {
             switch (pl.ppw * 8 + pl.rpl) {  // the lane layouts plan_fp_cb chooses from
                 case 9: cb_accumulate_par<1, 1, MINB>(A, P, warp, lane); break;
@@ -916,7 +987,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, 
             if (ps >= 0 && ps < PL->pass_cap) {  // never written by a build otherwise
                 cnt = PL->pass_count[ps];
                 rs = PL->pass_rec[ps];
-                if (cnt < 0 || cnt > pl.cap || rs < 0 || rs + cnt > PL->rec_cap) cnt = -1;
+                if (cnt < 0 || cnt > Lo.cap || rs < 0 || rs + cnt > PL->rec_cap) cnt = -1;
             }
             s_pslot[q] = ps;
             s_pcnt[q] = cnt;
@@ -981,7 +1052,7 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, 
         __syncthreads();
         // ---- 1. ordered compaction of the pixels that touch this channel block
         int count = 0, par = 0;
-        while (count <= pl.fill) {
+        while (count <= Lo.fill) {
             if (hp == nh) {
                 if (seg >= nchunks) {
                     more = false;

@@ -24,172 +24,14 @@
 // mbx_vcd_batched_refresh rewrite, so a prepared plan, and graphs captured from it, serve every call of a batch
 // shape.
 #include <algorithm>
+#include <cmath>
 #include <cstring>
 #include <vector>
 
-#include "back_project.cuh"
-#include "bp_fast.cuh"
 #include "direct_filter.cuh"
-#include "fp_cb.cuh"
-#include "mbx_common.cuh"
-#include "mbx_host.hpp"
-#include "mbx_reduce.cuh"
-#include "qggmrf.cuh"
+#include "vcd_batched.cuh"
 
 namespace mbx {
-
-constexpr int BT_THREADS = 256;
-constexpr int BT_ELEM_TILE = 2048;   // cylinder elements per tile (delta, apply)
-constexpr int BT_SINO_TILE = 4096;   // sinogram / recon elements per tile (linquad, error, stats)
-constexpr float BT_EPS_F32 = 1.1920928955078125e-07f;
-
-struct VcdScan {
-    float *recon;               // flat (Nr*Nc, S)
-    float *err;                 // (V, R, C)
-    const float *wts;           // (V, R, C) or NULL
-    float *hess;                // flat (Nr*Nc, S)
-    const int32_t *partition;   // (K, M)
-    float *bp, *delta, *dsino;  // workspace slices
-    const float *y;             // measured sinogram (set-up input) or NULL
-    long long nsino, nrecon;
-    int K, M, nr, nc, ns;
-};
-
-// Direct-recon filtering of one scan in the set-up: rows of y into err.
-struct FiltScan {
-    const float *in;
-    float *out;
-    long long rows;
-    int R, C, fdk;
-    double filter_scale, out_scale, D, ddc, ddr, dco, dro;
-};
-
-// A work list of projection tiles over the scans of a batch: per scan, its argument record(s) and tile count.
-// Tiles are numbered over the scans in `order` (decreasing per-tile cost) and handed out dynamically.
-struct ProjList {
-    const BpArgs *bp;      // back-projection records (or NULL)
-    const FpArgs *fp;      // forward-projection records (or NULL)
-    const int *off;        // [num_scans + 1] tile prefix over the positions of `order`
-    const int *dim;        // [num_scans] per scan: gx (back projection) or channel blocks (forward)
-    const int *order;      // [num_scans] scan at each position
-    const int *schedule;   // [num_steps][num_scans] record of each scan at each step, or NULL (record 0)
-    int stride;            // records per scan
-    int *counter;          // next tile (reset by a memset before each launch)
-    const CbPlanned *planned;  // forward lists: stored record passes of each record, or NULL (walk every tile)
-};
-
-// Projection work lists of a batch.  PL_BUILD covers every (scan, subset, view, channel block) tile: the builds
-// of the planned forward projections.
-enum { PL_BP = 0, PL_FP, PL_INIT_BP, PL_INIT_FP, PL_HESS, PL_BUILD, PL_COUNT };
-
-struct BatchedTables {
-    VcdScan *scans;
-    float *fm;          // [scan] 1 / sigma_y^2 (per call)
-    QParams *qp;        // [scan] qGGMRF parameters (per call)
-    BpArgs *bpargs;     // [scan][subset]
-    FpArgs *fpargs;     // [scan][subset]
-    BpArgs *init_bp;    // [scan]: filtered sinogram -> recon over the region of reconstruction
-    FpArgs *init_fp;    // [scan]: recon -> dsino over the region of reconstruction
-    BpArgs *hess_bp;    // [scan]: weights (or ones) -> Hessian over every pixel, squared coefficients
-    FiltScan *filt;     // [scan]
-    CbPlanned *planned; // [scan][subset] stored record passes of the subset forward projections (planned batches)
-    int *pl_off;        // [PL_COUNT][num_scans + 1]
-    int *pl_dim;        // [PL_COUNT][num_scans]
-    int *pl_order;      // [PL_COUNT][num_scans]
-    int *el_off, *sn_off, *rc_off, *flt_off;  // [num_scans + 1] tile prefix offsets (scan order)
-    int *box_first;     // [num_scans * K + 1] chunk prefix over (scan, subset) records
-    int *counters;      // [PL_COUNT]
-    int *schedule;      // [num_steps][num_scans]
-    double *p_prior, *p_fwd, *p_l1, *p_iter, *p_init;
-    float *alpha;       // [num_scans]
-    float *alpha_init;  // [num_scans]
-    double *step_stats; // [num_steps][num_scans][4]
-    double *iter_stats; // [num_iterations][num_scans][4]
-};
-
-struct BatchedPlanHost {
-    BatchedTables t;
-    int num_scans, kind, num_steps, num_iterations, ksum, has_setup;
-    int planned_fp;                 // subset forward projections replay stored record passes
-    int pl_grid_replay, pl_grid_build;  // grids of the replay and build kernels (variant fp_minb)
-    void *plan_cursors;             // [ksum] bump cursors of the planned lists (one memset resets them)
-    size_t plan_cursor_bytes;
-    int pl_total[PL_COUNT], pl_grid[PL_COUNT];
-    size_t pl_smem[PL_COUNT];
-    int el_total, sn_total, rc_total, flt_total, box_total;
-    int el_grid, sn_grid, rc_grid, flt_grid, box_grid;
-    size_t flt_smem;
-    int fp_minb;  // b_fp variant of the subset stage: 2 or 3 resident CTAs per SM
-    int magic;
-};
-static_assert(sizeof(BatchedPlanHost) <= sizeof(mbx_batched_plan), "plan record too large");
-constexpr int BT_MAGIC = 0x6d627863;
-
-static ProjList proj_list(const BatchedTables &T, int which, int num_scans) {
-    ProjList L;
-    L.bp = which == PL_BP ? T.bpargs : which == PL_INIT_BP ? T.init_bp : which == PL_HESS ? T.hess_bp : nullptr;
-    L.fp = which == PL_FP ? T.fpargs : which == PL_INIT_FP ? T.init_fp : nullptr;
-    L.off = T.pl_off + which * (num_scans + 1);
-    L.dim = T.pl_dim + which * num_scans;
-    L.order = T.pl_order + which * num_scans;
-    const bool subsets = which == PL_BP || which == PL_FP;
-    L.schedule = subsets ? T.schedule : nullptr;
-    L.stride = 0;  // set by the caller (the number of subsets for the subset lists)
-    L.counter = T.counters + which;
-    L.planned = nullptr;
-    return L;
-}
-
-__device__ __forceinline__ int find_scan(const int *__restrict__ off, int num_scans, int t) {
-    int lo = 0, hi = num_scans;  // off[lo] <= t < off[hi]
-    while (hi - lo > 1) {
-        const int mid = (lo + hi) >> 1;
-        if (__ldg(off + mid) <= t) lo = mid; else hi = mid;
-    }
-    return lo;
-}
-
-// Sum of NV values over the block into slot[NV * t + i] (fixed order).
-template <int NV>
-__device__ __forceinline__ void tile_reduce(const double (&v)[NV], double *slot) {
-    __shared__ double sh[32][NV];
-    const int lane = threadIdx.x & 31, warp = threadIdx.x >> 5;
-#pragma unroll
-    for (int i = 0; i < NV; ++i) {
-        const double a = warp_sum(v[i]);
-        if (lane == 0) sh[warp][i] = a;
-    }
-    __syncthreads();
-    if (warp == 0) {
-#pragma unroll
-        for (int i = 0; i < NV; ++i) {
-            double a = lane < BT_THREADS / 32 ? sh[lane][i] : 0.0;
-            a = warp_sum(a);
-            if (lane == 0) slot[i] = a;
-        }
-    }
-    __syncthreads();
-}
-
-// Next tile of a dynamically scheduled work list (one atomic per CTA per tile).
-__device__ __forceinline__ int fetch_tile(int *counter) {
-    __shared__ int s_next;
-    __syncthreads();  // every thread is done with the previous tile index
-    if (threadIdx.x == 0) s_next = atomicAdd(counter, 1);
-    __syncthreads();
-    return s_next;
-}
-
-#ifndef MBX_BBP_MIN_BLOCKS
-#define MBX_BBP_MIN_BLOCKS 3  // resident CTAs per SM the batched back projection is compiled for
-#endif
-
-// Record of scan s in a work list at a step.
-template <class A>
-__device__ __forceinline__ const A &list_record(const A *recs, const ProjList &L, int num_scans, int step, int s) {
-    const int r = L.schedule ? __ldg(L.schedule + step * num_scans + s) : 0;
-    return recs[s * L.stride + r];
-}
 
 template <int KIND>
 __global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(ProjList L, int num_scans, int step, int first, int total, int *err) {
@@ -200,58 +42,6 @@ __global__ void __launch_bounds__(BPF_THREADS, MBX_BBP_MIN_BLOCKS) b_bp(ProjList
         const int local = t - __ldg(L.off + k);
         const int gx = __ldg(L.dim + s);
         bp_fast_tile<KIND>(list_record(L.bp, L, num_scans, step, s), local % gx, local / gx, 0, smb, err);
-    }
-}
-
-// MINB: resident CTAs per SM the variant is compiled for (2 or 3, matching the plans' fp_cb minb).
-template <int KIND, int MINB>
-__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp(ProjList L, int num_scans, int step, int first, int total, int *err) {
-    extern __shared__ __align__(16) float smf2[];
-    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
-        const int k = find_scan(L.off, num_scans, t);
-        const int s = __ldg(L.order + k);
-        const int local = t - __ldg(L.off + k);
-        const int cbs = __ldg(L.dim + s);
-        fp_cb_tile<KIND, MINB>(list_record(L.fp, L, num_scans, step, s), local / cbs, local % cbs, smf2, err);
-    }
-}
-
-// Subset forward projection from stored record passes: the tile's passes are walked as stored (no scan, no
-// sort); a tile the build could not store is projected by the walk.
-template <int KIND, int MINB>
-__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp_replay(ProjList L, int num_scans, int step, int first, int total, int *err) {
-    extern __shared__ __align__(16) float smf3[];
-    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
-        const int k = find_scan(L.off, num_scans, t);
-        const int s = __ldg(L.order + k);
-        const int local = t - __ldg(L.off + k);
-        const int cbs = __ldg(L.dim + s);
-        const int r = L.schedule ? __ldg(L.schedule + step * num_scans + s) : 0;
-        const FpArgs &A = L.fp[s * L.stride + r];
-        const CbPlanned &pc = L.planned[s * L.stride + r];
-        const int view = local / cbs, cb = local % cbs;
-        const long long ptile = local;  // view * cbs + cb
-        if (pc.tile_npass[ptile] >= 0)
-            fp_cb_tile<KIND, MINB, CB_REPLAY>(A, view, cb, smf3, err, &pc, ptile);
-        else
-            fp_cb_tile<KIND, MINB, CB_WALK>(A, view, cb, smf3, err);
-    }
-}
-
-// Builds of the planned forward projections: every (scan, subset, view, channel block) tile scans and sorts its
-// pixels and stores the sorted passes.
-template <int KIND, int MINB>
-__global__ void __launch_bounds__(CB_THREADS, MINB) b_fp_build(ProjList L, int num_scans, int first, int total, int *err) {
-    extern __shared__ __align__(16) float smf4[];
-    for (int t = first + fetch_tile(L.counter); t < total; t = first + fetch_tile(L.counter)) {
-        const int k = find_scan(L.off, num_scans, t);
-        const int s = __ldg(L.order + k);
-        const int local = t - __ldg(L.off + k);
-        const int cbs = __ldg(L.dim + s);
-        const int per_subset = L.fp[s * L.stride].num_views_sel * cbs;
-        const int sub = local / per_subset, r = local - sub * per_subset;
-        fp_cb_tile<KIND, MINB, CB_BUILD>(L.fp[s * L.stride + sub], r / cbs, r % cbs, smf4, err,
-                                         L.planned + s * L.stride + sub, r);
     }
 }
 
@@ -541,6 +331,7 @@ struct ScanSizes {
     CbPlan fpp;   // subset (and initial) forward projection
     BpfPlan ibp;  // initial back projection over the region of reconstruction
     BpfPlan hbp;  // Hessian back projection over every pixel
+    int hbp_slices;  // > 0: hbp is planned on one slice and broadcast to this many (unit-weight parallel beam)
     bool setup;   // the scan carries the set-up inputs
 };
 
@@ -552,7 +343,7 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
     if (sc.num_subsets <= 0 || sc.subset_size <= 0) return MBX_ERR_INVALID_ARG;
     if (!(sc.qp.sigma_x > 0.0f) || !(sc.qp.T > 0.0f) || !(sc.qp.p > 0.0f)) return MBX_ERR_INVALID_ARG;
     z.bpp = plan_bp_fast(g, sc.subset_size, g.num_views);
-    z.fpp = plan_fp_cb(g);
+    z.fpp = plan_fp_cb(g, 0, 0, 2, 128, 0, MBX_BATCHED_FP_CAP);
     if (!z.bpp.ok || !z.fpp.ok) return MBX_ERR_UNSUPPORTED;  // batched path needs the radius-1 kernels
     if ((long long)sc.subset_size * g.num_recon_slices >= (1LL << 31)) return MBX_ERR_UNSUPPORTED;
     if (sc.subset_size > (1 << 24)) return MBX_ERR_UNSUPPORTED;  // list positions share a word with the bin
@@ -570,7 +361,12 @@ static int scan_sizes(const mbx_scan &sc, ScanSizes &z) {
             return MBX_ERR_INVALID_ARG;
         // the initial forward projection reads voxels by pixel index, which shares a word with the bin
         if (z.npix > (1 << 24) || z.nrecon >= (1LL << 31)) return MBX_ERR_UNSUPPORTED;
-        z.hbp = plan_bp_fast(g, z.npix, g.num_views);
+        z.hbp_slices = 0;
+        if (bp_unit_broadcast(g, nullptr, sc.weights)) {  // unit-weight parallel Hessian: one slice, broadcast
+            z.hbp = plan_bp_fast(one_slice_geometry(g), z.npix, g.num_views);
+            if (z.hbp.ok && z.hbp.splits == 1) z.hbp_slices = g.num_recon_slices;
+        }
+        if (z.hbp_slices == 0) z.hbp = plan_bp_fast(g, z.npix, g.num_views);
         if (!z.hbp.ok) return MBX_ERR_UNSUPPORTED;
         if (g.kind != MBX_GEOM_TRANSLATION) {  // translation geometry starts from zeros (no direct recon)
             if (filter_smem_bytes(g.num_det_channels, g.kind != MBX_GEOM_PARALLEL) > 200 * 1024)
@@ -757,28 +553,48 @@ static const void *bp_kernel_of(int kind) {
                                      : reinterpret_cast<const void *>(b_bp<MBX_GEOM_TRANSLATION>);
 }
 
-// The forward stage kernels: mode CB_WALK (b_fp), CB_REPLAY (b_fp_replay) or CB_BUILD (b_fp_build).
-template <int KIND>
-static const void *fp_kernel_mode(int minb, int mode) {
-    if (mode == CB_REPLAY)
-        return minb >= 3 ? reinterpret_cast<const void *>(b_fp_replay<KIND, 3>)
-                         : reinterpret_cast<const void *>(b_fp_replay<KIND, 2>);
-    return minb >= 3 ? reinterpret_cast<const void *>(b_fp_build<KIND, 3>)
-                     : reinterpret_cast<const void *>(b_fp_build<KIND, 2>);
+// The forward stage kernels of each geometry kind (compiled in b_fp_parallel.cu, b_fp_cone.cu, b_fp_translation.cu).
+const void *fp_stage_kernel_parallel(int minb, int mode);
+const void *fp_stage_kernel_cone(int minb, int mode);
+const void *fp_stage_kernel_translation(int minb, int mode);
+void launch_fp_stage_parallel(int minb, int mode, int grid, size_t smem, cudaStream_t st, const ProjList &L, int n,
+                              int step, int first, int total, int *err);
+void launch_fp_stage_cone(int minb, int mode, int grid, size_t smem, cudaStream_t st, const ProjList &L, int n,
+                          int step, int first, int total, int *err);
+void launch_fp_stage_translation(int minb, int mode, int grid, size_t smem, cudaStream_t st, const ProjList &L, int n,
+                                 int step, int first, int total, int *err);
+
+const void *fp_stage_kernel(int kind, int minb, int mode) {
+    return kind == MBX_GEOM_PARALLEL ? fp_stage_kernel_parallel(minb, mode)
+           : kind == MBX_GEOM_CONE   ? fp_stage_kernel_cone(minb, mode)
+                                     : fp_stage_kernel_translation(minb, mode);
 }
 
-static const void *fp_kernel_of(int kind, int minb, int mode = CB_WALK) {
-    if (mode != CB_WALK)
-        return kind == MBX_GEOM_PARALLEL ? fp_kernel_mode<MBX_GEOM_PARALLEL>(minb, mode)
-               : kind == MBX_GEOM_CONE   ? fp_kernel_mode<MBX_GEOM_CONE>(minb, mode)
-                                         : fp_kernel_mode<MBX_GEOM_TRANSLATION>(minb, mode);
-    if (minb >= 3)
-        return kind == MBX_GEOM_PARALLEL ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 3>)
-               : kind == MBX_GEOM_CONE   ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 3>)
-                                         : reinterpret_cast<const void *>(b_fp<MBX_GEOM_TRANSLATION, 3>);
-    return kind == MBX_GEOM_PARALLEL ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_PARALLEL, 2>)
-           : kind == MBX_GEOM_CONE   ? reinterpret_cast<const void *>(b_fp<MBX_GEOM_CONE, 2>)
-                                     : reinterpret_cast<const void *>(b_fp<MBX_GEOM_TRANSLATION, 2>);
+void launch_fp_stage(int kind, int minb, int mode, int grid, size_t smem, cudaStream_t st, const ProjList &L, int n,
+                     int step, int first, int total, int *err) {
+    if (kind == MBX_GEOM_PARALLEL)
+        launch_fp_stage_parallel(minb, mode, grid, smem, st, L, n, step, first, total, err);
+    else if (kind == MBX_GEOM_CONE)
+        launch_fp_stage_cone(minb, mode, grid, smem, st, L, n, step, first, total, err);
+    else
+        launch_fp_stage_translation(minb, mode, grid, smem, st, L, n, step, first, total, err);
+}
+
+// The forward stage kernel of a mode: CB_WALK (b_fp), CB_REPLAY (b_fp_replay) or CB_BUILD (b_fp_build).
+static const void *fp_kernel_of(int kind, int minb, int mode = CB_WALK) { return fp_stage_kernel(kind, minb, mode); }
+
+// Preferred shared-memory carveout of a kernel: what its resident CTAs of `threads` threads and smem bytes of
+// dynamic shared memory need (a hint; the driver rounds it up to a supported split of the SM's unified storage).
+static cudaError_t set_smem_carveout(const void *kern, int threads, size_t smem) {
+    int dev = 0, max_sm = 0, reserved = 0, per_sm = 0;
+    cudaError_t e = cudaGetDevice(&dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&max_sm, cudaDevAttrMaxSharedMemoryPerMultiprocessor, dev);
+    if (e == cudaSuccess) e = cudaDeviceGetAttribute(&reserved, cudaDevAttrReservedSharedMemoryPerBlock, dev);
+    if (e == cudaSuccess) e = cudaOccupancyMaxActiveBlocksPerMultiprocessor(&per_sm, kern, threads, smem);
+    if (e != cudaSuccess || max_sm <= 0 || per_sm <= 0) return e;
+    const double need = (double)per_sm * (double)(smem + (size_t)reserved);
+    const int pct = std::min(100, (int)std::ceil(100.0 * need / max_sm));
+    return cudaFuncSetAttribute(kern, cudaFuncAttributePreferredSharedMemoryCarveout, pct);
 }
 
 static int bp_grid(int kind, size_t smem, int total) {
@@ -807,18 +623,6 @@ static cudaError_t launch_bp_list(const BatchedPlanHost &P, int which, int step,
     return cudaGetLastError();
 }
 
-// One launch of a forward-projection work list (kernel variant for minb resident CTAs per SM).
-template <int KIND, int MINB>
-static void launch_fp_kernel(int mode, int grid, size_t smem, cudaStream_t st, const ProjList &L, int n, int step,
-                             int first, int total, int *err) {
-    if (mode == CB_REPLAY)
-        b_fp_replay<KIND, MINB><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
-    else if (mode == CB_BUILD)
-        b_fp_build<KIND, MINB><<<grid, CB_THREADS, smem, st>>>(L, n, first, total, err);
-    else
-        b_fp<KIND, MINB><<<grid, CB_THREADS, smem, st>>>(L, n, step, first, total, err);
-}
-
 // One launch of a forward-projection work list (kernel variant for minb resident CTAs per SM): the walk
 // (mode CB_WALK), the replay of planned passes (CB_REPLAY, subset list) or their build (CB_BUILD, PL_BUILD).
 static cudaError_t launch_fp_list(const BatchedPlanHost &P, int which, int minb, int step, int first, int total,
@@ -834,17 +638,7 @@ static cudaError_t launch_fp_list(const BatchedPlanHost &P, int which, int minb,
     cudaError_t e = cudaMemsetAsync(L.counter, 0, sizeof(int), st);
     if (e != cudaSuccess) return e;
     int *err = device_error_ptr();
-    const int n = P.num_scans;
-    if (P.kind == MBX_GEOM_PARALLEL) {
-        if (minb >= 3) launch_fp_kernel<MBX_GEOM_PARALLEL, 3>(mode, grid, smem, st, L, n, step, first, total, err);
-        else launch_fp_kernel<MBX_GEOM_PARALLEL, 2>(mode, grid, smem, st, L, n, step, first, total, err);
-    } else if (P.kind == MBX_GEOM_CONE) {
-        if (minb >= 3) launch_fp_kernel<MBX_GEOM_CONE, 3>(mode, grid, smem, st, L, n, step, first, total, err);
-        else launch_fp_kernel<MBX_GEOM_CONE, 2>(mode, grid, smem, st, L, n, step, first, total, err);
-    } else {
-        if (minb >= 3) launch_fp_kernel<MBX_GEOM_TRANSLATION, 3>(mode, grid, smem, st, L, n, step, first, total, err);
-        else launch_fp_kernel<MBX_GEOM_TRANSLATION, 2>(mode, grid, smem, st, L, n, step, first, total, err);
-    }
+    launch_fp_stage(P.kind, minb, mode, grid, smem, st, L, P.num_scans, step, first, total, err);
     note_launch();
     return cudaGetLastError();
 }
@@ -870,12 +664,13 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
                            const mbx_scan *scans, const FpArgs *hf2, cudaStream_t st) {
     const int num_scans = P.num_scans;
     std::vector<FpArgs> f3(hf2, hf2 + L.ksum);
-    size_t smem3 = 0;
+    size_t smem3 = 0, smem3r = 0;
     int ki = 0;
     for (int s = 0; s < num_scans; ++s) {
-        const CbPlan c3 = plan_fp_cb(scans[s].geom, 0, 0, 3, zs[s].fpp.nb);
+        const CbPlan c3 = plan_fp_cb(scans[s].geom, 0, 0, 3, zs[s].fpp.nb, 0, MBX_BATCHED_FP_CAP);
         if (!c3.ok || c3.nb != zs[s].fpp.nb || c3.cblocks != zs[s].fpp.cblocks) return MBX_OK;  // same work list only
-        smem3 = std::max(smem3, c3.smem);
+        smem3 = std::max(smem3, c3.walk.smem);
+        smem3r = std::max(smem3r, c3.replay.smem);
         for (int k = 0; k < scans[s].num_subsets; ++k, ++ki) f3[ki].plan = c3;
     }
     char *base = reinterpret_cast<char *>(P.t.scans) - L.scans;
@@ -887,6 +682,7 @@ static int tune_batched_fp(BatchedPlanHost &P, const Layout &L, const std::vecto
         if (e3 != cudaSuccess) return set_cuda_error(e3);
         P.fp_minb = 3;
         P.pl_smem[PL_FP] = smem3;
+        P.fp_smem_replay = smem3r;
         P.pl_grid[PL_FP] = fp_grid(P.kind, 3, smem3, P.pl_total[PL_FP]);
         return MBX_OK;
     };
@@ -939,11 +735,11 @@ static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mb
     size_t smem_alt = 0;
     for (int sc = 0; sc < num_scans; ++sc) {
         const CbPlan &c0 = orig[sc * K].plan;
-        const CbPlan q = plan_fp_cb(scans[sc].geom, 0, 0, c0.minb, c0.nb, c0.ppw);
+        const CbPlan q = plan_fp_cb(scans[sc].geom, 0, 0, c0.minb, c0.nb, c0.ppw, MBX_BATCHED_FP_CAP);
         if (!q.ok || q.nb != c0.nb || q.cblocks != c0.cblocks || q.minb != c0.minb) continue;
         can[sc] = 1;
         for (int j = 0; j < K; ++j) alt[sc * K + j].plan = q;
-        smem_alt = std::max(smem_alt, q.smem);
+        smem_alt = std::max(smem_alt, q.walk.smem);
     }
     std::vector<long long> key = batch_key(5, P, scans, false);
     auto use = [&](int sc, int c) {
@@ -955,8 +751,13 @@ static int tune_batched_fp_layouts(BatchedPlanHost &P, const Layout &L, const mb
     };
     auto apply_smem = [&]() {
         size_t sm = 0;
-        for (int k = 0; k < ksum; ++k) sm = std::max(sm, cur[k].plan.smem);
+        size_t smr = 0;
+        for (int k = 0; k < ksum; ++k) {
+            sm = std::max(sm, cur[k].plan.walk.smem);
+            smr = std::max(smr, cur[k].plan.replay.smem);
+        }
         P.pl_smem[PL_FP] = sm;
+        P.fp_smem_replay = smr;
         P.pl_grid[PL_FP] = fp_grid(P.kind, P.fp_minb, sm, P.pl_total[PL_FP]);
     };
     bool all_cached = true;
@@ -1265,8 +1066,10 @@ extern "C" int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans
             f.plan = z.fpp;
             f.chunk_box = reinterpret_cast<const int4 *>(base + L.fbox_off[s]);
             // Hessian: the weights (or ones: no sinogram) with squared coefficients over every pixel
-            hhb[s] = bp_args(g, sc.weights, nullptr, reinterpret_cast<const int32_t *>(base + L.arange), z.npix, 2,
+            hhb[s] = bp_args(z.hbp_slices > 0 ? one_slice_geometry(g) : g, sc.weights, nullptr,
+                             reinterpret_cast<const int32_t *>(base + L.arange), z.npix, 2,
                              const_cast<float *>(sc.fm_hessian), 0, z.hbp);
+            hhb[s].out_slices = z.hbp_slices;
             FiltScan &fl = hfl[s];
             fl.in = sc.sinogram;
             fl.out = sc.error_sinogram;
@@ -1295,7 +1098,7 @@ extern "C" int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans
             list_dims(w, scans[s], zs[s], tiles[s], dim[s], cost[s], L.plan_fp);
             ord[s] = s;
             const ScanSizes &z = zs[s];
-            const size_t sm = w == PL_BP ? z.bpp.smem : (w == PL_FP || w == PL_INIT_FP || w == PL_BUILD) ? z.fpp.smem
+            const size_t sm = w == PL_BP ? z.bpp.smem : (w == PL_FP || w == PL_INIT_FP || w == PL_BUILD) ? z.fpp.walk.smem
                               : w == PL_INIT_BP ? (z.setup ? z.ibp.smem : 0) : (z.setup ? z.hbp.smem : 0);
             pl_smem[w] = std::max(pl_smem[w], sm);
         }
@@ -1364,6 +1167,8 @@ extern "C" int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans
         P.pl_total[w] = L.pl_total[w];
         P.pl_smem[w] = pl_smem[w];
     }
+    P.fp_smem_replay = 0;
+    for (int s = 0; s < n; ++s) P.fp_smem_replay = std::max(P.fp_smem_replay, zs[s].fpp.replay.smem);
     P.el_total = L.el_total;
     P.sn_total = L.sn_total;
     P.rc_total = L.rc_total;
@@ -1443,7 +1248,11 @@ extern "C" int mbx_vcd_batched_prepare2(const mbx_scan *scans, int32_t num_scans
         if (rc2 != MBX_OK) return rc2;
     }
     if (P.planned_fp) {  // the replay and build kernels of the forward variant the tuner kept
-        P.pl_grid_replay = fp_grid(P.kind, P.fp_minb, P.pl_smem[PL_FP], P.pl_total[PL_FP], CB_REPLAY);
+        P.pl_grid_replay = fp_grid(P.kind, P.fp_minb, P.fp_smem_replay, P.pl_total[PL_FP], CB_REPLAY);
+        // the shared-memory carveout the resident replay CTAs need, no more: the rest of the SM's unified
+        // L1 / shared storage caches the row loads of the walk
+        e = set_smem_carveout(fp_kernel_of(P.kind, P.fp_minb, CB_REPLAY), CB_THREADS, P.fp_smem_replay);
+        if (e != cudaSuccess) return set_cuda_error(e);
         P.pl_grid_build = fp_grid(P.kind, P.fp_minb, P.pl_smem[PL_FP], std::max(1, P.pl_total[PL_BUILD]), CB_BUILD);
     }
     P.magic = BT_MAGIC;
@@ -1465,7 +1274,8 @@ static int launch_stage(const BatchedPlanHost *P, int step, int stage, cudaStrea
         case 1: b_delta<<<P->el_grid, BT_THREADS, 0, st>>>(T, n, step, P->el_total, err); break;
         case 2:
             e = launch_fp_list(*P, PL_FP, P->fp_minb, step, 0, P->pl_total[PL_FP],
-                               P->planned_fp ? P->pl_grid_replay : P->pl_grid[PL_FP], P->pl_smem[PL_FP], st,
+                               P->planned_fp ? P->pl_grid_replay : P->pl_grid[PL_FP],
+                               P->planned_fp ? P->fp_smem_replay : P->pl_smem[PL_FP], st,
                                P->planned_fp ? CB_REPLAY : CB_WALK);
             return e == cudaSuccess ? MBX_OK : set_cuda_error(e);
         case 3: b_linquad<<<P->sn_grid, BT_THREADS, 0, st>>>(T, n, P->sn_total); break;

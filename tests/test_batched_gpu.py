@@ -118,25 +118,28 @@ def test_batched_alternative_plans_match_default(cuda):
 
 def test_planned_forward_projections_match_the_walk(cuda):
     """The planned forward projections (each subset's sorted record passes stored once per reconstruction and
-    replayed every iteration) reconstruct bit for bit what the walk (scan and sort every time) does."""
+    replayed every iteration) reconstruct bit for bit what the walk (scan and sort every time) does, and a repeated
+    planned recon is bit for bit the same."""
     from mbirjax_b200 import batched as B
     shapes, seeds = [(40, 6, 48), (23, 9, 37), (61, 4, 64)], [3, 4, 5]
     out = {}
     old = B.PLAN_FORWARD
     try:
+        items = [_scan('parallel', v, r, c, sd) for (v, r, c), sd in zip(shapes, seeds)]
         for planned in (False, True):
             B.PLAN_FORWARD = planned
             B.release_batched_sessions()
-            items = [_scan('parallel', v, r, c, sd) for (v, r, c), sd in zip(shapes, seeds)]
             recons, _ = BatchedVCD([it[0] for it in items], [it[2] for it in items], seeds=seeds).recon(max_iterations=3)
             sess = next(iter(B._SESSIONS.values()))
             assert sess.planned_forward == planned
             out[planned] = [r.cpu() for r in recons]
+        again, _ = BatchedVCD([it[0] for it in items], [it[2] for it in items], seeds=seeds).recon(max_iterations=3)
     finally:
         B.PLAN_FORWARD = old
         B.release_batched_sessions()
-    for a, b in zip(out[False], out[True]):
+    for a, b, c in zip(out[False], out[True], again):
         assert torch.equal(a, b)
+        assert torch.equal(b, c.cpu())
 
 
 def test_graph_replays_count_their_kernels(cuda):

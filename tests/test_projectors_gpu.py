@@ -145,6 +145,13 @@ def test_hessian_diagonal(cuda, kind):
     idx = np.arange(nr * nc, dtype=np.int32)
     atax = model.sparse_back_project(model.sparse_forward_project(xx, idx), idx).cpu().numpy().reshape(nr, nc, ns)
     assert np.isclose(h[i, j, k], atax[i, j, k] / 0.01, rtol=1e-5)
+    # unit weights: the library back-projects no buffer of ones; it must give what a sinogram of ones gives (for
+    # parallel beam it projects one slice and writes it to every slice, which are then exactly equal)
+    ones = np.ones(geom.sinogram_shape, dtype=np.float32)
+    h1 = model.sparse_back_project(ones, idx, coeff_power=2).cpu().numpy().reshape(nr, nc, ns)
+    assert rel_l2(h, h1) <= 1e-6
+    if kind == 'parallel':
+        assert np.array_equal(h, np.broadcast_to(h[:, :, :1], h.shape))
 
 
 @pytest.mark.parametrize('kind', ['parallel', 'cone', 'translation'])
