@@ -31,6 +31,19 @@ __device__ __forceinline__ void flag_error(int *err, int bit) {
     if (err) atomicOr(err, bit);
 }
 
+// Quotient of i by d > 0, and the remainder in r: in 32-bit arithmetic when i fits in 31 bits (every element
+// index of a cylinder list the library admits), a fraction of the instructions of a 64-bit division.
+__device__ __forceinline__ long long div_rem(long long i, int d, int &r) {
+    if (i >= 0 && i <= 0x7fffffffLL) {
+        const unsigned q = (unsigned)i / (unsigned)d;
+        r = (int)((unsigned)i - q * (unsigned)d);
+        return (long long)q;
+    }
+    const long long q = i / d;
+    r = (int)(i - q * d);
+    return q;
+}
+
 // Recon (row, col) of a flat pixel index, as offsets from the recon centre in ALU (y_tilde, x_tilde).
 __device__ __forceinline__ void pixel_tilde(const mbx_geom &g, int idx, float &x_tilde, float &y_tilde) {
     const int row = idx / g.num_recon_cols;

@@ -50,7 +50,8 @@ inline QParams make_qparams(const mbx_qggmrf_params &qp) {
 __device__ __forceinline__ float two_b_tilde(float delta, float b, const QParams &q) {
     const float s = fabsf(delta) / q.t_sigma + 1.1920928955078125e-07f;
     const float d_q2 = powf(s, q.q_minus_2);
-    const float d_qp = powf(s, q.q_minus_p);
+    // p = 2 (the default) makes the two exponents equal: one power, the same value
+    const float d_qp = q.q_minus_p == q.q_minus_2 ? d_q2 : powf(s, q.q_minus_p);
     const float num = d_q2 * (q.q_over_p + d_qp);
     const float den = (1.0f + d_qp) * (1.0f + d_qp);
     return b * (q.scale * num / den);

@@ -59,8 +59,8 @@ __global__ void vcd_delta_kernel(const float *__restrict__ recon, int nr, int nc
     double pl = 0.0, pq = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long p = i / ns;
-        const int k = (int)(i - p * ns);
+        int k;
+        const long long p = div_rem(i, ns, k);
         const int idx = pix[p];
         float d = 0.0f;
         if (idx < 0 || idx >= nr * nc) {
@@ -95,8 +95,8 @@ __global__ void vcd_clip_kernel(const float *__restrict__ recon, int ns, const i
     const float pc = 1.0f / (*alpha + EPS_F32);
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long p = i / ns;
-        const int k = (int)(i - p * ns);
+        int k;
+        const long long p = div_rem(i, ns, k);
         const int idx = pix[p];
         if (idx < 0 || idx >= npix_grid) continue;  // flagged by vcd_delta_kernel; its delta is 0
         delta[i] = fmaxf(-pc * recon[(long long)idx * ns + k], delta[i]);
@@ -161,8 +161,8 @@ __global__ void vcd_apply_kernel(float *__restrict__ recon, int ns, const int32_
     double l1 = 0.0;
     for (long long i = blockIdx.x * (long long)blockDim.x + threadIdx.x; i < total;
          i += (long long)gridDim.x * blockDim.x) {
-        const long long p = i / ns;
-        const int k = (int)(i - p * ns);
+        int k;
+        const long long p = div_rem(i, ns, k);
         const int idx = pix[p];
         if (idx < 0 || idx >= npix_grid) continue;
         const float d = alpha * delta[i];

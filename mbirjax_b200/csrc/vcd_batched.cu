@@ -60,8 +60,8 @@ __global__ void __launch_bounds__(BT_THREADS) b_delta(BatchedTables T, int num_s
         const float fm = T.fm[s];
         double pl = 0.0, pq = 0.0;
         for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
-            const long long p = i / sc.ns;
-            const int k = (int)(i - p * sc.ns);
+            int k;
+            const long long p = div_rem(i, sc.ns, k);
             const int idx = pix[p];
             float d = 0.0f;
             if (idx < 0 || idx >= npix) {
@@ -146,8 +146,8 @@ __global__ void __launch_bounds__(BT_THREADS) b_apply(BatchedTables T, int num_s
         const int npix = sc.nr * sc.nc;
         double l1 = 0.0;
         for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
-            const long long p = i / sc.ns;
-            const int k = (int)(i - p * sc.ns);
+            int k;
+            const long long p = div_rem(i, sc.ns, k);
             const int idx = pix[p];
             if (idx < 0 || idx >= npix) continue;
             const float d = alpha * sc.delta[i];
