@@ -1019,7 +1019,9 @@ __device__ void fp_cb_tile(const FpArgs &A, int j, int cb, float *sm, int *err, 
                 if (tid == 0) flag_error(err, MBX_ERRFLAG_CACHE);
                 continue;
             }
-            __syncthreads();  // the previous pass is done with every list
+            // no barrier before overwriting the lists: every warp read its last record, bin and bin start of the
+            // previous pass before the edge-phase barrier that ends each walk, and after it only the tile is
+            // written (0.7% faster on the batched replay stage than with a barrier per pass here)
             for (int b = tid; b <= nbins; b += CB_THREADS) bstart[b] = PL->pass_bstart[(long long)ps * (nbins + 1) + b];
             for (int i = tid; i < count; i += CB_THREADS) {
                 rec[i] = PL->rec[rs + i];
