@@ -142,6 +142,35 @@ def test_planned_forward_projections_match_the_walk(cuda):
         assert torch.equal(b, c.cpu())
 
 
+def test_unplanned_tiles_are_walked_by_the_replay(cuda):
+    """A tile whose records need more stored passes than a plan holds (here every view of a 1280 x 1280 recon seen by a
+    128-channel detector: about 166 000 pixels in its one channel block, over 80 passes) is walked by the replay
+    kernel in the replay's shared memory with smaller passes; the recon matches the one without planned
+    projections (to float summation order: the passes differ)."""
+    from mbirjax_b200 import batched as B
+    views, rows, channels = 12, 4, 128
+    ang = np.linspace(0, np.pi, views, endpoint=False).astype(np.float32)
+    model = mb.ParallelBeamModel((views, rows, channels), ang)
+    model.set_params(recon_shape=(1280, 1280, rows), sharpness=0.0, granularity=[1], partition_sequence=[0],
+                     verbose=0)
+    rng = np.random.default_rng(9)
+    sino = rng.random((views, rows, channels)).astype(np.float32)
+    out = {}
+    old = B.PLAN_FORWARD
+    try:
+        for planned in (False, True):
+            B.PLAN_FORWARD = planned
+            B.release_batched_sessions()
+            recons, _ = BatchedVCD([model], [sino], seeds=[2]).recon(max_iterations=2)
+            assert next(iter(B._SESSIONS.values())).planned_forward == planned
+            out[planned] = recons[0].cpu().numpy()
+    finally:
+        B.PLAN_FORWARD = old
+        B.release_batched_sessions()
+    assert rel_l2(out[True], out[False]) <= 1e-6
+    assert np.abs(out[False]).max() > 0
+
+
 def test_graph_replays_count_their_kernels(cuda):
     """Every replay of the batched graphs adds the kernels its capture recorded to batched.replayed_launches(), so
     that a benchmark counting library launches sees the replayed ones too."""
