@@ -90,7 +90,24 @@ __global__ void __launch_bounds__(BT_THREADS) b_linquad(BatchedTables T, int num
         const long long e0 = (long long)local * BT_SINO_TILE;
         const long long e1 = min(sc.nsino, e0 + BT_SINO_TILE);
         double fl = 0.0, fq = 0.0;
-        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) {
+        // four elements per load when the scan's buffers are 16-byte aligned (tile starts are), the rest one by one
+        const bool vec = (((uintptr_t)sc.dsino | (uintptr_t)sc.err | (uintptr_t)sc.wts) & 15) == 0;
+        const long long full = vec ? e0 + ((e1 - e0) & ~3LL) : e0;
+        const float4 *ds4 = reinterpret_cast<const float4 *>(sc.dsino), *e4 = reinterpret_cast<const float4 *>(sc.err);
+        const float4 *w4 = reinterpret_cast<const float4 *>(sc.wts);
+        for (long long j = e0 / 4 + threadIdx.x; j < full / 4; j += BT_THREADS) {
+            const float4 ds = __ldg(ds4 + j), e = __ldg(e4 + j);
+            const float4 w = sc.wts ? __ldg(w4 + j) : make_float4(1.0f, 1.0f, 1.0f, 1.0f);
+            fl += (double)((w.x * e.x) * ds.x);
+            fq += (double)(ds.x * ds.x * w.x);
+            fl += (double)((w.y * e.y) * ds.y);
+            fq += (double)(ds.y * ds.y * w.y);
+            fl += (double)((w.z * e.z) * ds.z);
+            fq += (double)(ds.z * ds.z * w.z);
+            fl += (double)((w.w * e.w) * ds.w);
+            fq += (double)(ds.w * ds.w * w.w);
+        }
+        for (long long i = full + threadIdx.x; i < e1; i += BT_THREADS) {
             const float ds = sc.dsino[i], e = sc.err[i];
             const float w = sc.wts ? sc.wts[i] : 1.0f;
             fl += (double)((w * e) * ds);
@@ -167,7 +184,21 @@ __global__ void __launch_bounds__(BT_THREADS) b_error(BatchedTables T, int num_s
         const float alpha = T.alpha[s];
         const long long e0 = (long long)local * BT_SINO_TILE;
         const long long e1 = min(sc.nsino, e0 + BT_SINO_TILE);
-        for (long long i = e0 + threadIdx.x; i < e1; i += BT_THREADS) sc.err[i] -= alpha * sc.dsino[i];
+        // four elements per load when the scan's buffers are 16-byte aligned (tile starts are), the rest one by one
+        const bool vec = (((uintptr_t)sc.dsino | (uintptr_t)sc.err) & 15) == 0;
+        const long long full = vec ? e0 + ((e1 - e0) & ~3LL) : e0;
+        float4 *e4 = reinterpret_cast<float4 *>(sc.err);
+        const float4 *ds4 = reinterpret_cast<const float4 *>(sc.dsino);
+        for (long long j = e0 / 4 + threadIdx.x; j < full / 4; j += BT_THREADS) {
+            float4 e = e4[j];
+            const float4 d = __ldg(ds4 + j);
+            e.x -= alpha * d.x;
+            e.y -= alpha * d.y;
+            e.z -= alpha * d.z;
+            e.w -= alpha * d.w;
+            e4[j] = e;
+        }
+        for (long long i = full + threadIdx.x; i < e1; i += BT_THREADS) sc.err[i] -= alpha * sc.dsino[i];
     }
 }
 
