@@ -673,7 +673,7 @@ __device__ __forceinline__ void ldg_if(float &v, const float *p, int ok) {
 }
 
 #ifndef MBX_FPCB_LOADS2
-#define MBX_FPCB_LOADS2 16  // parallel walk: row loads in flight per lane, variant for 2 CTAs per SM
+#define MBX_FPCB_LOADS2 12  // parallel walk: row loads in flight per lane, variant for 2 CTAs per SM
 #endif
 #ifndef MBX_FPCB_LOADS3
 #define MBX_FPCB_LOADS3 16  // the same, variant for 3 CTAs per SM (85 registers)
@@ -690,8 +690,10 @@ __device__ __forceinline__ void ldg_if(float &v, const float *p, int ok) {
 // and bin from shared memory again and accumulates, so only the loaded values stay in registers across the load
 // latency (4% faster on the batched replay stage than keeping the records live).  Full iterations run unguarded;
 // the last one of a sub-group clamps its record positions to the warp's range and skips the clamped ones.
-// Measured and dropped: more loads in flight (24 or 32 per lane: 30% and 70% slower; the SM's L1 left beside the
-// shared memory of two CTAs thrashes), the row loads without L1 allocation or cached in L2 only (37% and 4%
+// Row loads in flight per lane, measured on the batched replay stage: 8, 10, 12, 16 -> 11.90, 11.39, 11.21, 11.40 ms
+// (24 and 32, in an earlier build: 15.0 and 19.5 ms against 11.6 for 16; more lines in flight thrash the L1 that
+// two CTAs' shared memory leaves).
+// Measured and dropped: the row loads without L1 allocation or cached in L2 only (37% and 4%
 // slower), one guarded loop instead of the unguarded loop and a tail (10% slower), sub-groups walking whole bins
 // of their own (they diverge at every bin end).
 template <int PPW, int RPL, int MINB>
