@@ -5,13 +5,46 @@
 //    order;
 //  - the replay layout holds the tile, the records of a walk-sized pass and the bin starts;
 //  - the smaller walk used by the replay kernel for tiles a build could not store fits the replay's shared memory;
+// and for the back projector's plans (bp_fast.cuh, staged and per-thread footprints, any pixel count and view
+// selection) that the CTA shape, slice tiles, view chunks and splits cover the work, that shared memory stays
+// within the 100 KB its launches allow, and that a cone slice tile's rows fit the row cache;
 // printing "ok <plans checked>" or the first failure.  Runs on the CPU (no device call).
 #include <cmath>
 #include <cstdio>
 
+#include "../mbirjax_b200/csrc/bp_fast.cuh"
 #include "../mbirjax_b200/csrc/fp_cb.cuh"
 
+namespace mbx {
+int num_sms() { return 148; }  // the device query of the library, for a B200
+}  // namespace mbx
+
 using namespace mbx;
+
+// Back-projection plan invariants; returns a failure text or nullptr.
+static const char *bp_plan_error(const mbx_geom &g, const BpfPlan &pl, long long n, int nv) {
+    const int S = g.num_recon_slices;
+    if (pl.nsl * pl.npg != 8 || (1 << pl.lg_pcta) != 32 * pl.npg) return "CTA shape";
+    if (pl.ts < 1 || pl.ts > BPF_ST || (long long)pl.tiles * pl.ts < S || (long long)(pl.tiles - 1) * pl.ts >= S)
+        return "slice tiles";
+    if (pl.gy != (pl.tiles + pl.nsl - 1) / pl.nsl) return "grid y";
+    if ((long long)pl.gx * 32 * pl.npg < n) return "grid x";
+    if (!pl.inline_fp && (pl.chunk % (32 * pl.npg) || pl.vc != pl.chunk / (32 * pl.npg) || pl.vc < 1)) return "chunk";
+    if (pl.splits < 1 || pl.splits > 64 || (long long)pl.splits * pl.views_per_split < nv ||
+        (long long)(pl.splits - 1) * pl.views_per_split >= nv)
+        return "view splits";
+    if ((pl.splits > 1) != (pl.workspace > 0) || (pl.splits > 1 && pl.workspace < (size_t)pl.splits * n * S * 4))
+        return "workspace";
+    if (pl.smem > 100 * 1024) return "shared memory";
+    if (g.kind != MBX_GEOM_PARALLEL && pl.ok) {
+        const double half_r = 0.5 * (g.num_recon_rows - 1), half_c = 0.5 * (g.num_recon_cols - 1);
+        const double rho = g.delta_voxel * std::sqrt(half_r * half_r + half_c * half_c);
+        const double inv = 1.0 / g.magnification - rho / g.source_detector_dist;
+        const double mag = g.kind == MBX_GEOM_TRANSLATION ? g.max_magnification : 1.0 / inv;
+        if (pl.ts * mag * g.delta_voxel / g.delta_det_row + 4 > BPF_CACHE_ROWS) return "row cache";
+    }
+    return nullptr;
+}
 
 static int fail(const char *what, int kind, int R, int C) {
     std::printf("FAIL %s kind=%d R=%d C=%d\n", what, kind, R, C);
@@ -82,6 +115,33 @@ int main() {
                             if (!layout_ok(pl, pl.small, kind, R, false)) return fail("small layout", kind, R, C);
                             if (pl.small.smem > pl.replay.smem) return fail("small walk over replay smem", kind, R, C);
                             if (pl.rpad < R || pl.rpad != pl.row_passes * pl.rl * pl.rpl) return fail("rows", kind, R, C);
+                        }
+            }
+    for (int kind : kinds)
+        for (int S = 1; S <= 200; S += (S < 40 ? 1 : 7))
+            for (int C : chans) {
+                mbx_geom g = {};
+                g.kind = kind;
+                g.num_views = 180;
+                g.num_det_rows = S;
+                g.num_det_channels = C;
+                g.num_recon_rows = g.num_recon_cols = C;
+                g.num_recon_slices = S;
+                g.psf_radius = g.bp_psf_radius = 1;
+                g.entries_per_cylinder_batch = 128;
+                g.delta_det_channel = g.delta_det_row = g.delta_voxel = 1.0f;
+                g.source_detector_dist = kind == MBX_GEOM_PARALLEL ? INFINITY : 4.0f * C;
+                g.magnification = kind == MBX_GEOM_PARALLEL ? 1.0f : 2.0f;
+                g.delta_recon_row = 1.0f;
+                g.max_magnification = kind == MBX_GEOM_TRANSLATION ? 2.0f : 0.0f;
+                for (long long n : {1LL, 31LL, 1000LL, 20000LL, (long long)C * C})
+                    for (int nv : {1, 16, 180})
+                        for (int inl = 0; inl <= 1; ++inl) {
+                            const BpfPlan pl = plan_bp_fast(g, n, nv, inl);
+                            if (!pl.ok) continue;
+                            ++checked;
+                            const char *e = bp_plan_error(g, pl, n, nv);
+                            if (e) return fail(e, kind, S, C);
                         }
             }
     std::printf("ok %ld\n", checked);
